@@ -1,0 +1,167 @@
+/*
+ * chanfast_cuda -- B200 (sm_100a) FP64 implementation of the RK3 substep of the
+ * staggered-grid channel-flow DNS of nasilemakbox/ubiquitous-spoon, behind a
+ * plain C ABI.  Two shared libraries implement it:
+ *
+ *   libchanfast_cuda.so  device engine + this instance API (cf_*)
+ *   libchanfast.so       drop-in drivers chanfast2 / chanfast4 in C, on top of
+ *                        the instance API
+ *
+ * Conventions
+ *  - Every cf_* function returns an int status: CF_OK (0) or a negative CF_E*
+ *    code; nothing aborts the process.  cf_strerror() names a code.
+ *  - Fields cross the ABI as flat FP64 arrays in one of two layouts:
+ *      CF_LAYOUT_PADDED   [nx+2*ngx][ny+2*ngy][nz+2*ngz], wall-normal index
+ *                         fastest, ghosts included -- the reference's field
+ *                         layout (d3tensor.c:9-42, chanfast.c:105-137)
+ *      CF_LAYOUT_INTERIOR [nx][ny][nz], interior only -- the reference's
+ *                         restart-file layout (io.c:211-297)
+ *    Axes are the reference's: x streamwise (periodic), y spanwise (periodic),
+ *    z wall-normal (walls, cosine-stretched).
+ *  - An instance owns its device memory and is bound to the CUDA device that
+ *    was current at cf_create.  Calls on one instance must be serialised by
+ *    the caller; distinct instances may be driven from distinct threads.
+ */
+#ifndef CHANFAST_CUDA_H
+#define CHANFAST_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CF_OK = 0,
+    CF_EINVAL = -1,      /* bad argument or unsupported configuration */
+    CF_ENOMEM = -2,      /* device or host allocation failed */
+    CF_ECUDA = -3,       /* a CUDA runtime call failed */
+    CF_EPIVOT = -4,      /* zero pivot in a band factorisation */
+    CF_ENONFINITE = -5,  /* a field contains NaN or Inf */
+    CF_EIO = -6          /* restart / log file error (drivers) */
+};
+
+enum { CF_U = 0, CF_V = 1, CF_W = 2, CF_C = 3, CF_P = 4 };
+enum { CF_LAYOUT_PADDED = 0, CF_LAYOUT_INTERIOR = 1 };
+
+/* Arguments of chanfast2 / chanfast4 (reference chanfast.h:1-21) that
+ * determine one run; p_row = p_col = 1, it/nt/istat/cfl belong to the driver. */
+typedef struct cf_config {
+    int order;               /* 2 (chanfast2) or 4 (chanfast4) */
+    int nx, ny, nz;          /* interior grid */
+    int ngx, ngy, ngz;       /* ghost widths of the padded layout; ngz must be 3 */
+    int uvolavgmode;         /* 1: constant flow rate (chanfast.c:515) */
+    int cvolavgmode;         /* 1: constant scalar mean (chanfast.c:602) */
+    double lx, ly, lz;       /* box; lz = channel height */
+    double dt, nu, prandtl, dpdx;
+    double want_uvolavg, want_cvolavg;
+    double setuframe, setvframe;      /* Galilean frame (chanfast.c:61-64) */
+    double betg_x, betg_y, betg_z;    /* buoyancy */
+} cf_config;
+
+typedef struct cf_instance cf_instance;
+
+/* Create / destroy an instance on the current CUDA device.  Replaces the
+ * setup part of chanfast2/chanfast4 (chanfast.c:85-301): grid metrics,
+ * field allocation, FFT plans, line-solve factorisations.  `stream` is a
+ * cudaStream_t (NULL: the instance creates its own). */
+int cf_create(const cf_config *cfg, void *stream, cf_instance **out);
+int cf_destroy(cf_instance *inst);
+
+/* Copy a field in or out.  Host pointers; `layout` as above.  cf_get_field
+ * fills the x/y ghosts of the padded layout periodically and returns the
+ * wall-normal ghost rows as they are held on the device.  Replaces io_read /
+ * io_write + ghostz_pad/ghostz_truncate (io.c:211-297, ghostz.c:152-177).
+ * CF_P is read-only. */
+int cf_set_field(cf_instance *inst, int field, const double *host, int layout);
+int cf_get_field(cf_instance *inst, int field, double *host, int layout);
+
+/* Seeded initial state, generated on the device: laminar Poiseuille u plus a
+ * uniform random perturbation of amplitude amp*1.5 on u, v, w (SplitMix64 of
+ * seed/field/global index), scalar -0.5 + z/2 plus c_amp noise, then made
+ * discretely divergence-free by one projection with dt = 1 (cases.c:426-470). */
+int cf_init_fields(cf_instance *inst, unsigned long long seed, double amp, double c_amp);
+
+/* Advance `nsub` RK3 substeps (3 per time step) -- the body of
+ * chanfast.c:395-656 (order 2) / 1319-1580 (order 4) -- asynchronously on
+ * the instance stream.  The substep counter and the previous-stage
+ * right-hand sides persist across calls. */
+int cf_step(cf_instance *inst, int nsub);
+
+/* Same as cf_step, replaying a CUDA graph of one full RK3 step (3 substeps)
+ * captured on first use; nsteps counts full steps. */
+int cf_step_graph(cf_instance *inst, int nsteps);
+
+/* Wait for all work of the instance. */
+int cf_sync(cf_instance *inst);
+
+/* Per-substep log rows (10 doubles each): mdpdx, nu du/dz bottom, top, bulk
+ * velocity, centreline velocity, then dcdt and the same four scalar
+ * statistics -- the values chanfast appends to pstat.dat / cstat.dat
+ * (chanfast.c:525-528, 612-615).  Returns the number of rows written into
+ * `out` (at most max_rows, most recent last) or a negative status. */
+long cf_get_log(cf_instance *inst, double *out, long max_rows);
+
+/* Number of substeps done so far. */
+long cf_substeps_done(const cf_instance *inst);
+
+/* max |div u| over the interior cells with the reference operator
+ * divergence{2,4} (pressure.c:40-117), evaluated on the device. */
+int cf_max_divergence(cf_instance *inst, double *out);
+
+/* CFL number of the current velocity field for time step dt, as get_cfl
+ * (get.c:390-416): max over interior cells of |u| dt/dx, |v| dt/dy,
+ * |w| dt/dzph, evaluated on the device; synchronises the instance. */
+int cf_cfl(cf_instance *inst, double dt, double *cfl);
+
+/* Change the time step (rebuilds the per-substep line-solve factorisations;
+ * used by the drivers when cflmode == 1, chanfast.c:385-391). */
+int cf_set_dt(cf_instance *inst, double dt);
+
+/* Device pointer of a field in the engine layout [n2][nx][ny] (k slowest),
+ * for callers that keep data on the device. */
+int cf_device_field(cf_instance *inst, int field, double **dev_ptr, long long *n_elems);
+
+/* Number of kernel launches the engine issues per substep. */
+int cf_launches_per_substep(const cf_instance *inst);
+
+const char *cf_strerror(int status);
+
+/* ------------------------------------------------------------------------
+ * Drop-in drivers (libchanfast.so).  Same names and arguments as the
+ * reference (chanfast.h:1-21, called at main.c:56-60); they read
+ * outputdir/{u,v,w,c}_it<it>.dat, run nt - it time steps on the current
+ * CUDA device, append outputdir/cfl.dat, pstat.dat and cstat.dat, and write
+ * outputdir/{u,v,w,c,p}_it<N>.dat every istat steps.  p_row * p_col must be
+ * 1.  The reference returns nothing and aborts on error; these print the
+ * failing status to stderr and return.  chanfast2_status / chanfast4_status
+ * return it instead.
+ * ------------------------------------------------------------------------ */
+void chanfast2(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+               int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+               double dt, double want_cfl, int cflmode, double nu, double prandtl,
+               double dpdx, double want_uvolavg, int uvolavgmode,
+               double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+               double betg_x, double betg_y, double betg_z);
+void chanfast4(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+               int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+               double dt, double want_cfl, int cflmode, double nu, double prandtl,
+               double dpdx, double want_uvolavg, int uvolavgmode,
+               double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+               double betg_x, double betg_y, double betg_z);
+int chanfast2_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                     int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                     double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                     double dpdx, double want_uvolavg, int uvolavgmode,
+                     double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                     double betg_x, double betg_y, double betg_z);
+int chanfast4_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                     int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                     double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                     double dpdx, double want_uvolavg, int uvolavgmode,
+                     double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                     double betg_x, double betg_y, double betg_z);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHANFAST_CUDA_H */

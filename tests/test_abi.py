@@ -1,0 +1,65 @@
+"""The C-ABI libraries load and export every entry point include/*.h declares
+(no device work: no GPU is needed)."""
+import ctypes
+import glob
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "ubiquitous-spoon_b200")
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    names.discard("if")
+    return names
+
+
+def exported(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+@pytest.fixture(scope="module")
+def libs(cf):
+    cf.lib()
+    cf.driver_lib()
+    return os.path.join(PKG, "libchanfast_cuda.so"), os.path.join(PKG, "libchanfast.so")
+
+
+def test_every_declared_symbol_is_exported(libs):
+    decl = declared_functions()
+    assert {"cf_create", "cf_step", "chanfast2", "chanfast4"} <= decl
+    have = exported(libs[0]) | exported(libs[1])
+    missing = sorted(decl - have)
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_strerror_and_argument_checks(cf):
+    L = cf.lib()
+    assert L.cf_strerror(0) == b"ok"
+    assert b"invalid" in L.cf_strerror(-1)
+    # argument validation happens before any device work
+    h = ctypes.c_void_p()
+    bad = cf.Config.make(order=3, nx=16, ny=16, nz=16, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3)
+    assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL
+    bad = cf.Config.make(order=4, nx=16, ny=16, nz=16, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3, ngz=2)
+    assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL
+    bad = cf.Config.make(order=4, nx=14, ny=16, nz=16, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3)
+    assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL  # 14 = 2*7: no radix-7 FFT
+    assert L.cf_step(None, 1) == cf.CF_EINVAL
+
+
+def test_config_mirrors_reference_arguments(cf):
+    import chanfast_np as cn
+    p = cn.Params(order=4, nx=8, ny=8, nz=8, lx=1, ly=1, lz=2, dt=1e-3, nu=1e-3)
+    c = cf.Config.from_params(p)
+    assert (c.order, c.nx, c.ngz) == (4, 8, 3)

@@ -1,0 +1,232 @@
+"""Python host mirror of the chanfast_cuda C ABI (include/chanfast_cuda.h).
+
+The compute path is the CUDA library libchanfast_cuda.so built in this
+directory (build.py); this module only binds it with ctypes and mirrors the
+reference's driver arguments (chanfast.h:1-21).  There is no CPU fallback:
+importing works without a GPU, but every call that needs the engine raises if
+the library is missing or no CUDA device is present.
+
+The directory name is not a Python identifier; import it with
+``importlib.import_module("ubiquitous-spoon_b200")`` (the repository root on
+sys.path).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_CUDA = os.path.join(HERE, "libchanfast_cuda.so")
+LIB_DRIVER = os.path.join(HERE, "libchanfast.so")
+
+CF_OK, CF_EINVAL, CF_ENOMEM, CF_ECUDA, CF_EPIVOT, CF_ENONFINITE, CF_EIO = 0, -1, -2, -3, -4, -5, -6
+FIELDS = {"u": 0, "v": 1, "w": 2, "c": 3, "p": 4}
+LAYOUT_PADDED, LAYOUT_INTERIOR = 0, 1
+LOG_COLS = 10
+
+_lib = None
+_drv = None
+
+
+class ChanfastError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__(f"{what}: status {status} ({strerror(status)})")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    """Mirror of cf_config."""
+
+    _fields_ = [(n, ctypes.c_int) for n in
+                ("order", "nx", "ny", "nz", "ngx", "ngy", "ngz", "uvolavgmode", "cvolavgmode")] + \
+               [(n, ctypes.c_double) for n in
+                ("lx", "ly", "lz", "dt", "nu", "prandtl", "dpdx", "want_uvolavg", "want_cvolavg",
+                 "setuframe", "setvframe", "betg_x", "betg_y", "betg_z")]
+
+    @classmethod
+    def make(cls, order, nx, ny, nz, lx, ly, lz, dt, nu, prandtl=1.0, dpdx=0.0,
+             want_uvolavg=1.0, uvolavgmode=1, want_cvolavg=0.0, cvolavgmode=1,
+             setuframe=0.0, setvframe=0.0, betg_x=0.0, betg_y=0.0, betg_z=0.0,
+             ngx=3, ngy=3, ngz=3):
+        c = cls()
+        for k, v in dict(order=order, nx=nx, ny=ny, nz=nz, ngx=ngx, ngy=ngy, ngz=ngz,
+                         uvolavgmode=uvolavgmode, cvolavgmode=cvolavgmode, lx=lx, ly=ly, lz=lz,
+                         dt=dt, nu=nu, prandtl=prandtl, dpdx=dpdx, want_uvolavg=want_uvolavg,
+                         want_cvolavg=want_cvolavg, setuframe=setuframe, setvframe=setvframe,
+                         betg_x=betg_x, betg_y=betg_y, betg_z=betg_z).items():
+            setattr(c, k, v)
+        return c
+
+    @classmethod
+    def from_params(cls, p):
+        """From any object with the same attribute names (e.g. the oracle's Params)."""
+        c = cls()
+        for name, _ in cls._fields_:
+            setattr(c, name, getattr(p, name))
+        return c
+
+    def padded_shape(self):
+        return (self.nx + 2 * self.ngx, self.ny + 2 * self.ngy, self.nz + 2 * self.ngz)
+
+    def interior_shape(self):
+        return (self.nx, self.ny, self.nz)
+
+
+def _bind(L):
+    vp, ip, dp, ll = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long
+    L.cf_create.argtypes = [ctypes.POINTER(Config), vp, ctypes.POINTER(vp)]
+    L.cf_destroy.argtypes = [vp]
+    L.cf_set_field.argtypes = [vp, ip, dp, ip]
+    L.cf_get_field.argtypes = [vp, ip, dp, ip]
+    L.cf_init_fields.argtypes = [vp, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_double]
+    L.cf_step.argtypes = [vp, ip]
+    L.cf_step_graph.argtypes = [vp, ip]
+    L.cf_sync.argtypes = [vp]
+    L.cf_get_log.restype = ll
+    L.cf_get_log.argtypes = [vp, dp, ll]
+    L.cf_substeps_done.restype = ll
+    L.cf_substeps_done.argtypes = [vp]
+    L.cf_max_divergence.argtypes = [vp, dp]
+    L.cf_cfl.argtypes = [vp, ctypes.c_double, dp]
+    L.cf_set_dt.argtypes = [vp, ctypes.c_double]
+    L.cf_device_field.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)]
+    L.cf_launches_per_substep.argtypes = [vp]
+    L.cf_strerror.restype = ctypes.c_char_p
+    L.cf_strerror.argtypes = [ip]
+    return L
+
+
+def lib():
+    """The engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_CUDA):
+            raise FileNotFoundError(f"{LIB_CUDA} not built; run python ubiquitous-spoon_b200/build.py")
+        _lib = _bind(ctypes.CDLL(LIB_CUDA))
+    return _lib
+
+
+def driver_lib():
+    """libchanfast.so: the C drop-in drivers chanfast2 / chanfast4."""
+    global _drv
+    if _drv is None:
+        lib()
+        if not os.path.exists(LIB_DRIVER):
+            raise FileNotFoundError(f"{LIB_DRIVER} not built")
+        D = ctypes.CDLL(LIB_DRIVER)
+        args = ([ctypes.c_int] * 11 + [ctypes.c_double] * 5 + [ctypes.c_int] + [ctypes.c_double] * 4
+                + [ctypes.c_int] + [ctypes.c_double, ctypes.c_int] + [ctypes.c_double] * 5)
+        for name in ("chanfast2_status", "chanfast4_status"):
+            getattr(D, name).argtypes = args
+            getattr(D, name).restype = ctypes.c_int
+        _drv = D
+    return _drv
+
+
+def strerror(status):
+    try:
+        return lib().cf_strerror(status).decode()
+    except Exception:
+        return "unknown"
+
+
+def _check(status, what):
+    if status != CF_OK:
+        raise ChanfastError(status, what)
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Instance:
+    """One channel-flow state resident on the current CUDA device."""
+
+    def __init__(self, cfg: Config, stream=None):
+        self.L = lib()
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        _check(self.L.cf_create(ctypes.byref(cfg), stream, ctypes.byref(h)), "cf_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.cf_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_field(self, name, array, layout=LAYOUT_PADDED):
+        shape = self.cfg.padded_shape() if layout == LAYOUT_PADDED else self.cfg.interior_shape()
+        a = np.ascontiguousarray(array, dtype=np.float64).reshape(shape)
+        _check(self.L.cf_set_field(self.h, FIELDS[name], _dp(a), layout), "cf_set_field")
+
+    def get_field(self, name, layout=LAYOUT_PADDED):
+        shape = self.cfg.padded_shape() if layout == LAYOUT_PADDED else self.cfg.interior_shape()
+        a = np.empty(shape)
+        _check(self.L.cf_get_field(self.h, FIELDS[name], _dp(a), layout), "cf_get_field")
+        return a
+
+    def init_fields(self, seed, amp, c_amp):
+        _check(self.L.cf_init_fields(self.h, seed, amp, c_amp), "cf_init_fields")
+
+    def step(self, nsub):
+        _check(self.L.cf_step(self.h, nsub), "cf_step")
+
+    def step_graph(self, nsteps):
+        _check(self.L.cf_step_graph(self.h, nsteps), "cf_step_graph")
+
+    def sync(self):
+        _check(self.L.cf_sync(self.h), "cf_sync")
+
+    def substeps_done(self):
+        return int(self.L.cf_substeps_done(self.h))
+
+    def log(self, max_rows=100000):
+        out = np.empty((max_rows, LOG_COLS))
+        n = self.L.cf_get_log(self.h, _dp(out), max_rows)
+        if n < 0:
+            _check(int(n), "cf_get_log")
+        return out[:n]
+
+    def max_divergence(self):
+        d = ctypes.c_double()
+        _check(self.L.cf_max_divergence(self.h, ctypes.byref(d)), "cf_max_divergence")
+        return d.value
+
+    def cfl(self, dt):
+        d = ctypes.c_double()
+        _check(self.L.cf_cfl(self.h, dt, ctypes.byref(d)), "cf_cfl")
+        return d.value
+
+    def set_dt(self, dt):
+        _check(self.L.cf_set_dt(self.h, dt), "cf_set_dt")
+
+    def device_field(self, name):
+        p = ctypes.c_void_p()
+        n = ctypes.c_longlong()
+        _check(self.L.cf_device_field(self.h, FIELDS[name], ctypes.byref(p), ctypes.byref(n)), "cf_device_field")
+        return p.value, n.value
+
+    def launches_per_substep(self):
+        return int(self.L.cf_launches_per_substep(self.h))
+
+
+def chanfast(order, *args):
+    """Call the C drop-in driver chanfast2/chanfast4 (same arguments as the
+    reference, chanfast.h:1-21); returns the status instead of aborting."""
+    D = driver_lib()
+    fn = D.chanfast2_status if order == 2 else D.chanfast4_status
+    return fn(*args)

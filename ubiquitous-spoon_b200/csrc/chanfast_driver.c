@@ -1,0 +1,178 @@
+/*
+ * Drop-in drivers chanfast2 / chanfast4 in C over the chanfast_cuda C ABI.
+ *
+ * Same arguments and file protocol as the reference drivers (chanfast.h:1-21,
+ * chanfast.c:71-992 / 995-1916) at p_row = p_col = 1:
+ *   - read outputdir/{u,v,w,c}_it<it>.dat (raw FP64, C order [nx][ny][nz],
+ *     io.c:259-297)
+ *   - for it in [it, nt): CFL of the current field (get.c:390-416), adapt dt
+ *     if cflmode == 1, append "it dt cfl" to outputdir/cfl.dat; three RK3
+ *     substeps on the GPU; append the mass-flux and scalar-mean statistics of
+ *     the last substep to outputdir/pstat.dat and outputdir/cstat.dat
+ *     (chanfast.c:525-528, 612-615)
+ *   - every istat steps write outputdir/{u,v,w,c}_it<it+1>.dat (io.c:211-257)
+ * The per-istat statistics profiles and spectra of chanfast.c:658-857 are
+ * not produced.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "chanfast_cuda.h"
+
+static int read_field(cf_instance *inst, int field, const char *name, int it, size_t n)
+{
+    char fname[256];
+    snprintf(fname, sizeof fname, "outputdir/%s_it%d.dat", name, it);
+    FILE *fp = fopen(fname, "rb");
+    if (!fp) return CF_EIO;
+    double *buf = (double *) malloc(n * sizeof(double));
+    if (!buf) { fclose(fp); return CF_ENOMEM; }
+    size_t got = fread(buf, sizeof(double), n, fp);
+    fclose(fp);
+    int rc = got == n ? cf_set_field(inst, field, buf, CF_LAYOUT_INTERIOR) : CF_EIO;
+    free(buf);
+    return rc;
+}
+
+static int write_field(cf_instance *inst, int field, const char *name, int it, size_t n)
+{
+    char fname[256];
+    snprintf(fname, sizeof fname, "outputdir/%s_it%d.dat", name, it);
+    double *buf = (double *) malloc(n * sizeof(double));
+    if (!buf) return CF_ENOMEM;
+    int rc = cf_get_field(inst, field, buf, CF_LAYOUT_INTERIOR);
+    if (rc == CF_OK) {
+        FILE *fp = fopen(fname, "wb");
+        if (!fp) rc = CF_EIO;
+        else {
+            if (fwrite(buf, sizeof(double), n, fp) != n) rc = CF_EIO;
+            if (fclose(fp) != 0) rc = CF_EIO;
+        }
+    }
+    free(buf);
+    return rc;
+}
+
+/* io_append_ascii (io.c:5-19) */
+static int append_ascii(const double *u, int n, const char *filename)
+{
+    FILE *fp = fopen(filename, "a");
+    if (!fp) return CF_EIO;
+    fprintf(fp, "%+e", u[0]);
+    for (int i = 1; i < n; i++) fprintf(fp, " %+e", u[i]);
+    fprintf(fp, "\n");
+    return fclose(fp) == 0 ? CF_OK : CF_EIO;
+}
+
+static int run(int order, int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+               int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+               double dt, double want_cfl, int cflmode, double nu, double prandtl,
+               double dpdx, double want_uvolavg, int uvolavgmode,
+               double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+               double betg_x, double betg_y, double betg_z)
+{
+    if (p_row * p_col != 1 || istat <= 0) return CF_EINVAL;
+    cf_config cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cfg.order = order;
+    cfg.nx = nx; cfg.ny = ny; cfg.nz = nz;
+    cfg.ngx = nghost_x; cfg.ngy = nghost_y; cfg.ngz = nghost_z;
+    cfg.uvolavgmode = uvolavgmode; cfg.cvolavgmode = cvolavgmode;
+    cfg.lx = lx; cfg.ly = ly; cfg.lz = lz;
+    cfg.dt = dt; cfg.nu = nu; cfg.prandtl = prandtl; cfg.dpdx = dpdx;
+    cfg.want_uvolavg = want_uvolavg; cfg.want_cvolavg = want_cvolavg;
+    cfg.setuframe = setuframe; cfg.setvframe = setvframe;
+    cfg.betg_x = betg_x; cfg.betg_y = betg_y; cfg.betg_z = betg_z;
+
+    cf_instance *inst = NULL;
+    int rc = cf_create(&cfg, NULL, &inst);
+    if (rc) return rc;
+    const size_t n = (size_t) nx * ny * nz;
+    const char *names[4] = {"u", "v", "w", "c"};
+    const int fields[4] = {CF_U, CF_V, CF_W, CF_C};
+    for (int f = 0; f < 4 && rc == CF_OK; f++) rc = read_field(inst, fields[f], names[f], it, n);
+
+    double log[10];
+    for (; rc == CF_OK && it < nt; it++) {
+        double cfl = 0.0;
+        rc = cf_cfl(inst, dt, &cfl);
+        if (rc) break;
+        if (cflmode == 1) {  /* chanfast.c:388-391 */
+            double ndt = dt * (cfl > 0.0 ? want_cfl / cfl : 1.0);
+            cfl = cfl > 0.0 ? want_cfl : cfl;
+            if (ndt != dt) {
+                dt = ndt;
+                rc = cf_set_dt(inst, dt);
+                if (rc) break;
+            }
+        }
+        double row[3] = {(double) it, dt, cfl};
+        rc = append_ascii(row, 3, "outputdir/cfl.dat");
+        if (rc) break;
+        rc = cf_step(inst, 3);
+        if (rc) break;
+        long got = cf_get_log(inst, log, 1);
+        if (got != 1) { rc = got < 0 ? (int) got : CF_ECUDA; break; }
+        double ps[6] = {(double) (it + 1), log[0], log[1], log[2], log[3], log[4]};
+        double cs[6] = {(double) (it + 1), log[5], log[6], log[7], log[8], log[9]};
+        rc = append_ascii(ps, 6, "outputdir/pstat.dat");
+        if (rc == CF_OK) rc = append_ascii(cs, 6, "outputdir/cstat.dat");
+        if (rc == CF_OK && (it + 1) % istat == 0)
+            for (int f = 0; f < 4 && rc == CF_OK; f++) rc = write_field(inst, fields[f], names[f], it + 1, n);
+    }
+    int rc2 = cf_destroy(inst);
+    return rc ? rc : rc2;
+}
+
+int chanfast2_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                     int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                     double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                     double dpdx, double want_uvolavg, int uvolavgmode,
+                     double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                     double betg_x, double betg_y, double betg_z)
+{
+    return run(2, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z, lx, ly, lz,
+               dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg,
+               cvolavgmode, setuframe, setvframe, betg_x, betg_y, betg_z);
+}
+
+int chanfast4_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                     int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                     double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                     double dpdx, double want_uvolavg, int uvolavgmode,
+                     double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                     double betg_x, double betg_y, double betg_z)
+{
+    return run(4, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z, lx, ly, lz,
+               dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg,
+               cvolavgmode, setuframe, setvframe, betg_x, betg_y, betg_z);
+}
+
+void chanfast2(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+               int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+               double dt, double want_cfl, int cflmode, double nu, double prandtl,
+               double dpdx, double want_uvolavg, int uvolavgmode,
+               double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+               double betg_x, double betg_y, double betg_z)
+{
+    int rc = chanfast2_status(p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z,
+                              lx, ly, lz, dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg,
+                              uvolavgmode, want_cvolavg, cvolavgmode, setuframe, setvframe,
+                              betg_x, betg_y, betg_z);
+    if (rc) fprintf(stderr, "chanfast2: %s\n", cf_strerror(rc));
+}
+
+void chanfast4(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+               int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+               double dt, double want_cfl, int cflmode, double nu, double prandtl,
+               double dpdx, double want_uvolavg, int uvolavgmode,
+               double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+               double betg_x, double betg_y, double betg_z)
+{
+    int rc = chanfast4_status(p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z,
+                              lx, ly, lz, dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg,
+                              uvolavgmode, want_cvolavg, cvolavgmode, setuframe, setvframe,
+                              betg_x, betg_y, betg_z);
+    if (rc) fprintf(stderr, "chanfast4: %s\n", cf_strerror(rc));
+}

@@ -1,0 +1,161 @@
+// Device engine of the channel-flow RK3 substep (sm_100a, FP64).
+//
+// Device layout of every field: [k][i][j], wall-normal index k slowest and
+// spanwise index j fastest, no x/y ghost cells (periodicity is modular
+// indexing), all n2 = nz + 2*gz wall-normal rows kept.  Column c = i*ny + j.
+// One z line is therefore a strided column whose rows are contiguous across
+// neighbouring columns, so the per-column line solves run one thread per
+// column with coalesced row accesses.  The reference's own layout
+// ([i][j][k], k fastest, padded by ghosts in x and y; d3tensor.c:9-42) is
+// converted only at the API boundary.
+//
+// Spectral layout: complex [k][kx][ky], kx in [0, nx/2], ky in [0, ny).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cf {
+
+constexpr int GZ = 3;                // wall-normal ghost rows (reference main.c:13)
+constexpr int MAX_FFT_STAGES = 12;
+constexpr int LOG_COLS = 10;
+
+// Band coefficient rows of one wall closure (rows k, k-+1, k-+2; a..g).
+struct WallRowsD {
+    double row[3][7];
+};
+
+// Geometry / metric tables shared by all kernels of an instance.
+struct Geo {
+    int order, nx, ny, nz, n2, nkx;
+    long long plane;      // nx*ny (points per k-plane)
+    long long splane;     // nkx*ny (spectral columns per k-plane)
+    double dx, dy;
+    const double* dz;     // [n2]
+    const double* dzp1h;  // 0.5*(dz[k+1]+dz[k])  [n2] (last entry 0)
+    const double* dzm1h;  // 0.5*(dz[k-1]+dz[k])  [n2] (first entry 0)
+    const double* dzp3h;  // 0.5*(dz[k+2]+dz[k+1])
+    const double* dzm3h;  // 0.5*(dz[k-2]+dz[k-1])
+    const double* dydz;   // dy*dz[k]
+    const double* dxdz;   // dx*dz[k]
+    double dxdy;          // dx*dy
+};
+
+// Line-solve factorisation on device (see host_band.h LineFactor).
+struct FactorD {
+    int k0, n;
+    const double *F1, *F2, *F3, *DEN, *P, *Q, *R;
+};
+
+// Arguments of one implicit solve launch.
+struct SolveArgs {
+    double* x;            // field (in: old value, out: new value)
+    const double* f;      // current RHS
+    const double* g;      // previous-stage RHS
+    const double* gshift; // device scalar added to g (mass-flux lazily applied), or null
+    FactorD fac;
+    const double* hbc;    // [n2]
+    double nuadt, gamdt, zetdt;
+    double bc_bot, bc_top;
+    WallRowsD bcb, bct;   // apply_bc closure rows for this field
+    double* partial;      // per-warp row sums [nwarps][n2] or null
+};
+
+struct FftPlan {
+    int n, nstages;
+    int radix[MAX_FFT_STAGES];
+    const double2* tw;    // tw[m] = exp(-2 pi i m / n)
+};
+
+struct Fields {
+    double *u, *v, *w, *c;
+};
+
+struct GhostArgs {
+    Fields F;
+    WallRowsD ub, ut, wb, wt;   // u-type and w-type closure rows
+    double bc_u, bc_v, bc_c_bot, bc_c_top, bc_w;
+};
+
+struct RhsArgs {
+    const double *u, *v, *w, *c;
+    double *fu, *fv, *fw, *fc;
+    double nu, kappa;              // nu and nu/prandtl
+    double betg_x, betg_y, betg_z;
+};
+
+struct MassArgs {
+    const double* avg;
+    const double* dz;
+    int order, nz, n2;
+    double kappa;
+    double green[4];      // statistics of the Green's function column
+    int mode;             // uvolavgmode / cvolavgmode
+    double target;        // want_uvolavg - uframe, or want_cvolavg
+    double fixed;         // -dpdx (u) or 0 (c) when mode != 1
+    double* m_out;        // device scalar: mdpdx / dcdt of this substep
+    long long* counter;   // device substep counter selecting the log row
+    double* log_base;     // log ring buffer [log_cap][LOG_COLS]
+    int log_cap;
+    int col;              // first column written: m, bottom gradient, top gradient, bulk, centreline
+    int advance;          // 1: increment the counter afterwards (last statistics of a substep)
+};
+
+struct DivArgs {
+    const double *u, *v, *w;
+    const double* gu;      // Green's function column of u (n2) or null
+    const double* mu;      // device scalar mdpdx or null
+    double2* spec;         // [n2][nkx][ny]
+    FftPlan px;
+    double c8;
+};
+
+struct FftyArgs {
+    double2* spec;
+    FftPlan py;
+    int sign;
+    int kfirst;
+    double c8;
+};
+
+struct C2rArgs {
+    const double2* spec;
+    double* p;
+    FftPlan px;
+    double c8;
+};
+
+struct PoissonArgs {
+    double2* spec;
+    double* scratch;          // width 3: 1 x [n2][ncol]; width 7: 3 x [n2][ncol]
+    const double *a, *b, *c, *e, *f, *g, *dpart, *dvol, *lamx, *lamy;
+    double red[2][6][7];
+    double dsub[2][6][3];
+    WallRowsD bot[2], top;
+    double dt, dxdx, dydy;
+};
+
+struct ProjArgs {
+    double *u, *v, *w, *c;
+    const double* p;
+    const double *gu, *gc;          // Green's function columns (n2) or null
+    const double *mu, *mc;          // device scalars mdpdx, dcdt or null
+    double dt;                      // (alpha + beta) dt of the substep
+};
+
+// ---------------------------------------------------------------- launchers
+void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st);
+void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st);
+void launch_solve(const Geo& G, const SolveArgs& A, bool is_w, bool shift, cudaStream_t st);
+void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st);
+void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st);
+void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st);
+void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st);
+void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st);
+void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st);
+cudaError_t fft_set_smem_limits(int max_n);
+size_t fft_smem_bytes(int n);
+constexpr int FFT_MAX_N = 512;
+
+}  // namespace cf

@@ -1,0 +1,828 @@
+// Host-side 1-D band construction; see host_band.h.  Every formula below
+// restates the reference closure or band row named beside it, keeping its
+// evaluation order (x86-64 builds without FMA contraction).
+#include "host_band.h"
+
+#include <cmath>
+#include <stdexcept>
+
+namespace cf {
+
+const double RK3_ALP[3] = {29.0 / 96.0, -3.0 / 40.0, 1.0 / 6.0};
+const double RK3_BET[3] = {37.0 / 160.0, 5.0 / 24.0, 1.0 / 6.0};
+const double RK3_GAM[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+const double RK3_ZET[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+Metrics make_metrics(int order, int nx, int ny, int nz, int gz, double lx, double ly, double lz)
+{
+    Metrics m;
+    m.order = order;
+    m.nx = nx;
+    m.ny = ny;
+    m.nz = nz;
+    m.gz = gz;
+    m.n2 = nz + 2 * gz;
+    m.lx = lx;
+    m.ly = ly;
+    m.lz = lz;
+    m.dx = lx / (double) nx;  // chanfast.c:141-142
+    m.dy = ly / (double) ny;
+    m.dz.assign(m.n2, 0.0);
+    for (int iz = 0; iz < nz; iz++)  // chanfast.c:184-189
+        m.dz[iz + gz] = lz * 0.5 * (std::cos(M_PI * (double) iz / (double) nz)
+                                    - std::cos(M_PI * (double) (iz + 1) / (double) nz));
+    for (int k = 0; k < gz; k++) m.dz[k] = m.dz[2 * gz - k - 1];  // ghost_even_z (ghost.c:31-54)
+    for (int k = m.n2 - gz; k < m.n2; k++) m.dz[k] = m.dz[2 * (m.n2 - gz) - k - 1];
+    return m;
+}
+
+// ---------------------------------------------------------------- closures
+// Cell-centred fields and pressure (diffuseu.c:617-940, pressure.c:446-770).
+
+static void u_stencil_bot2(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
+{
+    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+    if (t == BC_NEUMANN) { B.a[k] = 0.0; B.b[k] = -1.0 / dzp1h; B.c[k] = +1.0 / dzp1h; }
+    else { B.a[k] = 0.0; B.b[k] = 0.5; B.c[k] = 0.5; }
+    B.r[k] = bc;
+}
+
+static void u_stencil_top2(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
+{
+    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+    if (t == BC_NEUMANN) { B.a[k] = -1.0 / dzm1h; B.b[k] = +1.0 / dzm1h; B.c[k] = 0.0; }
+    else { B.a[k] = 0.5; B.b[k] = 0.5; B.c[k] = 0.0; }
+    B.r[k] = bc;
+}
+
+static void u_reduce_bot2(Band& B, int k)
+{
+    int kp1 = k + 1;
+    double fac = B.a[kp1] / B.b[k];
+    B.a[kp1] -= B.b[k] * fac;
+    B.b[kp1] -= B.c[k] * fac;
+    B.r[kp1] -= B.r[k] * fac;
+}
+
+static void u_reduce_top2(Band& B, int k)
+{
+    int km1 = k - 1;
+    double fac = B.c[km1] / B.b[k];
+    B.c[km1] -= B.b[k] * fac;
+    B.b[km1] -= B.a[k] * fac;
+    B.r[km1] -= B.r[k] * fac;
+}
+
+static void u_fill_bot2(Band& B, int k) { B.x[k] = (B.c[k] * B.x[k + 1] - B.r[k]) / -B.b[k]; }
+static void u_fill_top2(Band& B, int k) { B.x[k] = (B.a[k] * B.x[k - 1] - B.r[k]) / -B.b[k]; }
+
+static void u_stencil_bot4(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
+{
+    int km2 = k - 2, km1 = k - 1;
+    double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
+    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+    B.a[k] = 0.0;
+    B.b[k] = -A2 / dzm1h;
+    B.c[k] = -A1 / dzm1h - 2.0 * -A2 / dzp1h;
+    B.d[k] = +A1 / dzm1h - 2.0 * -A1 / dzp1h - A2 / dzp3h;
+    B.e[k] = +A2 / dzm1h - 2.0 * +A1 / dzp1h - A1 / dzp3h;
+    B.f[k] = -2.0 * +A2 / dzp1h + A1 / dzp3h;
+    B.g[k] = +A2 / dzp3h;
+    B.r[k] = 0.0;
+    B.a[km1] = 0.0; B.b[km1] = 0.0; B.c[km1] = 0.0;
+    if (t == BC_NEUMANN) {
+        B.d[km1] = -A2 / dzp1h; B.e[km1] = -A1 / dzp1h; B.f[km1] = +A1 / dzp1h; B.g[km1] = +A2 / dzp1h;
+    } else {
+        B.d[km1] = 0.5 * A2; B.e[km1] = 0.5 * (A1 + 2.0 * A2);
+        B.f[km1] = 0.5 * (A1 + 2.0 * A2); B.g[km1] = 0.5 * A2;
+    }
+    B.r[km1] = bc;
+    B.a[km2] = 0.0; B.b[km2] = 0.0; B.c[km2] = 0.0; B.d[km2] = 0.0; B.e[km2] = 0.0;
+    B.f[km2] = -1.0; B.g[km2] = +1.0; B.r[km2] = 0.0;
+}
+
+static void u_stencil_top4(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
+{
+    int kp2 = k + 2, kp1 = k + 1;
+    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+    double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
+    B.a[k] = -A2 / dzm3h;
+    B.b[k] = -A1 / dzm3h - 2.0 * -A2 / dzm1h;
+    B.c[k] = +A1 / dzm3h - 2.0 * -A1 / dzm1h - A2 / dzp1h;
+    B.d[k] = +A2 / dzm3h - 2.0 * +A1 / dzm1h - A1 / dzp1h;
+    B.e[k] = -2.0 * +A2 / dzm1h + A1 / dzp1h;
+    B.f[k] = +A2 / dzp1h;
+    B.g[k] = 0.0;
+    B.r[k] = 0.0;
+    if (t == BC_NEUMANN) {
+        B.a[kp1] = -A2 / dzm1h; B.b[kp1] = -A1 / dzm1h; B.c[kp1] = +A1 / dzm1h; B.d[kp1] = +A2 / dzm1h;
+    } else {
+        B.a[kp1] = 0.5 * A2; B.b[kp1] = 0.5 * (A1 + 2.0 * A2);
+        B.c[kp1] = 0.5 * (A1 + 2.0 * A2); B.d[kp1] = 0.5 * A2;
+    }
+    B.e[kp1] = 0.0; B.f[kp1] = 0.0; B.g[kp1] = 0.0; B.r[kp1] = bc;
+    B.a[kp2] = -1.0; B.b[kp2] = +1.0; B.c[kp2] = 0.0; B.d[kp2] = 0.0;
+    B.e[kp2] = 0.0; B.f[kp2] = 0.0; B.g[kp2] = 0.0; B.r[kp2] = 0.0;
+}
+
+// Bottom elimination of the ghost rows of a 7-band system (diffuseu.c:807-850).
+// `dsub` (optional) receives the three diagonal subtractions of rows k+1 and
+// the one of row k+2, in order, for the per-column diagonal of the pressure.
+static void u_reduce_bot4(Band& B, int k, double dsub[3][3])
+{
+    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
+    auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
+    auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
+    double fac, t;
+    fac = a[kp1] / b[k];
+    a[kp1] -= b[k] * fac; b[kp1] -= c[k] * fac; c[kp1] -= d[k] * fac;
+    t = e[k] * fac; d[kp1] -= t; if (dsub) dsub[0][0] = t;
+    e[kp1] -= f[k] * fac; f[kp1] -= g[k] * fac;
+    fac = b[kp1] / d[km1];
+    b[kp1] -= d[km1] * fac; c[kp1] -= e[km1] * fac;
+    t = f[km1] * fac; d[kp1] -= t; if (dsub) dsub[0][1] = t;
+    e[kp1] -= g[km1] * fac; r[kp1] -= r[km1] * fac;
+    fac = c[kp1] / f[km2];
+    c[kp1] -= f[km2] * fac;
+    t = g[km2] * fac; d[kp1] -= t; if (dsub) dsub[0][2] = t;
+    fac = a[kp2] / d[km1];
+    a[kp2] -= d[km1] * fac; b[kp2] -= e[km1] * fac; c[kp2] -= f[km1] * fac;
+    t = g[km1] * fac; d[kp2] -= t; if (dsub) dsub[1][0] = t;
+    r[kp2] -= r[km1] * fac;
+    fac = b[kp2] / f[km2];
+    b[kp2] -= f[km2] * fac; c[kp2] -= g[km2] * fac;
+    fac = a[kp3] / f[km2];
+    a[kp3] -= f[km2] * fac; b[kp3] -= g[km2] * fac;
+}
+
+// Top elimination (diffuseu.c:853-896); dsub rows: k-1 (three), k-2 (one).
+static void u_reduce_top4(Band& B, int k, double dsub[3][3])
+{
+    int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
+    auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
+    auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
+    double fac, t;
+    fac = g[km1] / f[k];
+    g[km1] -= f[k] * fac; f[km1] -= e[k] * fac; e[km1] -= d[k] * fac;
+    t = c[k] * fac; d[km1] -= t; if (dsub) dsub[0][0] = t;
+    c[km1] -= b[k] * fac; b[km1] -= a[k] * fac;
+    fac = f[km1] / d[kp1];
+    f[km1] -= d[kp1] * fac; e[km1] -= c[kp1] * fac;
+    t = b[kp1] * fac; d[km1] -= t; if (dsub) dsub[0][1] = t;
+    c[km1] -= a[kp1] * fac; r[km1] -= r[kp1] * fac;
+    fac = e[km1] / b[kp2];
+    e[km1] -= b[kp2] * fac;
+    t = a[kp2] * fac; d[km1] -= t; if (dsub) dsub[0][2] = t;
+    fac = g[km2] / d[kp1];
+    g[km2] -= d[kp1] * fac; f[km2] -= c[kp1] * fac; e[km2] -= b[kp1] * fac;
+    t = a[kp1] * fac; d[km2] -= t; if (dsub) dsub[1][0] = t;
+    r[km2] -= r[kp1] * fac;
+    fac = f[km2] / b[kp2];
+    f[km2] -= b[kp2] * fac; e[km2] -= a[kp2] * fac;
+    fac = g[km3] / b[kp2];
+    g[km3] -= b[kp2] * fac; f[km3] -= a[kp2] * fac;
+}
+
+static void u_fill_bot4(Band& B, int k)
+{
+    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
+    auto& x = B.x;
+    x[k] = (B.g[km2] * x[kp1]) / -B.f[km2];
+    x[km1] = (B.e[km1] * x[k] + B.f[km1] * x[kp1] + B.g[km1] * x[kp2] - B.r[km1]) / -B.d[km1];
+    x[km2] = (B.c[k] * x[km1] + B.d[k] * x[k] + B.e[k] * x[kp1] + B.f[k] * x[kp2]
+              + B.g[k] * x[kp3]) / -B.b[k];
+}
+
+static void u_fill_top4(Band& B, int k)
+{
+    int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
+    auto& x = B.x;
+    x[k] = (B.a[kp2] * x[km1]) / -B.b[kp2];
+    x[kp1] = (B.a[kp1] * x[km2] + B.b[kp1] * x[km1] + B.c[kp1] * x[k] - B.r[kp1]) / -B.d[kp1];
+    x[kp2] = (B.a[k] * x[km3] + B.b[k] * x[km2] + B.c[k] * x[km1] + B.d[k] * x[k]
+              + B.e[k] * x[kp1]) / -B.f[k];
+}
+
+// Face fields (diffusew.c:617-884); Dirichlet only.
+static void w_stencil2(Band& B, int k, double bc) { B.a[k] = 0.0; B.b[k] = 1.0; B.c[k] = 0.0; B.r[k] = bc; }
+
+static void w_reduce_bot2(Band& B, int k)
+{
+    int kp1 = k + 1;
+    double fac = B.a[kp1] / B.b[k];
+    B.a[kp1] -= B.b[k] * fac;
+    B.r[kp1] -= B.r[k] * fac;
+}
+
+static void w_reduce_top2(Band& B, int k)
+{
+    int km1 = k - 1;
+    double fac = B.c[km1] / B.b[k];
+    B.c[km1] -= B.b[k] * fac;
+    B.r[km1] -= B.r[k] * fac;
+}
+
+static void w_fill2(Band& B, int k) { B.x[k] = (-B.r[k]) / -B.b[k]; }
+
+static void w_stencil_bot4(Band& B, const std::vector<double>& dz, int k, double bc)
+{
+    int km2 = k - 2, km1 = k - 1;
+    double dzp0 = dz[k], dzp1 = dz[k + 1];
+    B.a[k] = 0.0;
+    B.b[k] = -A2 / dzp0;
+    B.c[k] = -A1 / dzp0 + A2 / dzp1;
+    B.d[k] = +A1 / dzp0 + A1 / dzp1;
+    B.e[k] = +A2 / dzp0 - A1 / dzp1;
+    B.f[k] = -A2 / dzp1;
+    B.g[k] = 0.0;
+    B.r[k] = 0.0;
+    B.a[km1] = 0.0; B.b[km1] = 0.0; B.c[km1] = 0.0; B.d[km1] = -1.0; B.e[km1] = +2.0;
+    B.f[km1] = -1.0; B.g[km1] = 0.0; B.r[km1] = 0.0;
+    B.a[km2] = 0.0; B.b[km2] = 0.0; B.c[km2] = 0.0; B.d[km2] = 0.0; B.e[km2] = 0.0;
+    B.f[km2] = 1.0; B.g[km2] = 0.0; B.r[km2] = bc;
+}
+
+static void w_stencil_top4(Band& B, const std::vector<double>& dz, int k, double bc)
+{
+    int kp2 = k + 2, kp1 = k + 1;
+    double dzp0 = dz[k], dzp1 = dz[k + 1];
+    B.a[k] = 0.0;
+    B.b[k] = -A2 / dzp0;
+    B.c[k] = -A1 / dzp0 + A2 / dzp1;
+    B.d[k] = +A1 / dzp0 + A1 / dzp1;
+    B.e[k] = +A2 / dzp0 - A1 / dzp1;
+    B.f[k] = -A2 / dzp1;
+    B.g[k] = 0.0;
+    B.r[k] = 0.0;
+    B.a[kp1] = 0.0; B.b[kp1] = -1.0; B.c[kp1] = +2.0; B.d[kp1] = -1.0;
+    B.e[kp1] = 0.0; B.f[kp1] = 0.0; B.g[kp1] = 0.0; B.r[kp1] = 0.0;
+    B.a[kp2] = 0.0; B.b[kp2] = 1.0; B.c[kp2] = 0.0; B.d[kp2] = 0.0;
+    B.e[kp2] = 0.0; B.f[kp2] = 0.0; B.g[kp2] = 0.0; B.r[kp2] = bc;
+}
+
+static void w_reduce_bot4(Band& B, int k)
+{
+    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
+    auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
+    auto& e = B.e; auto& f = B.f; auto& r = B.r;
+    double fac;
+    fac = a[kp1] / b[k];
+    a[kp1] -= b[k] * fac; b[kp1] -= c[k] * fac; c[kp1] -= d[k] * fac; d[kp1] -= e[k] * fac; e[kp1] -= f[k] * fac;
+    fac = b[kp1] / d[km1];
+    b[kp1] -= d[km1] * fac; c[kp1] -= e[km1] * fac; d[kp1] -= f[km1] * fac;
+    fac = c[kp1] / f[km2];
+    c[kp1] -= f[km2] * fac; r[kp1] -= r[km2] * fac;
+    fac = a[kp2] / d[km1];
+    a[kp2] -= d[km1] * fac; b[kp2] -= e[km1] * fac; c[kp2] -= f[km1] * fac;
+    fac = b[kp2] / f[km2];
+    b[kp2] -= f[km2] * fac; r[kp2] -= r[km2] * fac;
+    fac = a[kp3] / f[km2];
+    a[kp3] -= f[km2] * fac; r[kp3] -= r[km2] * fac;
+}
+
+static void w_reduce_top4(Band& B, int k)
+{
+    int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
+    auto& b = B.b; auto& c = B.c; auto& d = B.d;
+    auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
+    double fac;
+    fac = g[km1] / f[k];
+    g[km1] -= f[k] * fac; f[km1] -= e[k] * fac; e[km1] -= d[k] * fac; d[km1] -= c[k] * fac; c[km1] -= b[k] * fac;
+    fac = f[km1] / d[kp1];
+    f[km1] -= d[kp1] * fac; e[km1] -= c[kp1] * fac; d[km1] -= b[kp1] * fac;
+    fac = e[km1] / b[kp2];
+    e[km1] -= b[kp2] * fac; r[km1] -= r[kp2] * fac;
+    fac = g[km2] / d[kp1];
+    g[km2] -= d[kp1] * fac; f[km2] -= c[kp1] * fac; e[km2] -= b[kp1] * fac;
+    fac = f[km2] / b[kp2];
+    f[km2] -= b[kp2] * fac; r[km2] -= r[kp2] * fac;
+    fac = g[km3] / b[kp2];
+    g[km3] -= b[kp2] * fac; r[km3] -= r[kp2] * fac;
+}
+
+static void w_fill_bot4(Band& B, int k)
+{
+    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
+    auto& x = B.x;
+    x[k] = (-B.r[km2]) / -B.f[km2];
+    x[km1] = (B.e[km1] * x[k] + B.f[km1] * x[kp1]) / -B.d[km1];
+    x[km2] = (B.c[k] * x[km1] + B.d[k] * x[k] + B.e[k] * x[kp1] + B.f[k] * x[kp2]) / -B.b[k];
+}
+
+static void w_fill_top4(Band& B, int k)
+{
+    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
+    auto& x = B.x;
+    x[k] = (-B.r[kp2]) / -B.b[kp2];
+    x[kp1] = (B.b[kp1] * x[km1] + B.c[kp1] * x[k]) / -B.d[kp1];
+    x[kp2] = (B.b[k] * x[km2] + B.c[k] * x[km1] + B.d[k] * x[k] + B.e[k] * x[kp1]) / -B.f[k];
+}
+
+static WallRows rows_of(const Band& B, int k0, int step)
+{
+    WallRows w;
+    for (int q = 0; q < 3; q++) {
+        int k = k0 + q * step;
+        const double* src[7] = {&B.a[k], &B.b[k], &B.c[k], &B.d[k], &B.e[k], &B.f[k], &B.g[k]};
+        for (int t = 0; t < 7; t++) w.row[q][t] = *src[t];
+    }
+    return w;
+}
+
+WallRows bc_rows_u(const Metrics& m, bool bottom)
+{
+    Band B(m.n2);
+    int kb = m.gz - 1, kt = m.n2 - m.gz;
+    if (m.order == 2) {
+        if (bottom) { u_stencil_bot2(B, m.dz, kb, 0.0, BC_DIRICHLET); return rows_of(B, kb, -1); }
+        u_stencil_top2(B, m.dz, kt, 0.0, BC_DIRICHLET);
+        return rows_of(B, kt, +1);
+    }
+    if (bottom) { u_stencil_bot4(B, m.dz, kb, 0.0, BC_DIRICHLET); return rows_of(B, kb, -1); }
+    u_stencil_top4(B, m.dz, kt, 0.0, BC_DIRICHLET);
+    return rows_of(B, kt, +1);
+}
+
+WallRows bc_rows_w(const Metrics& m, bool bottom)
+{
+    Band B(m.n2);
+    int kb = m.gz - 1, kt = m.n2 - m.gz - 1;
+    if (m.order == 2) {
+        w_stencil2(B, bottom ? kb : kt, 0.0);
+        return rows_of(B, bottom ? kb : kt, bottom ? -1 : +1);
+    }
+    if (bottom) { w_stencil_bot4(B, m.dz, kb, 0.0); return rows_of(B, kb, -1); }
+    w_stencil_top4(B, m.dz, kt, 0.0);
+    return rows_of(B, kt, +1);
+}
+
+void apply_bc_u_col(const Metrics& m, std::vector<double>& x, double bc_bot, double bc_top)
+{
+    // apply_bc_u2 / apply_bc_u4 (diffuseu.c:37-104)
+    Band B(m.n2);
+    B.x = x;
+    int kb = m.gz - 1, kt = m.n2 - m.gz;
+    if (m.order == 2) {
+        u_stencil_bot2(B, m.dz, kb, bc_bot, BC_DIRICHLET);
+        u_stencil_top2(B, m.dz, kt, bc_top, BC_DIRICHLET);
+        u_fill_bot2(B, kb);
+        u_fill_top2(B, kt);
+    } else {
+        u_stencil_bot4(B, m.dz, kb, bc_bot, BC_DIRICHLET);
+        u_stencil_top4(B, m.dz, kt, bc_top, BC_DIRICHLET);
+        u_fill_bot4(B, kb);
+        u_fill_top4(B, kt);
+    }
+    x = B.x;
+}
+
+void apply_bc_w_col(const Metrics& m, std::vector<double>& x, double bc_bot, double bc_top)
+{
+    // apply_bc_w2 / apply_bc_w4 (diffusew.c:37-104)
+    Band B(m.n2);
+    B.x = x;
+    int kb = m.gz - 1, kt = m.n2 - m.gz - 1;
+    if (m.order == 2) {
+        w_stencil2(B, kb, bc_bot);
+        w_stencil2(B, kt, bc_top);
+        w_fill2(B, kb);
+        w_fill2(B, kt);
+    } else {
+        w_stencil_bot4(B, m.dz, kb, bc_bot);
+        w_stencil_top4(B, m.dz, kt, bc_top);
+        w_fill_bot4(B, kb);
+        w_fill_top4(B, kt);
+    }
+    x = B.x;
+}
+
+void helmholtz_u_col(const Metrics& m, const std::vector<double>& u, std::vector<double>& h, double nudt)
+{
+    const auto& dz = m.dz;
+    for (int k = m.gz; k < m.n2 - m.gz; k++) {
+        if (m.order == 2) {  // diffuseu.c:121-131
+            double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+            double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+            h[k] = u[k] + nudt * (((u[k + 1] - u[k]) / dzp1h - (u[k] - u[k - 1]) / dzm1h) / dz[k]);
+        } else {  // diffuseu.c:149-169
+            double wp3h = A1 * (u[k + 2] - u[k + 1]) + A2 * (u[k + 3] - u[k]);
+            double wp1h = A1 * (u[k + 1] - u[k]) + A2 * (u[k + 2] - u[k - 1]);
+            double wm1h = A1 * (u[k] - u[k - 1]) + A2 * (u[k + 1] - u[k - 2]);
+            double wm3h = A1 * (u[k - 1] - u[k - 2]) + A2 * (u[k] - u[k - 3]);
+            double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
+            double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+            double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+            double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
+            h[k] = u[k] + nudt * ((A1 * (wp1h / dzp1h - wm1h / dzm1h) + A2 * (wp3h / dzp3h - wm3h / dzm3h)) / dz[k]);
+        }
+    }
+}
+
+void helmholtz_w_col(const Metrics& m, const std::vector<double>& w, std::vector<double>& h, double nudt)
+{
+    const auto& dz = m.dz;
+    for (int k = m.gz; k < m.n2 - m.gz - 1; k++) {
+        double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+        if (m.order == 2) {  // diffusew.c:121-132
+            double dzp1 = dz[k + 1], dzm0 = dz[k];
+            h[k] = w[k] + nudt * (((w[k + 1] - w[k]) / dzp1 - (w[k] - w[k - 1]) / dzm0) / dzp1h);
+        } else {  // diffusew.c:150-171
+            double wp3h = A1 * (w[k + 2] - w[k + 1]) + A2 * (w[k + 3] - w[k]);
+            double wp1h = A1 * (w[k + 1] - w[k]) + A2 * (w[k + 2] - w[k - 1]);
+            double wm1h = A1 * (w[k] - w[k - 1]) + A2 * (w[k + 1] - w[k - 2]);
+            double wm3h = A1 * (w[k - 1] - w[k - 2]) + A2 * (w[k] - w[k - 3]);
+            double dzp2 = dz[k + 2], dzp1 = dz[k + 1], dzm0 = dz[k], dzm1 = dz[k - 1];
+            h[k] = w[k] + nudt * ((A1 * (wp1h / dzp1 - wm1h / dzm0) + A2 * (wp3h / dzp2 - wm3h / dzm1)) / dzp1h);
+        }
+    }
+}
+
+// ------------------------------------------------------- factorisation
+
+static LineFactor factor_band(const Band& B, int k0, int n, int width)
+{
+    LineFactor L;
+    L.k0 = k0;
+    L.n = n;
+    L.width = width;
+    L.F1.assign(n, 0.0); L.F2.assign(n, 0.0); L.F3.assign(n, 0.0); L.DEN.assign(n, 0.0);
+    L.P.assign(n, 0.0); L.Q.assign(n, 0.0); L.R.assign(n, 0.0);
+    auto A = [&](int i) { return B.a[k0 + i]; };
+    auto Bb = [&](int i) { return B.b[k0 + i]; };
+    auto C = [&](int i) { return B.c[k0 + i]; };
+    if (width == 3) {  // tridag.c:4-26
+        double bet = Bb(0);
+        if (bet == 0.0) throw std::runtime_error("zero pivot");
+        L.DEN[0] = bet;
+        std::vector<double> gam(n, 0.0);
+        for (int j = 1; j < n; j++) {
+            gam[j] = C(j - 1) / bet;
+            bet = Bb(j) - A(j) * gam[j];
+            if (bet == 0.0) throw std::runtime_error("zero pivot");
+            L.F1[j] = A(j);
+            L.DEN[j] = bet;
+        }
+        for (int j = 0; j < n - 1; j++) L.P[j] = gam[j + 1];
+        return L;
+    }
+    // heptdag.c:5-61
+    auto D = [&](int i) { return B.d[k0 + i]; };
+    auto E = [&](int i) { return B.e[k0 + i]; };
+    auto F = [&](int i) { return B.f[k0 + i]; };
+    auto G = [&](int i) { return B.g[k0 + i]; };
+    std::vector<double> p(n), q(n), r(n);
+    double den, alp, bet;
+    den = D(0);
+    if (den == 0.0) throw std::runtime_error("zero pivot");
+    p[0] = E(0) / den; q[0] = F(0) / den; r[0] = G(0) / den;
+    L.DEN[0] = den;
+    den = D(1) - C(1) * p[0];
+    if (den == 0.0) throw std::runtime_error("zero pivot");
+    p[1] = (E(1) - C(1) * q[0]) / den; q[1] = (F(1) - C(1) * r[0]) / den; r[1] = (G(1)) / den;
+    L.F1[1] = C(1); L.DEN[1] = den;
+    bet = C(2) - Bb(2) * p[0];
+    den = D(2) - Bb(2) * q[0] - bet * p[1];
+    if (den == 0.0) throw std::runtime_error("zero pivot");
+    p[2] = (E(2) - Bb(2) * r[0] - bet * q[1]) / den; q[2] = (F(2) - bet * r[1]) / den; r[2] = (G(2)) / den;
+    L.F2[2] = Bb(2); L.F1[2] = bet; L.DEN[2] = den;
+    for (int i = 3; i < n; i++) {
+        alp = Bb(i) - A(i) * p[i - 3];
+        bet = C(i) - A(i) * q[i - 3] - alp * p[i - 2];
+        den = D(i) - A(i) * r[i - 3] - alp * q[i - 2] - bet * p[i - 1];
+        if (den == 0.0) throw std::runtime_error("zero pivot");
+        p[i] = (E(i) - alp * r[i - 2] - bet * q[i - 1]) / den;
+        q[i] = (F(i) - bet * r[i - 1]) / den;
+        r[i] = (G(i)) / den;
+        L.F3[i] = A(i); L.F2[i] = alp; L.F1[i] = bet; L.DEN[i] = den;
+    }
+    // Back substitution uses p, q, r of rows < n-1 (x[n-1] = s[n-1]).
+    for (int i = 0; i < n - 1; i++) L.P[i] = p[i];
+    for (int i = 0; i < n - 2; i++) L.Q[i] = q[i];
+    for (int i = 0; i < n - 3; i++) L.R[i] = r[i];
+    return L;
+}
+
+static void apply_factor(const LineFactor& L, const double* rhs, double* x)
+{
+    std::vector<double> s(L.n + 3, 0.0);
+    double* sp = s.data() + 3;
+    for (int i = 0; i < L.n; i++)
+        sp[i] = (((rhs[i] - L.F3[i] * sp[i - 3]) - L.F2[i] * sp[i - 2]) - L.F1[i] * sp[i - 1]) / L.DEN[i];
+    std::vector<double> y(L.n + 3, 0.0);
+    for (int i = L.n - 1; i >= 0; i--)
+        y[i] = ((sp[i] - L.P[i] * y[i + 1]) - L.Q[i] * y[i + 2]) - L.R[i] * y[i + 3];
+    for (int i = 0; i < L.n; i++) x[i] = y[i];
+}
+
+// Interior band rows of solve_helmholtz1d_u{2,4} (diffuseu.c:190-201, 239-268).
+static void band_rows_u(const Metrics& m, Band& B, double nudt)
+{
+    const auto& dz = m.dz;
+    for (int k = m.gz; k < m.n2 - m.gz; k++) {
+        double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+        double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+        double dvol = dz[k];
+        if (m.order == 2) {
+            B.a[k] = +dvol * nudt / (dzm1h * dz[k]);
+            B.c[k] = +dvol * nudt / (dzp1h * dz[k]);
+            B.b[k] = -dvol * nudt / (dzm1h * dz[k]) - dvol * nudt / (dzp1h * dz[k]) + dvol;
+        } else {
+            double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
+            double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
+            B.a[k] = +A2 * A2 * dvol * nudt / (dzm3h * dz[k]);
+            B.g[k] = +A2 * A2 * dvol * nudt / (dzp3h * dz[k]);
+            B.b[k] = +A1 * A2 * dvol * nudt / (dzm1h * dz[k]) + A1 * A2 * dvol * nudt / (dzm3h * dz[k]);
+            B.f[k] = +A1 * A2 * dvol * nudt / (dzp1h * dz[k]) + A1 * A2 * dvol * nudt / (dzp3h * dz[k]);
+            B.c[k] = -A1 * A2 * dvol * nudt / (dzp1h * dz[k]) - A1 * A2 * dvol * nudt / (dzm3h * dz[k])
+                     + A1 * A1 * dvol * nudt / (dzm1h * dz[k]);
+            B.e[k] = -A1 * A2 * dvol * nudt / (dzm1h * dz[k]) - A1 * A2 * dvol * nudt / (dzp3h * dz[k])
+                     + A1 * A1 * dvol * nudt / (dzp1h * dz[k]);
+            B.d[k] = -A2 * A2 * dvol * nudt / (dzm3h * dz[k]) - A2 * A2 * dvol * nudt / (dzp3h * dz[k])
+                     - A1 * A1 * dvol * nudt / (dzm1h * dz[k]) - A1 * A1 * dvol * nudt / (dzp1h * dz[k])
+                     + dvol;
+        }
+    }
+}
+
+// Interior band rows of solve_helmholtz1d_w{2,4} (diffusew.c:192-205, 242-272).
+static void band_rows_w(const Metrics& m, Band& B, double nudt)
+{
+    const auto& dz = m.dz;
+    for (int k = m.gz; k < m.n2 - m.gz - 1; k++) {
+        double dzp1 = dz[k + 1], dzm0 = dz[k];
+        double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+        double dvol = dzp1h;
+        if (m.order == 2) {
+            B.a[k] = +dvol * nudt / (dzm0 * dzp1h);
+            B.c[k] = +dvol * nudt / (dzp1 * dzp1h);
+            B.b[k] = -dvol * nudt / (dzm0 * dzp1h) - dvol * nudt / (dzp1 * dzp1h) + dvol;
+        } else {
+            double dzp2 = dz[k + 2], dzm1 = dz[k - 1];
+            B.a[k] = +A2 * A2 * dvol * nudt / (dzm1 * dzp1h);
+            B.g[k] = +A2 * A2 * dvol * nudt / (dzp2 * dzp1h);
+            B.b[k] = +A1 * A2 * dvol * nudt / (dzm0 * dzp1h) + A1 * A2 * dvol * nudt / (dzm1 * dzp1h);
+            B.f[k] = +A1 * A2 * dvol * nudt / (dzp1 * dzp1h) + A1 * A2 * dvol * nudt / (dzp2 * dzp1h);
+            B.c[k] = -A1 * A2 * dvol * nudt / (dzp1 * dzp1h) - A1 * A2 * dvol * nudt / (dzm1 * dzp1h)
+                     + A1 * A1 * dvol * nudt / (dzm0 * dzp1h);
+            B.e[k] = -A1 * A2 * dvol * nudt / (dzm0 * dzp1h) - A1 * A2 * dvol * nudt / (dzp2 * dzp1h)
+                     + A1 * A1 * dvol * nudt / (dzp1 * dzp1h);
+            B.d[k] = -A2 * A2 * dvol * nudt / (dzm1 * dzp1h) - A2 * A2 * dvol * nudt / (dzp2 * dzp1h)
+                     - A1 * A1 * dvol * nudt / (dzm0 * dzp1h) - A1 * A1 * dvol * nudt / (dzp1 * dzp1h)
+                     + dvol;
+        }
+    }
+}
+
+double z_average(const Metrics& m, const double* avg)
+{
+    // get_z_avg (get.c:490-502)
+    double a = 0.0, l = 0.0;
+    for (int k = m.gz; k < m.nz + m.gz; k++) {
+        a += avg[k] * m.dz[k];
+        l += m.dz[k];
+    }
+    return a / l;
+}
+
+void profile_stats(const Metrics& m, const double* avg, double kappa, double out[4])
+{
+    // chanfast.c:487-496 (order 2) / 1411-1420 (order 4)
+    int g = m.gz, n2 = m.n2, nz = m.nz;
+    const auto& dz = m.dz;
+    out[0] = z_average(m, avg);
+    if (m.order == 4) {
+        out[1] = kappa * (A1 * (avg[g] - avg[g - 1]) + A2 * (avg[g + 1] - avg[g - 2])) / (0.5 * (dz[g] + dz[g - 1]));
+        out[2] = kappa * (A1 * (avg[n2 - g] - avg[n2 - g - 1]) + A2 * (avg[n2 - g + 1] - avg[n2 - g - 2]))
+                 / (0.5 * (dz[n2 - g] + dz[n2 - g - 1]));
+    } else {
+        out[1] = kappa * (avg[g] - avg[g - 1]) / (0.5 * (dz[g] + dz[g - 1]));
+        out[2] = kappa * (avg[n2 - g] - avg[n2 - g - 1]) / (0.5 * (dz[n2 - g] + dz[n2 - g - 1]));
+    }
+    out[3] = nz % 2 == 0 ? 0.5 * (avg[g + nz / 2 - 1] + avg[g + nz / 2]) : avg[g + nz / 2];
+}
+
+ImplicitSet make_implicit_u(const Metrics& m, double nubdt, double gamdt, double bc_bot,
+                            double bc_top, double kappa, bool want_green)
+{
+    ImplicitSet S;
+    int kb = m.gz - 1, kt = m.n2 - m.gz;
+    Band B(m.n2);
+    band_rows_u(m, B, -nubdt);
+    if (m.order == 2) {
+        u_stencil_bot2(B, m.dz, kb, 0.0, BC_DIRICHLET);
+        u_stencil_top2(B, m.dz, kt, 0.0, BC_DIRICHLET);
+        S.bot = rows_of(B, kb, -1);
+        S.top = rows_of(B, kt, +1);
+        u_reduce_bot2(B, kb);
+        u_reduce_top2(B, kt);
+        S.fac = factor_band(B, m.gz, m.nz, 3);
+    } else {
+        u_stencil_bot4(B, m.dz, kb, 0.0, BC_DIRICHLET);
+        u_stencil_top4(B, m.dz, kt, 0.0, BC_DIRICHLET);
+        S.bot = rows_of(B, kb, -1);
+        S.top = rows_of(B, kt, +1);
+        u_reduce_bot4(B, kb, nullptr);
+        u_reduce_top4(B, kt, nullptr);
+        S.fac = factor_band(B, m.gz, m.nz, 7);
+    }
+    // Boundary lifting (chanfast.c:473-477): bc := 0, apply_bc(bc), hbc = H(-nubdt) bc.
+    std::vector<double> bc(m.n2, 0.0), hbc(m.n2, 0.0);
+    apply_bc_u_col(m, bc, bc_bot, bc_top);
+    helmholtz_u_col(m, bc, hbc, -nubdt);
+    S.hbc = hbc;
+    if (want_green) {
+        std::vector<double> h(m.n2, gamdt), out(m.n2, 0.0);
+        solve_column(S, m, false, h, out);
+        S.green = out;
+        profile_stats(m, out.data(), kappa, S.green_stats);
+    }
+    return S;
+}
+
+ImplicitSet make_implicit_w(const Metrics& m, double nubdt, double bc_bot, double bc_top)
+{
+    ImplicitSet S;
+    int kb = m.gz - 1, kt = m.n2 - m.gz - 1;
+    Band B(m.n2);
+    band_rows_w(m, B, -nubdt);
+    if (m.order == 2) {
+        w_stencil2(B, kb, 0.0);
+        w_stencil2(B, kt, 0.0);
+        S.bot = rows_of(B, kb, -1);
+        S.top = rows_of(B, kt, +1);
+        w_reduce_bot2(B, kb);
+        w_reduce_top2(B, kt);
+        S.fac = factor_band(B, m.gz, m.nz - 1, 3);
+    } else {
+        w_stencil_bot4(B, m.dz, kb, 0.0);
+        w_stencil_top4(B, m.dz, kt, 0.0);
+        S.bot = rows_of(B, kb, -1);
+        S.top = rows_of(B, kt, +1);
+        w_reduce_bot4(B, kb);
+        w_reduce_top4(B, kt);
+        S.fac = factor_band(B, m.gz, m.nz - 1, 7);
+    }
+    std::vector<double> bc(m.n2, 0.0), hbc(m.n2, 0.0);
+    apply_bc_w_col(m, bc, bc_bot, bc_top);
+    helmholtz_w_col(m, bc, hbc, -nubdt);
+    S.hbc = hbc;
+    return S;
+}
+
+void solve_column(const ImplicitSet& s, const Metrics& m, bool is_w, std::vector<double>& h,
+                  std::vector<double>& out)
+{
+    // r = h * dvol (diffuseu.c:200, diffusew.c:204); the ghost rows carry
+    // bc = 0 so the elimination leaves r unchanged.
+    int k0 = s.fac.k0, n = s.fac.n;
+    std::vector<double> r(n);
+    for (int i = 0; i < n; i++) {
+        int k = k0 + i;
+        double dvol = is_w ? 0.5 * (m.dz[k + 1] + m.dz[k]) : m.dz[k];
+        r[i] = h[k] * dvol;
+    }
+    Band B(m.n2);
+    apply_factor(s.fac, r.data(), &B.x[k0]);
+    // ghost fill with the solve's closure rows (bc = 0)
+    auto put = [&](const WallRows& w, int k, int step) {
+        for (int q = 0; q < 3; q++) {
+            int kk = k + q * step;
+            B.a[kk] = w.row[q][0]; B.b[kk] = w.row[q][1]; B.c[kk] = w.row[q][2]; B.d[kk] = w.row[q][3];
+            B.e[kk] = w.row[q][4]; B.f[kk] = w.row[q][5]; B.g[kk] = w.row[q][6]; B.r[kk] = 0.0;
+        }
+    };
+    int kb = m.gz - 1, kt = is_w ? m.n2 - m.gz - 1 : m.n2 - m.gz;
+    if (m.order == 2) {
+        put(s.bot, kb, -1);
+        put(s.top, kt, +1);
+        if (is_w) { w_fill2(B, kb); w_fill2(B, kt); }
+        else { u_fill_bot2(B, kb); u_fill_top2(B, kt); }
+    } else {
+        put(s.bot, kb, -1);
+        put(s.top, kt, +1);
+        if (is_w) { w_fill_bot4(B, kb); w_fill_top4(B, kt); }
+        else { u_fill_bot4(B, kb); u_fill_top4(B, kt); }
+    }
+    out = B.x;
+}
+
+PoissonSet make_poisson(const Metrics& m, double dt)
+{
+    PoissonSet P;
+    P.width = m.order == 2 ? 3 : 7;
+    const auto& dz = m.dz;
+    double dx = m.dx, dy = m.dy;
+    int n2 = m.n2, g = m.gz, nz = m.nz;
+    P.dpart.assign(n2, 0.0);
+    P.dvol.assign(n2, 0.0);
+    Band B(n2);
+    for (int k = g; k < n2 - g; k++) {  // pressure.c:317-330 / 391-418
+        double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+        double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+        double dvol = dx * dy * dz[k];
+        P.dvol[k] = dvol;
+        if (m.order == 2) {
+            B.a[k] = +dvol * dt / (dzm1h * dz[k]);
+            B.c[k] = +dvol * dt / (dzp1h * dz[k]);
+            P.dpart[k] = -dvol * dt / (dzm1h * dz[k]) - dvol * dt / (dzp1h * dz[k]);
+        } else {
+            double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
+            double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
+            B.a[k] = +A2 * A2 * dvol * dt / (dzm3h * dz[k]);
+            B.g[k] = +A2 * A2 * dvol * dt / (dzp3h * dz[k]);
+            B.b[k] = +A1 * A2 * dvol * dt / (dzm1h * dz[k]) + A1 * A2 * dvol * dt / (dzm3h * dz[k]);
+            B.f[k] = +A1 * A2 * dvol * dt / (dzp1h * dz[k]) + A1 * A2 * dvol * dt / (dzp3h * dz[k]);
+            B.c[k] = -A1 * A2 * dvol * dt / (dzp1h * dz[k]) - A1 * A2 * dvol * dt / (dzm3h * dz[k])
+                     + A1 * A1 * dvol * dt / (dzm1h * dz[k]);
+            B.e[k] = -A1 * A2 * dvol * dt / (dzm1h * dz[k]) - A1 * A2 * dvol * dt / (dzp3h * dz[k])
+                     + A1 * A1 * dvol * dt / (dzp1h * dz[k]);
+            P.dpart[k] = -A2 * A2 * dvol * dt / (dzm3h * dz[k]) - A2 * A2 * dvol * dt / (dzp3h * dz[k])
+                         - A1 * A1 * dvol * dt / (dzm1h * dz[k]) - A1 * A1 * dvol * dt / (dzp1h * dz[k]);
+        }
+    }
+    int kb = g - 1, kt = n2 - g;
+    for (int v = 0; v < 2; v++) {
+        Band V = B;  // diagonal handled separately: keep d = 0 here
+        for (int k = g; k < n2 - g; k++) { if (m.order == 2) V.b[k] = 0.0; else V.d[k] = 0.0; }
+        BcKind bk = v == 1 ? BC_DIRICHLET : BC_NEUMANN;  // pressure.c:331-338
+        double ds_b[3][3] = {{0}}, ds_t[3][3] = {{0}};
+        if (m.order == 2) {
+            u_stencil_bot2(V, dz, kb, 0.0, bk);
+            u_stencil_top2(V, dz, kt, 0.0, BC_NEUMANN);
+            P.bot[v] = rows_of(V, kb, -1);
+            if (v == 0) P.top = rows_of(V, kt, +1);
+            // reduce_bot2: the diagonal of row kb+1 loses c[kb]*fac
+            double fac = V.a[kb + 1] / V.b[kb];
+            V.a[kb + 1] -= V.b[kb] * fac;
+            ds_b[0][0] = V.c[kb] * fac;
+            double fact = V.c[kt - 1] / V.b[kt];
+            V.c[kt - 1] -= V.b[kt] * fact;
+            ds_t[0][0] = V.a[kt] * fact;
+        } else {
+            u_stencil_bot4(V, dz, kb, 0.0, bk);
+            u_stencil_top4(V, dz, kt, 0.0, BC_NEUMANN);
+            P.bot[v] = rows_of(V, kb, -1);
+            if (v == 0) P.top = rows_of(V, kt, +1);
+            u_reduce_bot4(V, kb, ds_b);
+            u_reduce_top4(V, kt, ds_t);
+        }
+        int rows[6] = {g, g + 1, g + 2, n2 - g - 3, n2 - g - 2, n2 - g - 1};
+        for (int q = 0; q < 6; q++) {
+            int k = rows[q];
+            const double vals[7] = {V.a[k], V.b[k], V.c[k], V.d[k], V.e[k], V.f[k], V.g[k]};
+            for (int t = 0; t < 7; t++) P.red[v][q][t] = vals[t];
+            for (int t = 0; t < 3; t++) P.dsub[v][q][t] = 0.0;
+        }
+        // bottom: rows g (q=0) three subtractions, g+1 (q=1) one; top: n2-g-1 (q=5) three, n2-g-2 (q=4) one
+        for (int t = 0; t < 3; t++) P.dsub[v][0][t] = ds_b[0][t];
+        P.dsub[v][1][0] = ds_b[1][0];
+        for (int t = 0; t < 3; t++) P.dsub[v][5][t] = ds_t[0][t];
+        P.dsub[v][4][0] = ds_t[1][0];
+        if (v == 0) {
+            P.a.assign(n2, 0.0); P.b.assign(n2, 0.0); P.c.assign(n2, 0.0);
+            P.e.assign(n2, 0.0); P.f.assign(n2, 0.0); P.g.assign(n2, 0.0);
+            for (int k = g; k < n2 - g; k++) {
+                P.a[k] = V.a[k]; P.b[k] = V.b[k]; P.c[k] = V.c[k];
+                P.e[k] = V.e[k]; P.f[k] = V.f[k]; P.g[k] = V.g[k];
+            }
+        }
+    }
+    (void) nz;
+    auto lam = [&](int n, int i) {
+        double c1 = std::cos(2.0 * M_PI * 1.0 * (double) i / (double) n);
+        if (m.order == 2) return 2.0 - 2.0 * c1;
+        double c2 = std::cos(2.0 * M_PI * 2.0 * (double) i / (double) n);
+        double c3 = std::cos(2.0 * M_PI * 3.0 * (double) i / (double) n);
+        return (2.0 * A2 * A2 + 2.0 * A1 * A1) + (4.0 * A1 * A2 - 2.0 * A1 * A1) * c1
+               + (-4.0 * A1 * A2) * c2 + (-2.0 * A2 * A2) * c3;
+    };
+    P.lamx.resize(m.nx / 2 + 1);
+    for (int i = 0; i <= m.nx / 2; i++) P.lamx[i] = lam(m.nx, i);
+    P.lamy.resize(m.ny);
+    for (int j = 0; j < m.ny; j++) P.lamy[j] = lam(m.ny, j);
+    return P;
+}
+
+std::vector<double> z_at_p(const Metrics& m)
+{
+    std::vector<double> z(m.n2);
+    z[0] = 0.5 * m.dz[0];
+    for (int k = 1; k < m.n2; k++) z[k] = z[k - 1] + 0.5 * (m.dz[k - 1] + m.dz[k]);
+    double z0 = 0.5 * (z[m.gz - 1] + z[m.gz]);
+    for (int k = 0; k < m.n2; k++) z[k] -= z0;
+    return z;
+}
+
+std::vector<double> z_at_w(const Metrics& m)
+{
+    std::vector<double> z(m.n2);
+    z[0] = m.dz[0];
+    for (int k = 1; k < m.n2; k++) z[k] = z[k - 1] + m.dz[k];
+    double z0 = z[m.gz - 1];
+    for (int k = 0; k < m.n2; k++) z[k] -= z0;
+    return z;
+}
+
+}  // namespace cf

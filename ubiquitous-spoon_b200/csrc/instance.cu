@@ -1,0 +1,850 @@
+// Instance management and the C ABI of libchanfast_cuda.so.
+//
+// One cf_instance = one channel-flow state resident in device memory plus
+// the per-substep coefficient sets.  cf_step issues, per RK3 substep, the
+// kernel sequence that replaces the body of chanfast.c:395-656 (order 2) /
+// 1319-1580 (order 4):
+//   ghosts -> rhs -> solve u -> mass control u -> solve v -> solve c ->
+//   scalar-mean control c -> solve w -> divergence+x FFT -> y FFT ->
+//   Poisson -> inverse y FFT -> inverse x FFT -> projection
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "chanfast_cuda.h"
+#include "engine.cuh"
+#include "host_band.h"
+
+using namespace cf;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CF_CUDA(call)                                                                 \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+            return e_ == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA;            \
+        }                                                                             \
+    } while (0)
+
+// ------------------------------------------------------------ utility kernels
+
+constexpr unsigned long long GOLDEN = 0x9E3779B97F4A7C15ull;
+
+__device__ __forceinline__ double uniform_pm1(unsigned long long key, unsigned long long idx)
+{
+    // SplitMix64 output function of (key | idx); xi in [-1, 1)
+    unsigned long long z = (key | idx) + GOLDEN;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    double m = (double) (z >> 11);
+    return m * 0x1p-53 * 2.0 - 1.0;
+}
+
+__global__ void k_init_raw(Geo G, double* u, double* v, double* w, double* c, const double* zp,
+                           unsigned long long seed, double amp, double c_amp)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    const int k = blockIdx.z;
+    if (j >= G.ny) return;
+    const long long d = ((long long) k * G.nx + i) * G.ny + j;
+    const int iz = k - GZ;
+    if (iz < 0 || iz >= G.nz) {
+        u[d] = 0.0; v[d] = 0.0; w[d] = 0.0; c[d] = 0.0;
+        return;
+    }
+    const unsigned long long gidx = ((unsigned long long) i * G.ny + j) * G.nz + iz;
+    const double ucl = 1.5;
+    const double z = zp[k];
+    double xu = uniform_pm1((seed * 4 + 0) << 40, gidx);
+    double xv = uniform_pm1((seed * 4 + 1) << 40, gidx);
+    double xw = uniform_pm1((seed * 4 + 2) << 40, gidx);
+    double xc = uniform_pm1((seed * 4 + 3) << 40, gidx);
+    u[d] = 1.5 * (1.0 - (z - 1.0) * (z - 1.0)) + amp * ucl * xu;
+    v[d] = amp * ucl * xv;
+    w[d] = iz == G.nz - 1 ? 0.0 : amp * ucl * xw;   // face n2-gz-1 is the top wall
+    c[d] = -0.5 + z / 2.0 + c_amp * xc;
+}
+
+// Host layout [A][B][K] (A = nx + 2 ox, B = ny + 2 oy, K rows starting at
+// device row oz)  <->  device layout [n2][nx][ny].
+__global__ void k_host2dev(Geo G, const double* __restrict__ src, double* __restrict__ dst,
+                           int B, int K, int ox, int oy, int oz)
+{
+    __shared__ double tile[32][33];
+    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 32, i = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int jj = ty; jj < 32; jj += 8) {
+        int j = j0 + jj, kk = k0 + tx;
+        if (j < G.ny && kk < K) tile[jj][tx] = src[((long long) (i + ox) * B + (j + oy)) * K + kk];
+    }
+    __syncthreads();
+    for (int kq = ty; kq < 32; kq += 8) {
+        int kk = k0 + kq, j = j0 + tx;
+        if (j < G.ny && kk < K) dst[((long long) (kk + oz) * G.nx + i) * G.ny + j] = tile[tx][kq];
+    }
+}
+
+__global__ void k_dev2host(Geo G, const double* __restrict__ src, double* __restrict__ dst,
+                           int A, int B, int K, int ox, int oy, int oz)
+{
+    __shared__ double tile[32][33];
+    const int k0 = blockIdx.x * 32, b0 = blockIdx.y * 32, a = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    int i = a - ox;
+    i = ((i % G.nx) + G.nx) % G.nx;
+    for (int kq = ty; kq < 32; kq += 8) {
+        int kk = k0 + kq, b = b0 + tx;
+        if (b < B && kk < K) {
+            int j = ((b - oy) % G.ny + G.ny) % G.ny;
+            tile[kq][tx] = src[((long long) (kk + oz) * G.nx + i) * G.ny + j];
+        }
+    }
+    __syncthreads();
+    for (int bb = ty; bb < 32; bb += 8) {
+        int b = b0 + bb, kk = k0 + tx;
+        if (b < B && kk < K) dst[((long long) a * B + b) * K + kk] = tile[tx][bb];
+    }
+    (void) A;
+}
+
+template <int ORDER>
+__global__ void k_max_div(Geo G, const double* u, const double* v, const double* w, double* blockmax)
+{
+    __shared__ double red[256];
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    double m = 0.0;
+    const long long total = (long long) G.nz * G.plane;
+    for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long) gridDim.x * blockDim.x) {
+        int k = GZ + (int) (t / G.plane);
+        long long rem = t - (long long) (k - GZ) * G.plane;
+        int i = (int) (rem / ny), j = (int) (rem - (long long) i * ny);
+        auto I = [&](int kk, int ii, int jj) {
+            ii = ii < 0 ? ii + nx : (ii >= nx ? ii - nx : ii);
+            jj = jj < 0 ? jj + ny : (jj >= ny ? jj - ny : jj);
+            return ((long long) kk * nx + ii) * ny + jj;
+        };
+        double d;
+        if (ORDER == 2) {
+            d = (u[I(k, i, j)] - u[I(k, i - 1, j)]) / G.dx + (v[I(k, i, j)] - v[I(k, i, j - 1)]) / G.dy
+              + (w[I(k, i, j)] - w[I(k - 1, i, j)]) / G.dz[k];
+        } else {
+            const int kb = GZ - 1, kt = n2 - GZ - 1;
+            double wkm2 = (k - 2 == kb - 1) ? 2.0 * w[I(kb, i, j)] - w[I(kb + 1, i, j)] : w[I(k - 2, i, j)];
+            double wkp1 = (k + 1 == kt + 1) ? 2.0 * w[I(kt, i, j)] - w[I(kt - 1, i, j)] : w[I(k + 1, i, j)];
+            d = (A1 * (u[I(k, i, j)] - u[I(k, i - 1, j)]) + A2 * (u[I(k, i + 1, j)] - u[I(k, i - 2, j)])) / G.dx
+              + (A1 * (v[I(k, i, j)] - v[I(k, i, j - 1)]) + A2 * (v[I(k, i, j + 1)] - v[I(k, i, j - 2)])) / G.dy
+              + (A1 * (w[I(k, i, j)] - w[I(k - 1, i, j)]) + A2 * (wkp1 - wkm2)) / G.dz[k];
+        }
+        m = fmax(m, fabs(d));
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) blockmax[blockIdx.x] = red[0];
+}
+
+// get_cfl (get.c:390-416) over interior cells
+__global__ void k_cfl(Geo G, const double* u, const double* v, const double* w, double dt, double* blockmax)
+{
+    __shared__ double red[256];
+    double m = 0.0;
+    const long long total = (long long) G.nz * G.plane;
+    for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long) gridDim.x * blockDim.x) {
+        int k = GZ + (int) (t / G.plane);
+        long long d = (long long) GZ * G.plane + t;
+        double dzph = 0.5 * (G.dz[k] + G.dz[k + 1]);
+        double c;
+        if (m < (c = fabs(u[d]) * dt / G.dx)) m = c;
+        if (m < (c = fabs(v[d]) * dt / G.dy)) m = c;
+        if (m < (c = fabs(w[d]) * dt / dzph)) m = c;
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) blockmax[blockIdx.x] = red[0];
+}
+
+__global__ void k_zero(double* p, long long n)
+{
+    for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long) gridDim.x * blockDim.x)
+        p[t] = 0.0;
+}
+
+// ------------------------------------------------------------ host helpers
+
+// Packs host vectors into one device allocation.
+struct Arena {
+    std::vector<double> h;
+    size_t add(const std::vector<double>& v)
+    {
+        size_t off = h.size();
+        h.insert(h.end(), v.begin(), v.end());
+        while (h.size() % 4) h.push_back(0.0);  // 32-byte alignment of every table
+        return off;
+    }
+};
+
+WallRowsD to_dev(const WallRows& w)
+{
+    WallRowsD d;
+    std::memcpy(d.row, w.row, sizeof(d.row));
+    return d;
+}
+
+std::vector<int> fft_radices(int n)
+{
+    std::vector<int> r;
+    while (n % 8 == 0 && n > 8) { r.push_back(8); n /= 8; }
+    if (n == 8) { r.push_back(8); n = 1; }
+    while (n % 4 == 0) { r.push_back(4); n /= 4; }
+    while (n % 2 == 0) { r.push_back(2); n /= 2; }
+    while (n % 3 == 0) { r.push_back(3); n /= 3; }
+    while (n % 5 == 0) { r.push_back(5); n /= 5; }
+    if (n != 1) r.clear();
+    return r;
+}
+
+}  // namespace
+
+struct SetOffsets {
+    size_t F1, F2, F3, DEN, P, Q, R, hbc, green;
+    int k0, n;
+    WallRowsD bot, top;
+    double gstats[4];
+};
+
+struct PoissonOffsets {
+    size_t a, b, c, e, f, g, dpart, dvol;
+    PoissonSet host;
+};
+
+struct cf_instance {
+    cf_config cfg;
+    Metrics m;
+    Geo geo;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double *u = nullptr, *v = nullptr, *w = nullptr, *c = nullptr, *p = nullptr;
+    double* fbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* gbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+    double2* spec = nullptr;
+    double* scratch = nullptr;
+    double* partial = nullptr;
+    double* avg = nullptr;
+    double* dscal = nullptr;        // [0] mdpdx, [1] dcdt
+    long long* dcount = nullptr;    // device substep counter (log row)
+    double* dlog = nullptr;
+    int log_cap = 0;
+    double* staging = nullptr;
+    size_t staging_elems = 0;
+    double* coef = nullptr;         // arena of all tables
+    double* lamx = nullptr;         // inside coef
+    double* lamy = nullptr;
+    double* zp = nullptr;
+    double2 *twx = nullptr, *twy = nullptr;
+    FftPlan px, py;
+    double c8 = 0.0;
+    // per substep s (0..2): sets for u, v, c, w and the Poisson solve
+    SetOffsets set[3][4];
+    PoissonOffsets pois[3];
+    PoissonOffsets pois_init;
+    WallRowsD bc_ub, bc_ut, bc_wb, bc_wt;
+    long substep = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long log_rows_host = 0;
+};
+
+namespace {
+
+int check_config(const cf_config* c)
+{
+    if (!c) return CF_EINVAL;
+    if (c->order != 2 && c->order != 4) return CF_EINVAL;
+    if (c->ngz != GZ) return CF_EINVAL;
+    if (c->nx < 4 || c->ny < 4 || c->nz < (c->order == 4 ? 6 : 4)) return CF_EINVAL;
+    if (c->ngx < 0 || c->ngy < 0) return CF_EINVAL;
+    if (c->nx > FFT_MAX_N || c->ny > FFT_MAX_N) return CF_EINVAL;
+    if (fft_radices(c->nx).empty() || fft_radices(c->ny).empty()) return CF_EINVAL;
+    if (!(c->dt > 0.0) || !(c->nu >= 0.0) || !(c->prandtl > 0.0)) return CF_EINVAL;
+    if (!(c->lx > 0.0) || !(c->ly > 0.0) || !(c->lz > 0.0)) return CF_EINVAL;
+    return CF_OK;
+}
+
+// Build every per-substep coefficient table for time step dt and upload.
+int build_tables(cf_instance* I, double dt)
+{
+    const cf_config& C = I->cfg;
+    const Metrics& m = I->m;
+    Arena A;
+    auto addfac = [&](SetOffsets& so, const ImplicitSet& s) {
+        so.k0 = s.fac.k0;
+        so.n = s.fac.n;
+        so.F1 = A.add(s.fac.F1); so.F2 = A.add(s.fac.F2); so.F3 = A.add(s.fac.F3);
+        so.DEN = A.add(s.fac.DEN); so.P = A.add(s.fac.P); so.Q = A.add(s.fac.Q); so.R = A.add(s.fac.R);
+        so.hbc = A.add(s.hbc);
+        so.green = A.add(s.green.empty() ? std::vector<double>(m.n2, 0.0) : s.green);
+        so.bot = to_dev(s.bot);
+        so.top = to_dev(s.top);
+        std::memcpy(so.gstats, s.green_stats, sizeof(so.gstats));
+    };
+    double uf = C.setuframe, vf = C.setvframe;
+    try {
+        for (int s = 0; s < 3; s++) {
+            double nubdt = C.nu * RK3_BET[s] * dt;
+            double gamdt = RK3_GAM[s] * dt;
+            // chanfast.c:61-68: u, v walls at -frame, scalar -0.5 / +0.5, w 0
+            ImplicitSet su = make_implicit_u(m, nubdt, gamdt, 0.0 - uf, 0.0 - uf, C.nu, true);
+            ImplicitSet sv = make_implicit_u(m, nubdt, gamdt, 0.0 - vf, 0.0 - vf, C.nu, false);
+            ImplicitSet sc = make_implicit_u(m, nubdt / C.prandtl, gamdt, -0.5, +0.5, C.nu / C.prandtl, true);
+            ImplicitSet sw = make_implicit_w(m, nubdt, 0.0, 0.0);
+            addfac(I->set[s][0], su);
+            addfac(I->set[s][1], sv);
+            addfac(I->set[s][2], sc);
+            addfac(I->set[s][3], sw);
+        }
+    } catch (const std::exception&) {
+        g_last_error = "zero pivot in a line-solve factorisation";
+        return CF_EPIVOT;
+    }
+    auto addpois = [&](PoissonOffsets& po, double pdt) {
+        po.host = make_poisson(m, pdt);
+        po.a = A.add(po.host.a); po.b = A.add(po.host.b); po.c = A.add(po.host.c);
+        po.e = A.add(po.host.e); po.f = A.add(po.host.f); po.g = A.add(po.host.g);
+        po.dpart = A.add(po.host.dpart); po.dvol = A.add(po.host.dvol);
+    };
+    for (int s = 0; s < 3; s++) addpois(I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt);
+    addpois(I->pois_init, 1.0);
+    size_t o_lamx = A.add(I->pois_init.host.lamx);
+    size_t o_lamy = A.add(I->pois_init.host.lamy);
+    // metrics
+    int n2 = m.n2;
+    std::vector<double> dzp1h(n2, 0.0), dzm1h(n2, 0.0), dzp3h(n2, 0.0), dzm3h(n2, 0.0), dydz(n2), dxdz(n2);
+    for (int k = 0; k < n2; k++) {
+        if (k + 1 < n2) dzp1h[k] = 0.5 * (m.dz[k + 1] + m.dz[k]);
+        if (k >= 1) dzm1h[k] = 0.5 * (m.dz[k - 1] + m.dz[k]);
+        if (k + 2 < n2) dzp3h[k] = 0.5 * (m.dz[k + 2] + m.dz[k + 1]);
+        if (k >= 2) dzm3h[k] = 0.5 * (m.dz[k - 2] + m.dz[k - 1]);
+        dydz[k] = m.dy * m.dz[k];
+        dxdz[k] = m.dx * m.dz[k];
+    }
+    size_t o_dz = A.add(m.dz), o_p1 = A.add(dzp1h), o_m1 = A.add(dzm1h), o_p3 = A.add(dzp3h),
+           o_m3 = A.add(dzm3h), o_dydz = A.add(dydz), o_dxdz = A.add(dxdz);
+    size_t o_zp = A.add(z_at_p(m));
+
+    if (I->coef) { cudaFree(I->coef); I->coef = nullptr; }
+    CF_CUDA(cudaMalloc(&I->coef, A.h.size() * sizeof(double)));
+    CF_CUDA(cudaMemcpy(I->coef, A.h.data(), A.h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    double* b = I->coef;
+    Geo& G = I->geo;
+    G.dz = b + o_dz; G.dzp1h = b + o_p1; G.dzm1h = b + o_m1; G.dzp3h = b + o_p3; G.dzm3h = b + o_m3;
+    G.dydz = b + o_dydz; G.dxdz = b + o_dxdz;
+    I->lamx = b + o_lamx;
+    I->lamy = b + o_lamy;
+    I->zp = b + o_zp;
+    I->cfg.dt = dt;
+    // a new graph is needed whenever the tables move
+    if (I->gexec) { cudaGraphExecDestroy(I->gexec); I->gexec = nullptr; }
+    if (I->graph) { cudaGraphDestroy(I->graph); I->graph = nullptr; }
+    return CF_OK;
+}
+
+FactorD factor_of(cf_instance* I, const SetOffsets& so)
+{
+    double* b = I->coef;
+    FactorD f;
+    f.k0 = so.k0;
+    f.n = so.n;
+    f.F1 = b + so.F1; f.F2 = b + so.F2; f.F3 = b + so.F3; f.DEN = b + so.DEN;
+    f.P = b + so.P; f.Q = b + so.Q; f.R = b + so.R;
+    return f;
+}
+
+PoissonArgs poisson_args(cf_instance* I, const PoissonOffsets& po, double pdt)
+{
+    double* b = I->coef;
+    PoissonArgs A;
+    A.spec = I->spec;
+    A.scratch = I->scratch;
+    A.a = b + po.a; A.b = b + po.b; A.c = b + po.c; A.e = b + po.e; A.f = b + po.f; A.g = b + po.g;
+    A.dpart = b + po.dpart; A.dvol = b + po.dvol;
+    A.lamx = I->lamx;
+    A.lamy = I->lamy;
+    std::memcpy(A.red, po.host.red, sizeof(A.red));
+    std::memcpy(A.dsub, po.host.dsub, sizeof(A.dsub));
+    A.bot[0] = to_dev(po.host.bot[0]);
+    A.bot[1] = to_dev(po.host.bot[1]);
+    A.top = to_dev(po.host.top);
+    A.dt = pdt;
+    A.dxdx = I->m.dx * I->m.dx;
+    A.dydy = I->m.dy * I->m.dy;
+    return A;
+}
+
+// Divergence -> FFT -> Poisson -> inverse FFT -> projection with step `pdt`.
+// With `corr`, the lazily applied mass-flux corrections of substep set `s`
+// are folded in (divergence and projection read u + G_u * mdpdx, c + G_c * dcdt).
+void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr)
+{
+    const Geo& G = I->geo;
+    cudaStream_t st = I->stream;
+    double* b = I->coef;
+    DivArgs D{I->u, I->v, I->w, corr ? b + I->set[s][0].green : nullptr, corr ? I->dscal : nullptr,
+              I->spec, I->px, I->c8};
+    launch_div_fftx(G, D, st);
+    FftyArgs Y{I->spec, I->py, -1, GZ, I->c8};
+    launch_ffty(G, Y, G.nz, st);
+    launch_poisson(G, poisson_args(I, po, pdt), st);
+    FftyArgs Yb{I->spec, I->py, +1, 0, I->c8};
+    launch_ffty(G, Yb, G.n2, st);
+    C2rArgs X{I->spec, I->p, I->px, I->c8};
+    launch_fftx_c2r(G, X, st);
+    ProjArgs P;
+    P.u = I->u; P.v = I->v; P.w = I->w; P.c = I->c; P.p = I->p;
+    P.gu = corr ? b + I->set[s][0].green : nullptr;
+    P.gc = corr ? b + I->set[s][2].green : nullptr;
+    P.mu = corr ? I->dscal : nullptr;
+    P.mc = corr ? I->dscal + 1 : nullptr;
+    P.dt = pdt;
+    launch_project(G, P, st);
+}
+
+void enqueue_substep(cf_instance* I)
+{
+    const cf_config& C = I->cfg;
+    const Geo& G = I->geo;
+    cudaStream_t st = I->stream;
+    const int s = (int) (I->substep % 3);
+    const double dt = C.dt;
+    for (int q = 0; q < 4; q++) std::swap(I->fbuf[q], I->gbuf[q]);   // chanfast.c:397-402
+
+    GhostArgs GA;
+    GA.F = Fields{I->u, I->v, I->w, I->c};
+    GA.ub = I->bc_ub; GA.ut = I->bc_ut; GA.wb = I->bc_wb; GA.wt = I->bc_wt;
+    GA.bc_u = 0.0 - C.setuframe;
+    GA.bc_v = 0.0 - C.setvframe;
+    GA.bc_c_bot = -0.5;
+    GA.bc_c_top = +0.5;
+    GA.bc_w = 0.0;
+    launch_ghosts(G, GA, st);
+
+    RhsArgs R{I->u, I->v, I->w, I->c, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
+              C.nu, C.nu / C.prandtl, C.betg_x, C.betg_y, C.betg_z};
+    launch_rhs(G, R, st);
+
+    const double nuadt = C.nu * RK3_ALP[s] * dt;
+    const double gamdt = RK3_GAM[s] * dt;
+    const double zetdt = RK3_ZET[s] * dt;
+    double* fields[4] = {I->u, I->v, I->c, I->w};
+    const int fidx[4] = {0, 1, 3, 2};   // u, v, c, w -> f/g slots (u, v, w, c)
+    double bcb[4] = {0.0 - C.setuframe, 0.0 - C.setvframe, -0.5, 0.0};
+    double bct[4] = {0.0 - C.setuframe, 0.0 - C.setvframe, +0.5, 0.0};
+    for (int q = 0; q < 4; q++) {
+        const SetOffsets& so = I->set[s][q];
+        const bool is_w = q == 3, stats = q == 0 || q == 2;
+        SolveArgs S;
+        S.x = fields[q];
+        S.f = I->fbuf[fidx[q]];
+        S.g = I->gbuf[fidx[q]];
+        S.gshift = q == 0 ? I->dscal : (q == 2 ? I->dscal + 1 : nullptr);
+        S.fac = factor_of(I, so);
+        S.hbc = I->coef + so.hbc;
+        S.nuadt = q == 2 ? nuadt / C.prandtl : nuadt;
+        S.gamdt = gamdt;
+        S.zetdt = zetdt;
+        S.bc_bot = bcb[q];
+        S.bc_top = bct[q];
+        S.bcb = is_w ? I->bc_wb : I->bc_ub;
+        S.bct = is_w ? I->bc_wt : I->bc_ut;
+        S.partial = stats ? I->partial : nullptr;
+        launch_solve(G, S, is_w, S.gshift != nullptr, st);
+        if (stats) {
+            MassArgs M;
+            M.avg = I->avg;
+            M.dz = G.dz;
+            M.order = C.order;
+            M.nz = C.nz;
+            M.n2 = G.n2;
+            M.kappa = q == 0 ? C.nu : C.nu / C.prandtl;
+            std::memcpy(M.green, so.gstats, sizeof(M.green));
+            M.mode = q == 0 ? C.uvolavgmode : C.cvolavgmode;
+            M.target = q == 0 ? C.want_uvolavg - C.setuframe : C.want_cvolavg;
+            M.fixed = q == 0 ? -C.dpdx : 0.0;
+            M.m_out = I->dscal + (q == 0 ? 0 : 1);
+            M.counter = I->dcount;
+            M.log_base = I->dlog;
+            M.log_cap = I->log_cap;
+            M.col = q == 0 ? 0 : 5;
+            M.advance = q == 2 ? 1 : 0;
+            launch_mass(G, I->partial, I->avg, M, st);
+        }
+    }
+    pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true);
+    I->substep++;
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+
+extern "C" {
+
+const char* cf_strerror(int status)
+{
+    switch (status) {
+    case CF_OK: return "ok";
+    case CF_EINVAL: return "invalid argument or unsupported configuration";
+    case CF_ENOMEM: return "out of memory";
+    case CF_ECUDA: return g_last_error.empty() ? "CUDA runtime error" : g_last_error.c_str();
+    case CF_EPIVOT: return "zero pivot in a band factorisation";
+    case CF_ENONFINITE: return "non-finite value";
+    case CF_EIO: return "file I/O error";
+    default: return "unknown status";
+    }
+}
+
+int cf_destroy(cf_instance* I)
+{
+    if (!I) return CF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(I->device);
+    if (I->stream) cudaStreamSynchronize(I->stream);
+    if (I->gexec) cudaGraphExecDestroy(I->gexec);
+    if (I->graph) cudaGraphDestroy(I->graph);
+    void* bufs[] = {I->u, I->v, I->w, I->c, I->p, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
+                    I->gbuf[0], I->gbuf[1], I->gbuf[2], I->gbuf[3], I->spec, I->scratch, I->partial,
+                    I->avg, I->dscal, I->dcount, I->dlog, I->staging, I->coef, I->twx, I->twy};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (I->own_stream && I->stream) cudaStreamDestroy(I->stream);
+    cudaSetDevice(prev);
+    delete I;
+    return CF_OK;
+}
+
+static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
+{
+    I->cfg = *cfg;
+    const cf_config& C = *cfg;
+    CF_CUDA(cudaGetDevice(&I->device));
+    I->m = make_metrics(C.order, C.nx, C.ny, C.nz, GZ, C.lx, C.ly, C.lz);
+    Geo& G = I->geo;
+    G.order = C.order;
+    G.nx = C.nx;
+    G.ny = C.ny;
+    G.nz = C.nz;
+    G.n2 = C.nz + 2 * GZ;
+    G.nkx = C.nx / 2 + 1;
+    G.plane = (long long) C.nx * C.ny;
+    G.splane = (long long) G.nkx * C.ny;
+    G.dx = I->m.dx;
+    G.dy = I->m.dy;
+    G.dxdy = I->m.dx * I->m.dy;
+    if (stream) {
+        I->stream = (cudaStream_t) stream;
+    } else {
+        CF_CUDA(cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking));
+        I->own_stream = true;
+    }
+    const size_t fb = (size_t) G.plane * G.n2 * sizeof(double);
+    double** fl[] = {&I->u, &I->v, &I->w, &I->c, &I->p, &I->fbuf[0], &I->fbuf[1], &I->fbuf[2], &I->fbuf[3],
+                     &I->gbuf[0], &I->gbuf[1], &I->gbuf[2], &I->gbuf[3]};
+    for (double** pp : fl) {
+        CF_CUDA(cudaMalloc(pp, fb));
+        CF_CUDA(cudaMemsetAsync(*pp, 0, fb, I->stream));
+    }
+    CF_CUDA(cudaMalloc(&I->spec, (size_t) G.splane * G.n2 * sizeof(double2)));
+    CF_CUDA(cudaMemsetAsync(I->spec, 0, (size_t) G.splane * G.n2 * sizeof(double2), I->stream));
+    const int nscr = C.order == 4 ? 3 : 1;
+    CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
+    const long long nwarps = ((G.plane + 127) / 128) * 4;   // per-warp partial sums of k_solve
+    CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
+    CF_CUDA(cudaMalloc(&I->avg, (size_t) G.n2 * sizeof(double)));
+    CF_CUDA(cudaMalloc(&I->dscal, 8 * sizeof(double)));
+    CF_CUDA(cudaMemsetAsync(I->dscal, 0, 8 * sizeof(double), I->stream));
+    CF_CUDA(cudaMalloc(&I->dcount, sizeof(long long)));
+    CF_CUDA(cudaMemsetAsync(I->dcount, 0, sizeof(long long), I->stream));
+    I->log_cap = 3 * 4096;
+    CF_CUDA(cudaMalloc(&I->dlog, (size_t) I->log_cap * LOG_COLS * sizeof(double)));
+    CF_CUDA(cudaMemsetAsync(I->dlog, 0, (size_t) I->log_cap * LOG_COLS * sizeof(double), I->stream));
+    // FFT plans
+    auto plan = [&](int n, FftPlan& P, double2*& tw) -> int {
+        std::vector<int> r = fft_radices(n);
+        P.n = n;
+        P.nstages = (int) r.size();
+        for (int q = 0; q < P.nstages; q++) P.radix[q] = r[q];
+        std::vector<double2> t(n);
+        for (int q = 0; q < n; q++) {
+            double a = 2.0 * M_PI * (double) q / (double) n;
+            t[q] = make_double2(std::cos(a), -std::sin(a));
+        }
+        CF_CUDA(cudaMalloc(&tw, n * sizeof(double2)));
+        CF_CUDA(cudaMemcpy(tw, t.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+        P.tw = tw;
+        return CF_OK;
+    };
+    int rc = plan(C.nx, I->px, I->twx);
+    if (rc) return rc;
+    rc = plan(C.ny, I->py, I->twy);
+    if (rc) return rc;
+    I->c8 = std::cos(M_PI / 4.0);
+    CF_CUDA(fft_set_smem_limits(std::max(C.nx, C.ny)));
+    I->bc_ub = to_dev(bc_rows_u(I->m, true));
+    I->bc_ut = to_dev(bc_rows_u(I->m, false));
+    I->bc_wb = to_dev(bc_rows_w(I->m, true));
+    I->bc_wt = to_dev(bc_rows_w(I->m, false));
+    rc = build_tables(I, C.dt);
+    if (rc) return rc;
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    return CF_OK;
+}
+
+int cf_create(const cf_config* cfg, void* stream, cf_instance** out)
+{
+    if (!out) return CF_EINVAL;
+    *out = nullptr;
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    cf_instance* I = new (std::nothrow) cf_instance();
+    if (!I) return CF_ENOMEM;
+    rc = create_impl(cfg, stream, I);
+    if (rc) {
+        cf_destroy(I);
+        return rc;
+    }
+    *out = I;
+    return CF_OK;
+}
+
+static double* field_ptr(cf_instance* I, int f)
+{
+    switch (f) {
+    case CF_U: return I->u;
+    case CF_V: return I->v;
+    case CF_W: return I->w;
+    case CF_C: return I->c;
+    case CF_P: return I->p;
+    default: return nullptr;
+    }
+}
+
+static int layout_dims(cf_instance* I, int layout, int& A, int& B, int& K, int& ox, int& oy, int& oz)
+{
+    const cf_config& C = I->cfg;
+    if (layout == CF_LAYOUT_PADDED) {
+        A = C.nx + 2 * C.ngx; B = C.ny + 2 * C.ngy; K = C.nz + 2 * GZ;
+        ox = C.ngx; oy = C.ngy; oz = 0;
+    } else if (layout == CF_LAYOUT_INTERIOR) {
+        A = C.nx; B = C.ny; K = C.nz;
+        ox = 0; oy = 0; oz = GZ;
+    } else {
+        return CF_EINVAL;
+    }
+    return CF_OK;
+}
+
+static int ensure_staging(cf_instance* I, size_t n)
+{
+    if (I->staging_elems >= n) return CF_OK;
+    if (I->staging) cudaFree(I->staging);
+    I->staging = nullptr;
+    I->staging_elems = 0;
+    CF_CUDA(cudaMalloc(&I->staging, n * sizeof(double)));
+    I->staging_elems = n;
+    return CF_OK;
+}
+
+int cf_set_field(cf_instance* I, int field, const double* host, int layout)
+{
+    if (!I || !host || field < CF_U || field > CF_C) return CF_EINVAL;
+    int A, B, K, ox, oy, oz;
+    if (layout_dims(I, layout, A, B, K, ox, oy, oz)) return CF_EINVAL;
+    size_t n = (size_t) A * B * K;
+    int rc = ensure_staging(I, n);
+    if (rc) return rc;
+    CF_CUDA(cudaMemcpyAsync(I->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, I->stream));
+    dim3 blk(32, 8), grd((K + 31) / 32, (I->geo.ny + 31) / 32, I->geo.nx);
+    k_host2dev<<<grd, blk, 0, I->stream>>>(I->geo, I->staging, field_ptr(I, field), B, K, ox, oy, oz);
+    CF_CUDA(cudaGetLastError());
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    return CF_OK;
+}
+
+int cf_get_field(cf_instance* I, int field, double* host, int layout)
+{
+    if (!I || !host || field < CF_U || field > CF_P) return CF_EINVAL;
+    int A, B, K, ox, oy, oz;
+    if (layout_dims(I, layout, A, B, K, ox, oy, oz)) return CF_EINVAL;
+    size_t n = (size_t) A * B * K;
+    int rc = ensure_staging(I, n);
+    if (rc) return rc;
+    dim3 blk(32, 8), grd((K + 31) / 32, (B + 31) / 32, A);
+    k_dev2host<<<grd, blk, 0, I->stream>>>(I->geo, field_ptr(I, field), I->staging, A, B, K, ox, oy, oz);
+    CF_CUDA(cudaGetLastError());
+    CF_CUDA(cudaMemcpyAsync(host, I->staging, n * sizeof(double), cudaMemcpyDeviceToHost, I->stream));
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    return CF_OK;
+}
+
+int cf_init_fields(cf_instance* I, unsigned long long seed, double amp, double c_amp)
+{
+    if (!I) return CF_EINVAL;
+    const Geo& G = I->geo;
+    dim3 blk(128), grd((G.ny + 127) / 128, G.nx, G.n2);
+    k_init_raw<<<grd, blk, 0, I->stream>>>(G, I->u, I->v, I->w, I->c, I->zp, seed, amp, c_amp);
+    CF_CUDA(cudaGetLastError());
+    pressure_sequence(I, I->pois_init, 1.0, 0, false);
+    CF_CUDA(cudaGetLastError());
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    return CF_OK;
+}
+
+int cf_step(cf_instance* I, int nsub)
+{
+    if (!I || nsub < 0) return CF_EINVAL;
+    for (int q = 0; q < nsub; q++) {
+        enqueue_substep(I);
+        CF_CUDA(cudaGetLastError());
+    }
+    return CF_OK;
+}
+
+int cf_step_graph(cf_instance* I, int nsteps)
+{
+    if (!I || nsteps < 0) return CF_EINVAL;
+    // align to the start of an RK3 step
+    while (I->substep % 3 != 0 && nsteps > 0) {
+        int rc = cf_step(I, 1);
+        if (rc) return rc;
+    }
+    // The graph holds two RK3 steps: an even number of f/g swaps leaves the
+    // buffer roles where capture found them.
+    while (nsteps >= 2) {
+        if (!I->gexec) {
+            long saved = I->substep;
+            CF_CUDA(cudaStreamBeginCapture(I->stream, cudaStreamCaptureModeThreadLocal));
+            for (int q = 0; q < 6; q++) enqueue_substep(I);
+            cudaError_t e = cudaStreamEndCapture(I->stream, &I->graph);
+            I->substep = saved;
+            CF_CUDA(e);
+            CF_CUDA(cudaGraphInstantiate(&I->gexec, I->graph, 0));
+        }
+        CF_CUDA(cudaGraphLaunch(I->gexec, I->stream));
+        I->substep += 6;
+        nsteps -= 2;
+    }
+    if (nsteps > 0) return cf_step(I, 3 * nsteps);
+    return CF_OK;
+}
+
+int cf_sync(cf_instance* I)
+{
+    if (!I) return CF_EINVAL;
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    return CF_OK;
+}
+
+long cf_substeps_done(const cf_instance* I) { return I ? I->substep : CF_EINVAL; }
+
+long cf_get_log(cf_instance* I, double* out, long max_rows)
+{
+    if (!I || max_rows < 0) return CF_EINVAL;
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    long long count = 0;
+    CF_CUDA(cudaMemcpy(&count, I->dcount, sizeof(count), cudaMemcpyDeviceToHost));
+    long long avail = count < I->log_cap ? count : I->log_cap;
+    long long nret = avail < max_rows ? avail : max_rows;
+    if (!out || nret == 0) return (long) nret;
+    std::vector<double> all((size_t) I->log_cap * LOG_COLS);
+    CF_CUDA(cudaMemcpy(all.data(), I->dlog, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (long long r = 0; r < nret; r++) {
+        long long row = count - nret + r;
+        std::memcpy(out + r * LOG_COLS, all.data() + (row % I->log_cap) * LOG_COLS, LOG_COLS * sizeof(double));
+    }
+    return (long) nret;
+}
+
+int cf_max_divergence(cf_instance* I, double* out)
+{
+    if (!I || !out) return CF_EINVAL;
+    const int nb = 592;
+    double* d = nullptr;
+    CF_CUDA(cudaMalloc(&d, nb * sizeof(double)));
+    if (I->cfg.order == 2) k_max_div<2><<<nb, 256, 0, I->stream>>>(I->geo, I->u, I->v, I->w, d);
+    else k_max_div<4><<<nb, 256, 0, I->stream>>>(I->geo, I->u, I->v, I->w, d);
+    std::vector<double> h(nb);
+    cudaError_t e = cudaMemcpyAsync(h.data(), d, nb * sizeof(double), cudaMemcpyDeviceToHost, I->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(I->stream);
+    cudaFree(d);
+    CF_CUDA(e);
+    double m = 0.0;
+    for (double x : h) m = std::fmax(m, x);
+    *out = m;
+    return CF_OK;
+}
+
+int cf_cfl(cf_instance* I, double dt, double* cfl)
+{
+    if (!I || !cfl) return CF_EINVAL;
+    const int nb = 592;
+    double* d = nullptr;
+    CF_CUDA(cudaMalloc(&d, nb * sizeof(double)));
+    k_cfl<<<nb, 256, 0, I->stream>>>(I->geo, I->u, I->v, I->w, dt, d);
+    std::vector<double> h(nb);
+    cudaError_t e = cudaMemcpyAsync(h.data(), d, nb * sizeof(double), cudaMemcpyDeviceToHost, I->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(I->stream);
+    cudaFree(d);
+    CF_CUDA(e);
+    double m = 0.0;
+    for (double x : h) m = std::fmax(m, x);
+    *cfl = m;
+    return CF_OK;
+}
+
+int cf_set_dt(cf_instance* I, double dt)
+{
+    if (!I || !(dt > 0.0)) return CF_EINVAL;
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    return build_tables(I, dt);
+}
+
+int cf_device_field(cf_instance* I, int field, double** dev_ptr, long long* n_elems)
+{
+    if (!I || !dev_ptr) return CF_EINVAL;
+    double* p = field_ptr(I, field);
+    if (!p) return CF_EINVAL;
+    *dev_ptr = p;
+    if (n_elems) *n_elems = I->geo.plane * I->geo.n2;
+    return CF_OK;
+}
+
+int cf_launches_per_substep(const cf_instance* I)
+{
+    // ghosts, rhs, 4 solves, 2 x (row average + mass control), div+fftx,
+    // ffty, poisson, ffty, fftx_c2r, project
+    return I ? 16 : CF_EINVAL;
+}
+
+}  // extern "C"

@@ -1,0 +1,565 @@
+// Pressure projection: divergence, 2-D real FFT over (x, y), per-wavenumber
+// banded Poisson solve in z, inverse FFT, projection.
+//
+//   k_div_fftx   divergence{2,4} (pressure.c:40-117) fused with the real DFT
+//                along x and its 1/nx scaling (fft.c:38-51, 161-177)
+//   k_ffty       complex DFT along y, forward with 1/ny (fft.c:97-118,186-202)
+//                or backward unscaled
+//   k_poisson    pressure_poisson{2,4} (pressure.c:293-443): one thread per
+//                (kx, ky) column, Re and Im sharing one factorisation
+//   k_fftx_c2r   inverse real DFT along x (fft.c:53-63, 180-183): the
+//                half spectrum is completed by Hermitian symmetry, the
+//                imaginary parts of the DC and Nyquist bins are ignored
+//   k_project    project{2,4} (pressure.c:120-194) fused with the lazily
+//                applied mass-flux / scalar-mean corrections of the substep
+//                (chanfast.c:516-519, 603-606)
+//
+// FFTs run in shared memory: a Stockham autosort mixed-radix (2/3/4/5/8)
+// transform over L lines of one thread block, twiddles from a host table.
+#include "engine.cuh"
+#include "host_band.h"
+
+namespace cf {
+
+__device__ __forceinline__ int wrapp(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// multiply by s*i (s = +-1)
+__device__ __forceinline__ double2 cmul_si(double2 a, int s)
+{
+    return s > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+struct FftCtx {
+    double2* buf;
+    int N, L;
+    bool line_major;      // element (pos, line) at buf[line*N + pos], else buf[pos*L + line]
+    int sign;             // -1 forward, +1 backward
+    const double2* tw;    // exp(-2 pi i m / N)
+    double c8;            // cos(pi/4) from the host table
+};
+
+__device__ __forceinline__ int fidx(const FftCtx& F, int pos, int line)
+{
+    return F.line_major ? line * F.N + pos : pos * F.L + line;
+}
+
+__device__ __forceinline__ double2 twid(const FftCtx& F, int m)
+{
+    double2 t = __ldg(&F.tw[m]);
+    if (F.sign > 0) t.y = -t.y;
+    return t;
+}
+
+template <int R>
+__device__ __forceinline__ void dft_small(double2* v, const FftCtx& F)
+{
+    const int s = F.sign;
+    if (R == 2) {
+        double2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if (R == 4) {
+        double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+        double2 t2 = cadd(v[1], v[3]), t3 = cmul_si(csub(v[1], v[3]), s);
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    } else if (R == 8) {
+        double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<4>(e, F);
+        dft_small<4>(o, F);
+        const double c = F.c8;
+        // W8^1 = c (1 + s i), W8^2 = s i, W8^3 = c (-1 + s i)
+        double2 o1 = make_double2(c * (o[1].x - s * o[1].y), c * (o[1].y + s * o[1].x));
+        double2 o2 = cmul_si(o[2], s);
+        double2 o3 = make_double2(c * (-o[3].x - s * o[3].y), c * (-o[3].y + s * o[3].x));
+        v[0] = cadd(e[0], o[0]); v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);   v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);   v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);   v[7] = csub(e[3], o3);
+    } else {
+        // generic (3, 5): roots of unity from the host table
+        double2 out[R];
+        const int step = F.N / R;
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            double2 acc = v[0];
+#pragma unroll
+            for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid(F, ((r * q) % R) * step)));
+            out[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < R; q++) v[q] = out[q];
+    }
+}
+
+// One Stockham stage of radix R (Ns = product of the previous radices).
+template <int R, int MAXB>
+__device__ void fft_stage(const FftCtx& F, int Ns)
+{
+    const int NR = F.N / R;
+    const int nb = NR * F.L;
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    double2 v[MAXB][R];
+    int jj[MAXB], ll[MAXB];
+#pragma unroll
+    for (int t = 0; t < MAXB; t++) {
+        int b = tid + t * nthr;
+        jj[t] = -1;
+        if (b < nb) {
+            int line, j;
+            if (F.line_major) { line = b / NR; j = b - line * NR; }
+            else { j = b / F.L; line = b - j * F.L; }
+            jj[t] = j;
+            ll[t] = line;
+            int k = j % Ns;
+            int tstep = F.N / (Ns * R);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                double2 a = F.buf[fidx(F, j + r * NR, line)];
+                if (r > 0 && k > 0) a = cmul(a, twid(F, (r * k * tstep) % F.N));
+                v[t][r] = a;
+            }
+            dft_small<R>(v[t], F);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < MAXB; t++) {
+        if (jj[t] < 0) continue;
+        int j = jj[t], k = j % Ns;
+        int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) F.buf[fidx(F, idxD + r * Ns, ll[t])] = v[t][r];
+    }
+    __syncthreads();
+}
+
+// Full transform; `plan` radices multiply to N.  MAXC bounds N*L/blockDim.
+template <int MAXC>
+__device__ void fft_run(const FftCtx& F, const FftPlan& plan)
+{
+    int Ns = 1;
+    for (int s = 0; s < plan.nstages; s++) {
+        int R = plan.radix[s];
+        switch (R) {
+        case 2: fft_stage<2, MAXC / 2>(F, Ns); break;
+        case 3: fft_stage<3, MAXC / 3 + 1>(F, Ns); break;
+        case 4: fft_stage<4, MAXC / 4>(F, Ns); break;
+        case 5: fft_stage<5, MAXC / 5 + 1>(F, Ns); break;
+        default: fft_stage<8, MAXC / 8>(F, Ns); break;
+        }
+        Ns *= R;
+    }
+}
+
+constexpr int FFT_L = 8;        // lines per block (x transforms: 8 consecutive j)
+constexpr int FFT_THREADS = 256;
+constexpr int FFT_MAXC = 16;    // N * L / threads for N <= 512
+
+// --------------------------------------------------------- divergence + x FFT
+
+
+template <int ORDER>
+__global__ void __launch_bounds__(FFT_THREADS) k_div_fftx(Geo G, DivArgs A)
+{
+    extern __shared__ double2 sbuf[];
+    const int k = GZ + blockIdx.y;
+    const int j0 = blockIdx.x * FFT_L;
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const double dx = G.dx, dy = G.dy, dzk = G.dz[k];
+    const double uc = A.mu ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
+    const bool corr = A.mu != nullptr;
+    auto I = [&](int kk, int i, int j) { return ((long long) kk * nx + i) * ny + j; };
+    const int kb = GZ - 1, kt = n2 - GZ - 1;
+    for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
+        int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
+        double d = 0.0;
+        if (j < ny) {
+            auto U = [&](int di) { double t = __ldg(A.u + I(k, wrapp(i + di, nx), j)); return corr ? t + uc : t; };
+            auto V = [&](int dj) { return __ldg(A.v + I(k, i, wrapp(j + dj, ny))); };
+            auto Wr = [&](int kk) { return __ldg(A.w + I(kk, i, j)); };
+            if (ORDER == 2) {
+                d = (U(0) - U(-1)) / dx + (V(0) - V(-1)) / dy + (Wr(k) - Wr(k - 1)) / dzk;
+            } else {
+                double wkm2 = (k - 2 == kb - 1) ? 2.0 * Wr(kb) - Wr(kb + 1) : Wr(k - 2);  // pressure.c:80-87
+                double wkp1 = (k + 1 == kt + 1) ? 2.0 * Wr(kt) - Wr(kt - 1) : Wr(k + 1);  // pressure.c:88-95
+                d = (A1 * (U(0) - U(-1)) + A2 * (U(1) - U(-2))) / dx
+                  + (A1 * (V(0) - V(-1)) + A2 * (V(1) - V(-2))) / dy
+                  + (A1 * (Wr(k) - Wr(k - 1)) + A2 * (wkp1 - wkm2)) / dzk;
+            }
+        }
+        sbuf[i * FFT_L + jj] = make_double2(d, 0.0);
+    }
+    __syncthreads();
+    FftCtx F{sbuf, nx, FFT_L, false, -1, A.px.tw, A.c8};
+    fft_run<FFT_MAXC>(F, A.px);
+    const int nkx = G.nkx;
+    const double scale = 1.0 / (double) nx;
+    for (int idx = threadIdx.x; idx < nkx * FFT_L; idx += blockDim.x) {
+        int kx = idx / FFT_L, jj = idx - kx * FFT_L, j = j0 + jj;
+        if (j >= ny) continue;
+        double2 t = sbuf[kx * FFT_L + jj];
+        t.x *= scale;
+        t.y *= scale;
+        A.spec[((long long) k * nkx + kx) * ny + j] = t;
+    }
+}
+
+// ------------------------------------------------------------------ y FFT
+
+
+__global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
+{
+    extern __shared__ double2 sbuf[];
+    const int k = A.kfirst + blockIdx.y;
+    const int kx0 = blockIdx.x * FFT_L;
+    const int ny = G.ny, nkx = G.nkx;
+    const int nl = min(FFT_L, nkx - kx0);
+    double2* base = A.spec + ((long long) k * nkx + kx0) * ny;
+    for (int idx = threadIdx.x; idx < FFT_L * ny; idx += blockDim.x) {
+        int line = idx / ny;
+        sbuf[idx] = line < nl ? base[idx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    FftCtx F{sbuf, ny, FFT_L, true, A.sign, A.py.tw, A.c8};
+    fft_run<FFT_MAXC>(F, A.py);
+    const double scale = 1.0 / (double) ny;
+    for (int idx = threadIdx.x; idx < nl * ny; idx += blockDim.x) {
+        double2 t = sbuf[idx];
+        if (A.sign < 0) { t.x *= scale; t.y *= scale; }
+        base[idx] = t;
+    }
+}
+
+// ---------------------------------------------------------- inverse x FFT
+
+
+__global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
+{
+    extern __shared__ double2 sbuf[];
+    const int k = blockIdx.y;
+    const int j0 = blockIdx.x * FFT_L;
+    const int nx = G.nx, ny = G.ny, nkx = G.nkx;
+    for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
+        int pos = idx / FFT_L, jj = idx - pos * FFT_L, j = j0 + jj;
+        double2 t = make_double2(0.0, 0.0);
+        if (j < ny) {
+            if (pos < nkx) {
+                t = A.spec[((long long) k * nkx + pos) * ny + j];
+                if (pos == 0 || 2 * pos == nx) t.y = 0.0;
+            } else {
+                t = A.spec[((long long) k * nkx + (nx - pos)) * ny + j];
+                t.y = -t.y;
+            }
+        }
+        sbuf[pos * FFT_L + jj] = t;
+    }
+    __syncthreads();
+    FftCtx F{sbuf, nx, FFT_L, false, +1, A.px.tw, A.c8};
+    fft_run<FFT_MAXC>(F, A.px);
+    for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
+        int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
+        if (j < ny) A.p[((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
+    }
+}
+
+// ------------------------------------------------------------ Poisson in z
+
+
+template <int ORDER>
+__device__ __forceinline__ void fill_bot(const WallRowsD& R, double x0, double x1, double x2,
+                                         double& g1, double& g2, double& g3)
+{
+    // ghost_fill_bot{2,4} with r = 0 (pressure.c:516-522, 728-747)
+    if (ORDER == 2) {
+        g1 = (R.row[0][2] * x0 - 0.0) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (R.row[2][6] * x0) / -R.row[2][5];
+        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0 + R.row[1][6] * x1 - 0.0) / -R.row[1][3];
+        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1
+              + R.row[0][6] * x2) / -R.row[0][1];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void fill_top(const WallRowsD& R, double x0, double x1, double x2,
+                                         double& g1, double& g2, double& g3)
+{
+    // ghost_fill_top{2,4} with r = 0 (pressure.c:525-531, 750-769)
+    if (ORDER == 2) {
+        g1 = (R.row[0][0] * x0 - 0.0) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (R.row[2][0] * x0) / -R.row[2][1];
+        g2 = (R.row[1][0] * x1 + R.row[1][1] * x0 + R.row[1][2] * g1 - 0.0) / -R.row[1][3];
+        g3 = (R.row[0][0] * x2 + R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1
+              + R.row[0][4] * g2) / -R.row[0][5];
+    }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_poisson(Geo G, PoissonArgs A)
+{
+    const long long ncol = G.splane;
+    const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int ny = G.ny, n2 = G.n2, nz = G.nz;
+    const int kx = (int) (col / ny), ky = (int) (col - (long long) kx * ny);
+    const int var = (kx == 0 && ky == 0) ? 1 : 0;   // pressure.c:331-338
+    const double lamx = A.lamx[kx], lamy = A.lamy[ky];
+    double2* sp = A.spec;
+    auto S = [&](int k) -> double2& { return sp[(long long) k * ncol + col]; };
+    auto bq = [&](int i) { return i < 3 ? i : (i >= nz - 3 ? 6 - (nz - i) : -1); };
+
+    // Coefficients of interior row i (k = GZ + i) for this column.
+    auto coef = [&](int i, double* cf) {
+        const int k = GZ + i;
+        const int q = bq(i);
+        const double dv = A.dvol[k];
+        double d = (A.dpart[k] - lamx * dv * A.dt / A.dxdx) - lamy * dv * A.dt / A.dydy;
+        if (q >= 0) {
+            d = ((d - A.dsub[var][q][0]) - A.dsub[var][q][1]) - A.dsub[var][q][2];
+            for (int t = 0; t < 7; t++) cf[t] = A.red[var][q][t];
+        } else {
+            cf[0] = A.a[k]; cf[1] = A.b[k]; cf[2] = A.c[k];
+            cf[4] = A.e[k]; cf[5] = A.f[k]; cf[6] = A.g[k];
+        }
+        cf[3] = d;
+    };
+
+    if (ORDER == 2) {
+        // tridag.c:4-26; the diagonal is cf[1] for the 3-band rows
+        double* gam = A.scratch;
+        double cfv[7];
+        coef(0, cfv);
+        double bet = cfv[3];
+        double2 r0 = S(GZ);
+        double2 u = make_double2(r0.x * A.dvol[GZ] / bet, r0.y * A.dvol[GZ] / bet);
+        S(GZ) = u;
+        double cprev = cfv[2];
+        for (int i = 1; i < nz; i++) {
+            const int k = GZ + i;
+            coef(i, cfv);
+            double gm = cprev / bet;
+            bet = cfv[3] - cfv[0] * gm;
+            gam[(long long) k * ncol + col] = gm;
+            double2 r = S(k);
+            double rx = r.x * A.dvol[k], ry = r.y * A.dvol[k];
+            u = make_double2((rx - cfv[0] * u.x) / bet, (ry - cfv[0] * u.y) / bet);
+            S(k) = u;
+            cprev = cfv[2];
+        }
+        double2 nxt = u;
+        double2 top1 = u, top2 = u, top3 = u;
+        double2 b0 = u, b1v = u, b2v = u;
+        for (int i = nz - 2; i >= 0; i--) {
+            const int k = GZ + i;
+            double gm = gam[(long long) (k + 1) * ncol + col];
+            double2 t = S(k);
+            t.x -= gm * nxt.x;
+            t.y -= gm * nxt.y;
+            S(k) = t;
+            nxt = t;
+            if (i == nz - 2) top2 = t;
+            if (i == 1) b1v = t;
+            if (i == 0) b0 = t;
+        }
+        (void) top3; (void) b2v;
+        if (nz == 1) b0 = top1;
+        double g1, g2, g3;
+        fill_bot<2>(A.bot[var], b0.x, 0.0, 0.0, g1, g2, g3);
+        double h1;
+        fill_bot<2>(A.bot[var], b0.y, 0.0, 0.0, h1, g2, g3);
+        S(GZ - 1) = make_double2(g1, h1);
+        fill_top<2>(A.top, top1.x, 0.0, 0.0, g1, g2, g3);
+        fill_top<2>(A.top, top1.y, 0.0, 0.0, h1, g2, g3);
+        S(n2 - GZ) = make_double2(g1, h1);
+        for (int k = 0; k < GZ - 1; k++) S(k) = make_double2(0.0, 0.0);
+        for (int k = n2 - GZ + 1; k < n2; k++) S(k) = make_double2(0.0, 0.0);
+        (void) b1v; (void) top2;
+        return;
+    }
+
+    // heptdag.c:5-61 with per-column pivots; p, q, r spill to scratch
+    double* Pp = A.scratch;
+    double* Qp = A.scratch + (long long) n2 * ncol;
+    double* Rp = A.scratch + 2 * (long long) n2 * ncol;
+    auto at = [&](double* base, int k) -> double& { return base[(long long) k * ncol + col]; };
+    double p3 = 0, q3 = 0, r3 = 0, p2 = 0, q2 = 0, r2 = 0, p1 = 0, q1 = 0, r1 = 0;   // rows i-3, i-2, i-1
+    double2 s3 = make_double2(0, 0), s2 = s3, s1 = s3;
+    double cf[7];
+    for (int i = 0; i < nz; i++) {
+        const int k = GZ + i;
+        coef(i, cf);
+        const double a = cf[0], b = cf[1], c = cf[2], d = cf[3], e = cf[4], f = cf[5], g = cf[6];
+        double2 h = S(k);
+        const double dv = A.dvol[k];
+        h.x = h.x * dv;
+        h.y = h.y * dv;
+        double den, p, q, r;
+        double2 s;
+        if (i == 0) {
+            den = d;
+            p = e / den; q = f / den; r = g / den;
+            s = make_double2(h.x / den, h.y / den);
+        } else if (i == 1) {
+            den = d - c * p1;
+            p = (e - c * q1) / den; q = (f - c * r1) / den; r = (g) / den;
+            s = make_double2((h.x - c * s1.x) / den, (h.y - c * s1.y) / den);
+        } else if (i == 2) {
+            double bet = c - b * p2;
+            den = d - b * q2 - bet * p1;
+            p = (e - b * r2 - bet * q1) / den; q = (f - bet * r1) / den; r = (g) / den;
+            s = make_double2((h.x - b * s2.x - bet * s1.x) / den, (h.y - b * s2.y - bet * s1.y) / den);
+        } else {
+            double alp = b - a * p3;
+            double bet = c - a * q3 - alp * p2;
+            den = d - a * r3 - alp * q2 - bet * p1;
+            p = (e - alp * r2 - bet * q1) / den;
+            q = (f - bet * r1) / den;
+            r = (g) / den;
+            s = make_double2((h.x - a * s3.x - alp * s2.x - bet * s1.x) / den,
+                             (h.y - a * s3.y - alp * s2.y - bet * s1.y) / den);
+        }
+        at(Pp, k) = p; at(Qp, k) = q; at(Rp, k) = r;
+        S(k) = s;
+        p3 = p2; q3 = q2; r3 = r2; p2 = p1; q2 = q1; r2 = r1; p1 = p; q1 = q; r1 = r;
+        s3 = s2; s2 = s1; s1 = s;
+    }
+    // back substitution (heptdag.c:50-55)
+    double2 x1 = S(GZ + nz - 1), x2 = make_double2(0, 0), x3 = x2;
+    double2 tp[3], bt[3];
+    tp[0] = x1;
+    for (int i = nz - 2; i >= 0; i--) {
+        const int k = GZ + i;
+        double2 sv = S(k);
+        double p = at(Pp, k), q = at(Qp, k), r = at(Rp, k);
+        double2 xv;
+        if (i == nz - 2) {
+            xv = make_double2(sv.x - p * x1.x, sv.y - p * x1.y);
+        } else if (i == nz - 3) {
+            xv = make_double2(sv.x - p * x1.x - q * x2.x, sv.y - p * x1.y - q * x2.y);
+        } else {
+            xv = make_double2(sv.x - p * x1.x - q * x2.x - r * x3.x, sv.y - p * x1.y - q * x2.y - r * x3.y);
+        }
+        S(k) = xv;
+        x3 = x2; x2 = x1; x1 = xv;
+        if (i >= nz - 3) tp[nz - 1 - i] = xv;
+        if (i < 3) bt[i] = xv;
+    }
+    double g1, g2, g3, h1, h2, h3;
+    fill_bot<4>(A.bot[var], bt[0].x, bt[1].x, bt[2].x, g1, g2, g3);
+    fill_bot<4>(A.bot[var], bt[0].y, bt[1].y, bt[2].y, h1, h2, h3);
+    S(GZ - 1) = make_double2(g1, h1);
+    S(GZ - 2) = make_double2(g2, h2);
+    S(GZ - 3) = make_double2(g3, h3);
+    fill_top<4>(A.top, tp[0].x, tp[1].x, tp[2].x, g1, g2, g3);
+    fill_top<4>(A.top, tp[0].y, tp[1].y, tp[2].y, h1, h2, h3);
+    S(n2 - GZ) = make_double2(g1, h1);
+    S(n2 - GZ + 1) = make_double2(g2, h2);
+    S(n2 - GZ + 2) = make_double2(g3, h3);
+}
+
+// ------------------------------------------------------------ projection
+
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (j >= G.ny || i >= G.nx) return;
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    auto I = [&](int kk, int ii, int jj) {
+        return ((long long) kk * nx + wrapp(ii, nx)) * ny + wrapp(jj, ny);
+    };
+    const long long ijk = I(k, i, j);
+    const double* __restrict__ p = A.p;
+    const double dt = A.dt;
+    const bool inner = k >= GZ && k < n2 - GZ;
+    double u = A.u[ijk];
+    if (A.mu) u = u + A.gu[k] * (*A.mu);      // chanfast.c:516-519
+    if (inner) {
+        double up1h;
+        if (ORDER == 2) up1h = __ldg(p + I(k, i + 1, j)) - __ldg(p + ijk);
+        else up1h = A1 * (__ldg(p + I(k, i + 1, j)) - __ldg(p + ijk)) + A2 * (__ldg(p + I(k, i + 2, j)) - __ldg(p + I(k, i - 1, j)));
+        u = u - up1h * dt / G.dx;
+        double vp1h;
+        if (ORDER == 2) vp1h = __ldg(p + I(k, i, j + 1)) - __ldg(p + ijk);
+        else vp1h = A1 * (__ldg(p + I(k, i, j + 1)) - __ldg(p + ijk)) + A2 * (__ldg(p + I(k, i, j + 2)) - __ldg(p + I(k, i, j - 1)));
+        A.v[ijk] = A.v[ijk] - vp1h * dt / G.dy;
+    }
+    A.u[ijk] = u;
+    if (k >= GZ - 1 && k < n2 - GZ) {
+        double wp1h;
+        if (ORDER == 2) wp1h = __ldg(p + I(k + 1, i, j)) - __ldg(p + ijk);
+        else wp1h = A1 * (__ldg(p + I(k + 1, i, j)) - __ldg(p + ijk)) + A2 * (__ldg(p + I(k + 2, i, j)) - __ldg(p + I(k - 1, i, j)));
+        A.w[ijk] = A.w[ijk] - wp1h * dt / G.dzp1h[k];
+    }
+    if (A.mc) A.c[ijk] = A.c[ijk] + A.gc[k] * (*A.mc);   // chanfast.c:603-606
+}
+
+// -------------------------------------------------------------- launchers
+
+size_t fft_smem_bytes(int n) { return (size_t) n * FFT_L * sizeof(double2); }
+
+void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st)
+{
+    dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.nz);
+    size_t sm = fft_smem_bytes(G.nx);
+    if (G.order == 2) k_div_fftx<2><<<grd, FFT_THREADS, sm, st>>>(G, A);
+    else k_div_fftx<4><<<grd, FFT_THREADS, sm, st>>>(G, A);
+}
+
+void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st)
+{
+    dim3 grd((G.nkx + FFT_L - 1) / FFT_L, nrows);
+    k_ffty<<<grd, FFT_THREADS, fft_smem_bytes(G.ny), st>>>(G, A);
+}
+
+void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st)
+{
+    dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.n2);
+    k_fftx_c2r<<<grd, FFT_THREADS, fft_smem_bytes(G.nx), st>>>(G, A);
+}
+
+void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
+{
+    unsigned nb = (unsigned) ((G.splane + 127) / 128);
+    if (G.order == 2) k_poisson<2><<<nb, 128, 0, st>>>(G, A);
+    else k_poisson<4><<<nb, 128, 0, st>>>(G, A);
+}
+
+void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st)
+{
+    dim3 blk(32, 4, 1);
+    dim3 grd((G.ny + 31) / 32, (G.nx + 3) / 4, G.n2);
+    if (G.order == 2) k_project<2><<<grd, blk, 0, st>>>(G, A);
+    else k_project<4><<<grd, blk, 0, st>>>(G, A);
+}
+
+cudaError_t fft_set_smem_limits(int max_n)
+{
+    size_t sm = fft_smem_bytes(max_n);
+    cudaError_t e = cudaSuccess;
+    if (sm > 48 * 1024) {
+        int v = (int) sm;
+        e = cudaFuncSetAttribute(k_div_fftx<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    }
+    return e;
+}
+
+}  // namespace cf

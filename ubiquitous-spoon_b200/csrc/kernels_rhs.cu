@@ -1,0 +1,374 @@
+// Explicit right-hand side of the RK3 substep and the wall ghost refresh.
+//
+// k_ghosts:  apply_bc_u{2,4} / apply_bc_w{2,4} of chanfast.c:404-418 for
+//            every column, plus the in-place wall rewrite that
+//            massflux{x,y,z}4 performs before the advection (advect.c:100-131).
+// k_rhs:     fused massflux{x,y,z} + advect{u,v,w} + add_laplacexy_operator
+//            + flux_quick + advect_scalar + add_buoyancy
+//            (chanfast.c:420-452 / 1344-1376) for every interior point; mass
+//            fluxes are formed on the fly and never stored.  Expressions keep
+//            the reference's evaluation order (compiled with -fmad=false).
+#include "engine.cuh"
+#include "host_band.h"
+
+namespace cf {
+
+__device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+
+// ------------------------------------------------------------------ ghosts
+
+template <int ORDER>
+__device__ __forceinline__ void bc_u_bot(const WallRowsD& R, double bc, double x0, double x1, double x2,
+                                         double& g1, double& g2, double& g3)
+{
+    // ghost_fill_bot{2,4} (diffuseu.c:687-693, 899-918): rows k = gz-1, k-1, k-2
+    if (ORDER == 2) {
+        g1 = (R.row[0][2] * x0 - bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (R.row[2][6] * x0) / -R.row[2][5];
+        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0 + R.row[1][6] * x1 - bc) / -R.row[1][3];
+        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1
+              + R.row[0][6] * x2) / -R.row[0][1];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void bc_u_top(const WallRowsD& R, double bc, double x0, double x1, double x2,
+                                         double& g1, double& g2, double& g3)
+{
+    // ghost_fill_top{2,4} (diffuseu.c:696-702, 921-940); x0 = x[kt-1], x1 = x[kt-2], x2 = x[kt-3]
+    if (ORDER == 2) {
+        g1 = (R.row[0][0] * x0 - bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (R.row[2][0] * x0) / -R.row[2][1];
+        g2 = (R.row[1][0] * x1 + R.row[1][1] * x0 + R.row[1][2] * g1 - bc) / -R.row[1][3];
+        g3 = (R.row[0][0] * x2 + R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1
+              + R.row[0][4] * g2) / -R.row[0][5];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void bc_w_bot(const WallRowsD& R, double bc, double x0, double x1,
+                                         double& g1, double& g2, double& g3)
+{
+    // diffusew.c:667-680 (order 2), 849-865 (order 4); x0 = w[gz], x1 = w[gz+1]
+    if (ORDER == 2) {
+        g1 = (-bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (-bc) / -R.row[2][5];
+        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0) / -R.row[1][3];
+        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1) / -R.row[0][1];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void bc_w_top(const WallRowsD& R, double bc, double x0, double x1,
+                                         double& g1, double& g2, double& g3)
+{
+    // x0 = w[kt-1], x1 = w[kt-2] with kt = n2-gz-1 the top wall face
+    if (ORDER == 2) {
+        g1 = (-bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (-bc) / -R.row[2][1];
+        g2 = (R.row[1][1] * x0 + R.row[1][2] * g1) / -R.row[1][3];
+        g3 = (R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1 + R.row[0][4] * g2) / -R.row[0][5];
+    }
+}
+
+
+// One thread per column: wall ghost rows of u, v, c (apply_bc_u) and w
+// (apply_bc_w, then the massflux4 extrapolation of advect.c:100-131).
+template <int ORDER>
+__global__ void k_ghosts(Geo G, GhostArgs A)
+{
+    long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= G.plane) return;
+    const long long P = G.plane;
+    const int n2 = G.n2, kb = GZ - 1, kt = n2 - GZ;
+    auto at = [&](double* f, int k) -> double& { return f[(long long) k * P + col]; };
+    double* uf[3] = {A.F.u, A.F.v, A.F.c};
+    double bcb[3] = {A.bc_u, A.bc_v, A.bc_c_bot};
+    double bct[3] = {A.bc_u, A.bc_v, A.bc_c_top};
+    for (int q = 0; q < 3; q++) {
+        double* f = uf[q];
+        double g1, g2, g3;
+        bc_u_bot<ORDER>(A.ub, bcb[q], at(f, kb + 1), at(f, kb + 2), at(f, kb + 3), g1, g2, g3);
+        at(f, kb) = g1;
+        if (ORDER == 4) { at(f, kb - 1) = g2; at(f, kb - 2) = g3; }
+        bc_u_top<ORDER>(A.ut, bct[q], at(f, kt - 1), at(f, kt - 2), at(f, kt - 3), g1, g2, g3);
+        at(f, kt) = g1;
+        if (ORDER == 4) { at(f, kt + 1) = g2; at(f, kt + 2) = g3; }
+    }
+    double* w = A.F.w;
+    const int wt = n2 - GZ - 1;
+    double g1, g2, g3;
+    bc_w_bot<ORDER>(A.wb, A.bc_w, at(w, kb + 1), at(w, kb + 2), g1, g2, g3);
+    double top1, top2, top3;
+    bc_w_top<ORDER>(A.wt, A.bc_w, at(w, wt - 1), at(w, wt - 2), top1, top2, top3);
+    at(w, kb) = g1;
+    at(w, wt) = top1;
+    if (ORDER == 4) {
+        // massflux4 wall extrapolation (advect.c:108-109, 124-125)
+        at(w, kb - 1) = 2.0 * g1 - at(w, kb + 1);
+        at(w, kb - 2) = 2.0 * g1 - at(w, kb + 2);
+        at(w, wt + 1) = 2.0 * top1 - at(w, wt - 1);
+        at(w, wt + 2) = 2.0 * top1 - at(w, wt - 2);
+    }
+    (void) g2; (void) g3; (void) top2; (void) top3;
+}
+
+// --------------------------------------------------------------------- RHS
+
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_rhs(Geo G, RhsArgs A)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = GZ + blockIdx.z;
+    if (j >= G.ny || i >= G.nx) return;
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const double dx = G.dx, dy = G.dy, dxdy = G.dxdy;
+    const double* __restrict__ dz = G.dz;
+    const double* __restrict__ dydz = G.dydz;
+    const double* __restrict__ dxdz = G.dxdz;
+
+    auto I = [&](int di, int dj, int dk) -> long long {
+        return ((long long) (k + dk) * nx + wrapi(i + di, nx)) * ny + wrapi(j + dj, ny);
+    };
+    auto U = [&](int di, int dj, int dk) { return __ldg(A.u + I(di, dj, dk)); };
+    auto V = [&](int di, int dj, int dk) { return __ldg(A.v + I(di, dj, dk)); };
+    auto W = [&](int di, int dj, int dk) { return __ldg(A.w + I(di, dj, dk)); };
+    auto C = [&](int di, int dj, int dk) { return __ldg(A.c + I(di, dj, dk)); };
+    const long long ijk = I(0, 0, 0);
+    const double vol = dx * dy * dz[k];
+    const bool do_w = k < n2 - GZ - 1;
+    const int kb = GZ - 1, kt = n2 - GZ;   // wall ghost rows of cell-centred fields
+
+    double fu, fv, fw = 0.0, fc;
+
+    if (ORDER == 2) {
+        // massflux{x,y,z}2 (advect.c:6-85) formed on the fly
+        auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
+        auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
+        auto mx_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)); };
+        auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
+        auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
+        auto my_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)); };
+        auto mz_u = [&](int di, int dj, int dk) { return 0.5 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1)); };
+        auto mz_v = [&](int di, int dj, int dk) { return 0.5 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1)); };
+        auto mz_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)); };
+
+        {   // advectu2 (advect.c:286-350)
+            double q0 = U(0, 0, 0);
+            double xph = mx_u(0, 0, 0) * 0.5 * (q0 + U(1, 0, 0));
+            double yph = mx_v(0, 0, 0) * 0.5 * (q0 + U(0, 1, 0));
+            double zph = mx_w(0, 0, 0) * 0.5 * (q0 + U(0, 0, 1));
+            double xmh = mx_u(-1, 0, 0) * 0.5 * (q0 + U(-1, 0, 0));
+            double ymh = mx_v(0, -1, 0) * 0.5 * (q0 + U(0, -1, 0));
+            double zmh = mx_w(0, 0, -1) * 0.5 * (q0 + U(0, 0, -1));
+            if (k == n2 - GZ - 1) zph = mx_w(0, 0, 0) * (0.5 * (U(0, 0, kt - 1 - k) + U(0, 0, kt - k)));
+            if (k == GZ) zmh = mx_w(0, 0, -1) * (0.5 * (U(0, 0, kb - k) + U(0, 0, kb + 1 - k)));
+            fu = -((xph - xmh) + (yph - ymh) + (zph - zmh)) / vol;
+        }
+        {   // advectv2 (advect.c:353-417)
+            double q0 = V(0, 0, 0);
+            double xph = my_u(0, 0, 0) * 0.5 * (q0 + V(1, 0, 0));
+            double yph = my_v(0, 0, 0) * 0.5 * (q0 + V(0, 1, 0));
+            double zph = my_w(0, 0, 0) * 0.5 * (q0 + V(0, 0, 1));
+            double xmh = my_u(-1, 0, 0) * 0.5 * (q0 + V(-1, 0, 0));
+            double ymh = my_v(0, -1, 0) * 0.5 * (q0 + V(0, -1, 0));
+            double zmh = my_w(0, 0, -1) * 0.5 * (q0 + V(0, 0, -1));
+            if (k == n2 - GZ - 1) zph = my_w(0, 0, 0) * (0.5 * (V(0, 0, kt - 1 - k) + V(0, 0, kt - k)));
+            if (k == GZ) zmh = my_w(0, 0, -1) * (0.5 * (V(0, 0, kb - k) + V(0, 0, kb + 1 - k)));
+            fv = -((xph - xmh) + (yph - ymh) + (zph - zmh)) / vol;
+        }
+        if (do_w) {   // advectw2 (advect.c:420-463)
+            double q0 = W(0, 0, 0);
+            double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
+            double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
+            double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
+            double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
+            double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
+            double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
+            fw = -((xph - xmh) + (yph - ymh) + (zph - zmh)) / (dx * dy * G.dzp1h[k]);
+        }
+        // add_laplacexy_operator_{u,w}2 (diffuseu.c:286-313, diffusew.c:290-317)
+        auto lap2 = [&](auto F, double nu) {
+            double q0 = F(0, 0, 0);
+            return nu * (((F(1, 0, 0) - q0) / dx - (q0 - F(-1, 0, 0)) / dx) / dx
+                         + ((F(0, 1, 0) - q0) / dy - (q0 - F(0, -1, 0)) / dy) / dy);
+        };
+        fu += lap2(U, A.nu);
+        fv += lap2(V, A.nu);
+        if (do_w) fw += lap2(W, A.nu);
+    } else {
+        // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation
+        auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+            return B1 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)) + B2 * (d * U(di - 1, dj, dk) + d * U(di + 2, dj, dk)); };
+        auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+            return B1 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)) + B2 * (d * V(di - 1, dj, dk) + d * V(di + 2, dj, dk)); };
+        auto mx_w = [&](int di, int dj, int dk) {
+            return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
+        auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+            return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
+        auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+            return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
+        auto my_w = [&](int di, int dj, int dk) {
+            return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
+        auto mz_u = [&](int di, int dj, int dk) {
+            return B1 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1))
+                 + B2 * (dydz[k + dk - 1] * U(di, dj, dk - 1) + dydz[k + dk + 2] * U(di, dj, dk + 2)); };
+        auto mz_v = [&](int di, int dj, int dk) {
+            return B1 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1))
+                 + B2 * (dxdz[k + dk - 1] * V(di, dj, dk - 1) + dxdz[k + dk + 2] * V(di, dj, dk + 2)); };
+        auto mz_w = [&](int di, int dj, int dk) {
+            return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)) + B2 * (dxdy * W(di, dj, dk - 1) + dxdy * W(di, dj, dk + 2)); };
+
+        // advectu4 / advectv4 share their structure (advect.c:466-669); the
+        // wall-adjacent z fluxes use the 4th-order wall value qbc.
+        auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {
+            double q0 = Q(0, 0, 0);
+            double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
+            double yph = MY(0, 0, 0) * 0.5 * (q0 + Q(0, 1, 0));
+            double zph = MZ(0, 0, 0) * 0.5 * (q0 + Q(0, 0, 1));
+            double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
+            double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
+            double zmh = MZ(0, 0, -1) * 0.5 * (q0 + Q(0, 0, -1));
+            double xp3 = MX(1, 0, 0) * 0.5 * (q0 + Q(3, 0, 0));
+            double yp3 = MY(0, 1, 0) * 0.5 * (q0 + Q(0, 3, 0));
+            double zp3 = MZ(0, 0, 1) * 0.5 * (q0 + Q(0, 0, 3));
+            double xm3 = MX(-2, 0, 0) * 0.5 * (q0 + Q(-3, 0, 0));
+            double ym3 = MY(0, -2, 0) * 0.5 * (q0 + Q(0, -3, 0));
+            double zm3 = MZ(0, 0, -2) * 0.5 * (q0 + Q(0, 0, -3));
+            if (k >= n2 - GZ - 2 || k <= GZ + 1) {
+                double qbot = 0.5 * A2 * (Q(0, 0, kb - 1 - k) + Q(0, 0, kb + 2 - k))
+                            + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kb - k) + Q(0, 0, kb + 1 - k));
+                double qtop = 0.5 * A2 * (Q(0, 0, kt - 2 - k) + Q(0, 0, kt + 1 - k))
+                            + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kt - 1 - k) + Q(0, 0, kt - k));
+                if (k == n2 - GZ - 1) {
+                    zph = MZ(0, 0, 0) * qtop;
+                    zp3 = -MZ(0, 0, -1) * 0.5 * (Q(0, 0, -2) + Q(0, 0, 1)) + 2.0 * MZ(0, 0, 0) * qtop;
+                }
+                if (k == n2 - GZ - 2) zp3 = MZ(0, 0, 1) * qtop;
+                if (k == GZ) {
+                    zmh = MZ(0, 0, -1) * qbot;
+                    zm3 = -MZ(0, 0, 0) * 0.5 * (Q(0, 0, 2) + Q(0, 0, -1)) + 2.0 * MZ(0, 0, -1) * qbot;
+                }
+                if (k == GZ + 1) zm3 = MZ(0, 0, -2) * qbot;
+            }
+            return -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
+                     + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) / vol;
+        };
+        fu = adv_cell(U, mx_u, mx_v, mx_w);
+        fv = adv_cell(V, my_u, my_v, my_w);
+        if (do_w) {   // advectw4 (advect.c:672-734)
+            double q0 = W(0, 0, 0);
+            double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
+            double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
+            double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
+            double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
+            double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
+            double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
+            double xp3 = mz_u(1, 0, 0) * 0.5 * (q0 + W(3, 0, 0));
+            double yp3 = mz_v(0, 1, 0) * 0.5 * (q0 + W(0, 3, 0));
+            double zp3 = mz_w(0, 0, 1) * 0.5 * (q0 + W(0, 0, 3));
+            double xm3 = mz_u(-2, 0, 0) * 0.5 * (q0 + W(-3, 0, 0));
+            double ym3 = mz_v(0, -2, 0) * 0.5 * (q0 + W(0, -3, 0));
+            double zm3 = mz_w(0, 0, -2) * 0.5 * (q0 + W(0, 0, -3));
+            fw = -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
+                   + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) / (dx * dy * G.dzp1h[k]);
+        }
+        // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363)
+        auto lap4 = [&](auto F, double nu) {
+            double q0 = F(0, 0, 0);
+            double up3h = A1 * (F(2, 0, 0) - F(1, 0, 0)) + A2 * (F(3, 0, 0) - q0);
+            double up1h = A1 * (F(1, 0, 0) - q0) + A2 * (F(2, 0, 0) - F(-1, 0, 0));
+            double um1h = A1 * (q0 - F(-1, 0, 0)) + A2 * (F(1, 0, 0) - F(-2, 0, 0));
+            double um3h = A1 * (F(-1, 0, 0) - F(-2, 0, 0)) + A2 * (q0 - F(-3, 0, 0));
+            double vp3h = A1 * (F(0, 2, 0) - F(0, 1, 0)) + A2 * (F(0, 3, 0) - q0);
+            double vp1h = A1 * (F(0, 1, 0) - q0) + A2 * (F(0, 2, 0) - F(0, -1, 0));
+            double vm1h = A1 * (q0 - F(0, -1, 0)) + A2 * (F(0, 1, 0) - F(0, -2, 0));
+            double vm3h = A1 * (F(0, -1, 0) - F(0, -2, 0)) + A2 * (q0 - F(0, -3, 0));
+            return nu * ((A1 * (up1h / dx - um1h / dx) + A2 * (up3h / dx - um3h / dx)) / dx
+                         + (A1 * (vp1h / dy - vm1h / dy) + A2 * (vp3h / dy - vm3h / dy)) / dy);
+        };
+        fu += lap4(U, A.nu);
+        fv += lap4(V, A.nu);
+        if (do_w) fw += lap4(W, A.nu);
+    }
+
+    {   // flux_quick + advect_scalar (scalar.c:79-162), order independent
+        const double q = -0.125;
+        auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
+            double cph = 0.5 * (c0 + c1);
+            cph += m > 0.0 ? q * (c1 - 2.0 * c0 + cm1) : q * (c2 - 2.0 * c1 + c0);
+            return m * cph;
+        };
+        double c0 = C(0, 0, 0);
+        double fxp = quick(dydz[k] * U(0, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0), C(2, 0, 0));
+        double fxm = quick(dydz[k] * U(-1, 0, 0), C(-2, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0));
+        double fyp = quick(dxdz[k] * V(0, 0, 0), C(0, -1, 0), c0, C(0, 1, 0), C(0, 2, 0));
+        double fym = quick(dxdz[k] * V(0, -1, 0), C(0, -2, 0), C(0, -1, 0), c0, C(0, 1, 0));
+        double fzp = quick(dxdy * W(0, 0, 0), C(0, 0, -1), c0, C(0, 0, 1), C(0, 0, 2));
+        double fzm = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), c0, C(0, 0, 1));
+        fc = -((fxp - fxm) + (fyp - fym) + (fzp - fzm)) / vol;
+        if (ORDER == 2) {
+            double nu = A.kappa;
+            fc += nu * (((C(1, 0, 0) - c0) / dx - (c0 - C(-1, 0, 0)) / dx) / dx
+                        + ((C(0, 1, 0) - c0) / dy - (c0 - C(0, -1, 0)) / dy) / dy);
+        } else {
+            double up3h = A1 * (C(2, 0, 0) - C(1, 0, 0)) + A2 * (C(3, 0, 0) - c0);
+            double up1h = A1 * (C(1, 0, 0) - c0) + A2 * (C(2, 0, 0) - C(-1, 0, 0));
+            double um1h = A1 * (c0 - C(-1, 0, 0)) + A2 * (C(1, 0, 0) - C(-2, 0, 0));
+            double um3h = A1 * (C(-1, 0, 0) - C(-2, 0, 0)) + A2 * (c0 - C(-3, 0, 0));
+            double vp3h = A1 * (C(0, 2, 0) - C(0, 1, 0)) + A2 * (C(0, 3, 0) - c0);
+            double vp1h = A1 * (C(0, 1, 0) - c0) + A2 * (C(0, 2, 0) - C(0, -1, 0));
+            double vm1h = A1 * (c0 - C(0, -1, 0)) + A2 * (C(0, 1, 0) - C(0, -2, 0));
+            double vm3h = A1 * (C(0, -1, 0) - C(0, -2, 0)) + A2 * (c0 - C(0, -3, 0));
+            fc += A.kappa * ((A1 * (up1h / dx - um1h / dx) + A2 * (up3h / dx - um3h / dx)) / dx
+                             + (A1 * (vp1h / dy - vm1h / dy) + A2 * (vp3h / dy - vm3h / dy)) / dy);
+        }
+        // add_buoyancy{2,4} (scalar.c:6-76)
+        if (ORDER == 2) {
+            fu += 0.5 * (c0 + C(1, 0, 0)) * A.betg_x;
+            fv += 0.5 * (c0 + C(0, 1, 0)) * A.betg_y;
+            if (do_w) fw += 0.5 * (c0 + C(0, 0, 1)) * A.betg_z;
+        } else {
+            double cphx = B1 * (c0 + C(1, 0, 0)) + B2 * (C(-1, 0, 0) + C(2, 0, 0));
+            double cphy = B1 * (c0 + C(0, 1, 0)) + B2 * (C(0, -1, 0) + C(0, 2, 0));
+            fu += cphx * A.betg_x;
+            fv += cphy * A.betg_y;
+            if (do_w) fw += (B1 * (c0 + C(0, 0, 1)) + B2 * (C(0, 0, -1) + C(0, 0, 2))) * A.betg_z;
+        }
+    }
+    A.fu[ijk] = fu;
+    A.fv[ijk] = fv;
+    if (do_w) A.fw[ijk] = fw;
+    A.fc[ijk] = fc;
+}
+
+// ------------------------------------------------------------- launchers
+
+void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st)
+{
+    int th = 256;
+    long long nb = (G.plane + th - 1) / th;
+    if (G.order == 2) k_ghosts<2><<<(unsigned) nb, th, 0, st>>>(G, A);
+    else k_ghosts<4><<<(unsigned) nb, th, 0, st>>>(G, A);
+}
+
+void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st)
+{
+    dim3 blk(32, 4, 1);
+    dim3 grd((G.ny + 31) / 32, (G.nx + 3) / 4, G.nz);
+    if (G.order == 2) k_rhs<2><<<grd, blk, 0, st>>>(G, A);
+    else k_rhs<4><<<grd, blk, 0, st>>>(G, A);
+}
+
+}  // namespace cf

@@ -1,0 +1,298 @@
+// Implicit wall-normal diffusion: one thread per column.
+//
+// Per column this kernel does what chanfast.c:459-482 does for one field
+// (order 2; :1383-1406 order 4):
+//   h  = helmholtz1d_operator(x, nuadt) + gamdt*f + zetdt*g - hbc
+//   x  = solve_helmholtz1d(h, -nubdt)       (tridag.c / heptdag.c)
+//   apply_bc(x)
+// The band matrix is the same for every column, so its factorisation
+// (forward multipliers F1..F3, pivots DEN, back multipliers P, Q, R) comes
+// precomputed from host_band.cpp and only the right-hand side streams.  The
+// forward-substituted vector s is kept in the field's own storage between
+// the two sweeps.  With `partial` set, each warp also writes the sum of its
+// 32 columns for every row (input of get_xy_avg, get.c:281-302).
+#include "engine.cuh"
+#include "host_band.h"
+
+namespace cf {
+
+template <int ORDER>
+__device__ __forceinline__ void bcu_bot(const WallRowsD& R, double bc, double x0, double x1, double x2,
+                                        double& g1, double& g2, double& g3)
+{
+    if (ORDER == 2) {
+        g1 = (R.row[0][2] * x0 - bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (R.row[2][6] * x0) / -R.row[2][5];
+        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0 + R.row[1][6] * x1 - bc) / -R.row[1][3];
+        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1
+              + R.row[0][6] * x2) / -R.row[0][1];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void bcu_top(const WallRowsD& R, double bc, double x0, double x1, double x2,
+                                        double& g1, double& g2, double& g3)
+{
+    if (ORDER == 2) {
+        g1 = (R.row[0][0] * x0 - bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (R.row[2][0] * x0) / -R.row[2][1];
+        g2 = (R.row[1][0] * x1 + R.row[1][1] * x0 + R.row[1][2] * g1 - bc) / -R.row[1][3];
+        g3 = (R.row[0][0] * x2 + R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1
+              + R.row[0][4] * g2) / -R.row[0][5];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void bcw_bot(const WallRowsD& R, double bc, double x0, double x1,
+                                        double& g1, double& g2, double& g3)
+{
+    if (ORDER == 2) {
+        g1 = (-bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (-bc) / -R.row[2][5];
+        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0) / -R.row[1][3];
+        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1) / -R.row[0][1];
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void bcw_top(const WallRowsD& R, double bc, double x0, double x1,
+                                        double& g1, double& g2, double& g3)
+{
+    if (ORDER == 2) {
+        g1 = (-bc) / -R.row[0][1];
+        g2 = g3 = 0.0;
+    } else {
+        g1 = (-bc) / -R.row[2][1];
+        g2 = (R.row[1][1] * x0 + R.row[1][2] * g1) / -R.row[1][3];
+        g3 = (R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1 + R.row[0][4] * g2) / -R.row[0][5];
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int ORDER, bool IS_W, bool SHIFT>
+__global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
+{
+    const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = col < G.plane;
+    const long long P = G.plane;
+    const int n2 = G.n2;
+    const int kb = GZ - 1;                          // bottom wall ghost row / face
+    const int kt = IS_W ? n2 - GZ - 1 : n2 - GZ;    // top wall ghost row / face
+    const int n = A.fac.n, k0 = A.fac.k0;
+    double* __restrict__ x = A.x;
+    const double* __restrict__ dz = G.dz;
+    const long long cc = active ? col : 0;
+    auto ld = [&](const double* p, int k) { return p[(long long) k * P + cc]; };
+
+    // Old ghost values: cell fields carry apply_bc values already (k_ghosts);
+    // face fields recompute apply_bc_w here (k_ghosts stored the massflux4
+    // extrapolation there instead).
+    double gb[3], gt[3];
+    if (IS_W) {
+        bcw_bot<ORDER>(A.bcb, A.bc_bot, ld(x, kb + 1), ld(x, kb + 2), gb[0], gb[1], gb[2]);
+        bcw_top<ORDER>(A.bct, A.bc_top, ld(x, kt - 1), ld(x, kt - 2), gt[0], gt[1], gt[2]);
+    }
+    auto old = [&](int k) -> double {
+        if (IS_W) {
+            if (k <= kb) return gb[kb - k];
+            if (k >= kt) return gt[k - kt];
+        }
+        return ld(x, k);
+    };
+
+    constexpr int H = ORDER == 2 ? 1 : 3;
+    double win[2 * H + 1];  // old x at rows k-H .. k+H
+#pragma unroll
+    for (int q = 0; q < 2 * H + 1; q++) win[q] = old(k0 - H + q);
+
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    const double shift = SHIFT ? *A.gshift : 0.0;
+    for (int i = 0; i < n; i++) {
+        const int k = k0 + i;
+        double hv;
+        const double u0 = win[H];
+        if (ORDER == 2) {
+            if (!IS_W) {  // helmholtz1d_operator_u2 (diffuseu.c:121-131)
+                hv = u0 + A.nuadt * (((win[2] - u0) / G.dzp1h[k] - (u0 - win[0]) / G.dzm1h[k]) / dz[k]);
+            } else {      // helmholtz1d_operator_w2 (diffusew.c:121-132)
+                hv = u0 + A.nuadt * (((win[2] - u0) / dz[k + 1] - (u0 - win[0]) / dz[k]) / G.dzp1h[k]);
+            }
+        } else {
+            double wp3h = A1 * (win[5] - win[4]) + A2 * (win[6] - u0);
+            double wp1h = A1 * (win[4] - u0) + A2 * (win[5] - win[2]);
+            double wm1h = A1 * (u0 - win[2]) + A2 * (win[4] - win[1]);
+            double wm3h = A1 * (win[2] - win[1]) + A2 * (u0 - win[0]);
+            if (!IS_W)    // helmholtz1d_operator_u4 (diffuseu.c:149-169)
+                hv = u0 + A.nuadt * ((A1 * (wp1h / G.dzp1h[k] - wm1h / G.dzm1h[k])
+                                      + A2 * (wp3h / G.dzp3h[k] - wm3h / G.dzm3h[k])) / dz[k]);
+            else          // helmholtz1d_operator_w4 (diffusew.c:150-171)
+                hv = u0 + A.nuadt * ((A1 * (wp1h / dz[k + 1] - wm1h / dz[k])
+                                      + A2 * (wp3h / dz[k + 2] - wm3h / dz[k - 1])) / G.dzp1h[k]);
+        }
+        double gk = ld(A.g, k);
+        if (SHIFT) gk = gk + shift;   // f += mdpdx of the previous substep (chanfast.c:516-519)
+        hv = hv + (A.gamdt * ld(A.f, k) + A.zetdt * gk);
+        hv = hv - A.hbc[k];
+        const double r = hv * (IS_W ? G.dzp1h[k] : dz[k]);
+        double s;
+        if (ORDER == 2) s = (r - A.fac.F1[i] * s1) / A.fac.DEN[i];
+        else s = (((r - A.fac.F3[i] * s3) - A.fac.F2[i] * s2) - A.fac.F1[i] * s1) / A.fac.DEN[i];
+        s3 = s2; s2 = s1; s1 = s;
+        if (active) x[(long long) k * P + col] = s;
+#pragma unroll
+        for (int q = 0; q < 2 * H; q++) win[q] = win[q + 1];
+        win[2 * H] = (i + 1 < n) ? old(k + H + 1) : 0.0;
+    }
+
+    // back substitution
+    double y1 = 0.0, y2 = 0.0, y3 = 0.0;
+    double top[3] = {0, 0, 0}, bot[3] = {0, 0, 0};
+    const bool stats = A.partial != nullptr;
+    const long long wrow = ((long long) blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    for (int i = n - 1; i >= 0; i--) {
+        const int k = k0 + i;
+        double s = active ? x[(long long) k * P + col] : 0.0;
+        double y;
+        if (ORDER == 2) y = s - A.fac.P[i] * y1;
+        else y = ((s - A.fac.P[i] * y1) - A.fac.Q[i] * y2) - A.fac.R[i] * y3;
+        y3 = y2; y2 = y1; y1 = y;
+        if (active) x[(long long) k * P + col] = y;
+        if (i >= n - 3) top[n - 1 - i] = y;
+        if (i < 3) bot[i] = y;
+        if (stats) {
+            double t = warp_sum(active ? y : 0.0);
+            if ((threadIdx.x & 31) == 0) A.partial[wrow * n2 + k] = t;
+        }
+    }
+
+    // apply_bc after the solve (chanfast.c:481-482)
+    double b1, b2, b3, t1, t2, t3;
+    if (IS_W) {
+        bcw_bot<ORDER>(A.bcb, A.bc_bot, bot[0], bot[1], b1, b2, b3);
+        bcw_top<ORDER>(A.bct, A.bc_top, top[0], top[1], t1, t2, t3);
+    } else {
+        bcu_bot<ORDER>(A.bcb, A.bc_bot, bot[0], bot[1], bot[2], b1, b2, b3);
+        bcu_top<ORDER>(A.bct, A.bc_top, top[0], top[1], top[2], t1, t2, t3);
+    }
+    if (active) {
+        x[(long long) kb * P + col] = b1;
+        x[(long long) kt * P + col] = t1;
+        if (ORDER == 4) {
+            x[(long long) (kb - 1) * P + col] = b2;
+            x[(long long) (kb - 2) * P + col] = b3;
+            x[(long long) (kt + 1) * P + col] = t2;
+            x[(long long) (kt + 2) * P + col] = t3;
+        }
+    }
+    if (stats) {
+        // ghost rows as the reference holds them after apply_bc; rows the
+        // second-order closure does not touch are zero there.
+        for (int k = 0; k < n2; k++) {
+            if (k >= k0 && k < k0 + n) continue;
+            double v = 0.0;
+            if (k == kb) v = b1;
+            else if (k == kt) v = t1;
+            else if (ORDER == 4 && k == kb - 1) v = b2;
+            else if (ORDER == 4 && k == kb - 2) v = b3;
+            else if (ORDER == 4 && k == kt + 1) v = t2;
+            else if (ORDER == 4 && k == kt + 2) v = t3;
+            double t = warp_sum(active ? v : 0.0);
+            if ((threadIdx.x & 31) == 0) A.partial[wrow * n2 + k] = t;
+        }
+    }
+}
+
+// Row sums of the per-warp partials -> xy-average profile avg[k]
+// (get_xy_avg, get.c:281-302).  One block per row, fixed summation order.
+__global__ void k_row_average(const double* __restrict__ partial, long long nwarps, int n2,
+                              double scale, double* __restrict__ avg)
+{
+    __shared__ double red[256];
+    const int k = blockIdx.x;
+    double s = 0.0;
+    for (long long w = threadIdx.x; w < nwarps; w += blockDim.x) s += partial[w * n2 + k];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) avg[k] = red[0] * scale;
+}
+
+
+// Bulk-mean control of chanfast.c:485-529 (u) / 572-616 (c).
+__global__ void k_mass_control(MassArgs A)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double* avg = A.avg;
+    const double* dz = A.dz;
+    const int g = GZ, n2 = A.n2, nz = A.nz;
+    double a = 0.0, l = 0.0;  // get_z_avg (get.c:490-502)
+    for (int k = g; k < nz + g; k++) {
+        a += avg[k] * dz[k];
+        l += dz[k];
+    }
+    double s[4];
+    s[0] = a / l;
+    if (A.order == 4) {
+        s[1] = A.kappa * (A1 * (avg[g] - avg[g - 1]) + A2 * (avg[g + 1] - avg[g - 2])) / (0.5 * (dz[g] + dz[g - 1]));
+        s[2] = A.kappa * (A1 * (avg[n2 - g] - avg[n2 - g - 1]) + A2 * (avg[n2 - g + 1] - avg[n2 - g - 2]))
+               / (0.5 * (dz[n2 - g] + dz[n2 - g - 1]));
+    } else {
+        s[1] = A.kappa * (avg[g] - avg[g - 1]) / (0.5 * (dz[g] + dz[g - 1]));
+        s[2] = A.kappa * (avg[n2 - g] - avg[n2 - g - 1]) / (0.5 * (dz[n2 - g] + dz[n2 - g - 1]));
+    }
+    s[3] = nz % 2 == 0 ? 0.5 * (avg[g + nz / 2 - 1] + avg[g + nz / 2]) : avg[g + nz / 2];
+    double m = A.mode == 1 ? (A.target - s[0]) / A.green[0] : A.fixed;
+    for (int t = 0; t < 4; t++) s[t] += A.green[t] * m;
+    *A.m_out = m;
+    if (A.log_base) {
+        long long cnt = *A.counter;
+        double* row = A.log_base + (cnt % A.log_cap) * LOG_COLS + A.col;
+        row[0] = m;
+        row[1] = s[1];
+        row[2] = s[2];
+        row[3] = s[0];
+        row[4] = s[3];
+        if (A.advance) *A.counter = cnt + 1;
+    }
+}
+
+void launch_solve(const Geo& G, const SolveArgs& A, bool is_w, bool shift, cudaStream_t st)
+{
+    int th = 128;
+    unsigned nb = (unsigned) ((G.plane + th - 1) / th);
+#define CF_SOLVE(O, W, S) k_solve<O, W, S><<<nb, th, 0, st>>>(G, A)
+    if (G.order == 2) {
+        if (is_w) CF_SOLVE(2, true, false);
+        else if (shift) CF_SOLVE(2, false, true);
+        else CF_SOLVE(2, false, false);
+    } else {
+        if (is_w) CF_SOLVE(4, true, false);
+        else if (shift) CF_SOLVE(4, false, true);
+        else CF_SOLVE(4, false, false);
+    }
+#undef CF_SOLVE
+}
+
+void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st)
+{
+    long long nwarps = ((G.plane + 127) / 128) * 4;   // k_solve launches 128-thread blocks
+    double scale = 1.0 / ((double) G.nx * (double) G.ny);
+    k_row_average<<<G.n2, 256, 0, st>>>(partial, nwarps, G.n2, scale, avg);
+    k_mass_control<<<1, 32, 0, st>>>(M);
+}
+
+}  // namespace cf
