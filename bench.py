@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 point-substeps per second of the channel-flow RK3 substep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the large single instance, sized for one B200): order-4 chanfast4
+substep, grid nx = 512 (streamwise) x ny = 512 (spanwise) x nz = 384
+(wall-normal, cosine-stretched), box 2pi x pi x 2, Re_b = 20000 (nu = 1/20000,
+U_b = 1), dt = 2.5e-4, passive scalar Pr = 0.71, constant flow rate and scalar
+mean; initial state laminar Poiseuille + divergence-projected seeded
+perturbation (amplitude 0.05 U_cl, scalar noise 0.01), generated on the device.
+Synthetic data: there is no dataset.
+
+A bench step is one RK3 time step = 3 substeps; value = interior points x 3 x K
+(summed over ranks) / device time of the K steps (CUDA events on the instance
+stream, max over ranks).  With N > 1 every rank runs an independent replica
+(weak scaling, no collective on the data path).  Every field is 805 MB, far
+above the 126 MB L2, so no flush is needed between steps.
+
+--impl reference times the reference's own CPU implementation (the unmodified
+sources compiled by oracle/Makefile) on a bounded sample of the same workload
+on this host's cores; only rank 0 works.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import importlib
+import io
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # the large single instance (headline)
+    "config2": dict(name="chanfast4 512x512x384 Re_b=20000", order=4, nx=512, ny=512, nz=384,
+                    lx=2 * math.pi, ly=math.pi, lz=2.0, dt=2.5e-4, nu=1.0 / 20000.0, prandtl=0.71,
+                    seed=2, amp=0.05, c_amp=0.01, run_steps=50),
+    # mid size, used for profiling captures
+    "config1": dict(name="chanfast4 256x256x192 Re_b=10000", order=4, nx=256, ny=256, nz=192,
+                    lx=2 * math.pi, ly=math.pi, lz=2.0, dt=5e-4, nu=1.0 / 10000.0, prandtl=0.71,
+                    seed=1, amp=0.1, c_amp=0.01, run_steps=200),
+    # the reference's own CPU-runnable case
+    "config0": dict(name="chanfast2 64x64x64 Re_b=2800", order=2, nx=64, ny=64, nz=64,
+                    lx=4 * math.pi, ly=4 * math.pi / 3, lz=2.0, dt=1e-3, nu=1.0 / 2800.0, prandtl=1.0,
+                    seed=0, amp=0.1, c_amp=0.0, run_steps=100),
+}
+WORKLOAD = WORKLOADS["config2"]
+B_ALG = 240.0            # algorithmic HBM bytes per point-substep (whole substep)
+METRIC = "FP64 Mpt-substeps/s"
+# Minimal bytes per interior point of each kernel group (own inputs + outputs)
+KERNEL_BYTES = {"rhs": 64.0, "solve_u": 32.0, "solve_v": 32.0, "solve_c": 32.0, "solve_w": 32.0,
+                "div_fftx": 32.0, "ffty_fwd": 16.0, "poisson": 16.0, "ffty_bwd": 16.0,
+                "fftx_c2r": 16.0, "project": 72.0}
+# CPU-baseline sample: same order / nz / dt / viscosity, fewer x-y points per process
+CPU_SAMPLE = dict(nx=128, ny=128, substeps=2)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = [r for r in csv.reader(io.StringIO(getattr(self, "out", ""))) if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------ CPU reference
+
+def _ref_worker(args):
+    """One single-rank reference instance (oracle/_ref) on a sample grid."""
+    wname, nx, ny, nsub, warm, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import chanfast_np as cn
+    import ic
+    import ref
+    w = WORKLOADS[wname]
+    prm = cn.Params(order=w["order"], nx=nx, ny=ny, nz=w["nz"], lx=w["lx"], ly=w["ly"], lz=w["lz"],
+                    dt=w["dt"], nu=w["nu"], prandtl=w["prandtl"])
+    g = cn.Grid(prm)
+    R = ref.RefInstance(prm)
+    u, v, wf, c = ic.raw_state(prm, g.dz, seed, w["amp"], w["c_amp"])
+    for nm, a in zip("uvwc", (u, v, wf, c)):
+        R.set(nm, a)
+    R.project(1.0)
+    if warm:
+        R.substeps(warm)
+    t0 = time.perf_counter()
+    R.substeps(nsub)
+    dt = time.perf_counter() - t0
+    R.close()
+    return dt
+
+
+def cpu_reference(nsub, warm, nproc=None):
+    """Aggregate reference throughput on `nproc` independent single-rank
+    processes (one per core) -- Mpt-substeps/s."""
+    if nproc is None:
+        ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        try:
+            mem_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2 ** 30
+        except (ValueError, OSError):
+            mem_gb = 16.0
+        nproc = max(1, min(ncpu, int(mem_gb // 3), 64))
+    nx, ny = CPU_SAMPLE["nx"], CPU_SAMPLE["ny"]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(nproc) as pool:
+        wname = next(k for k, v in WORKLOADS.items() if v is WORKLOAD)
+        times = pool.map(_ref_worker, [(wname, nx, ny, nsub, warm, 100 + r) for r in range(nproc)])
+    pts = nx * ny * WORKLOAD["nz"]
+    value = sum(pts * nsub / t for t in times) / 1e6
+    sample = (f"unmodified reference chanfast{WORKLOAD['order']} substep (oracle/_ref, single-rank MPI/FFTW shims, "
+              f"gcc -O3 -funroll-loops) on {nproc} independent {nx}x{ny}x{WORKLOAD['nz']} instances, "
+              f"{nsub} timed substeps each after {warm} warm-up")
+    return value, nproc, sample, max(times)
+
+
+def ensure_reference():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available():
+        if os.path.isdir(ref.REFERENCE_SRC):
+            ref.build()
+        else:
+            return False
+    return True
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    cf = importlib.import_module("ubiquitous-spoon_b200")
+    w = WORKLOAD
+    cfg = cf.Config.make(order=w["order"], nx=w["nx"], ny=w["ny"], nz=w["nz"], lx=w["lx"], ly=w["ly"],
+                         lz=w["lz"], dt=w["dt"], nu=w["nu"], prandtl=w["prandtl"])
+    stream = torch.cuda.Stream()
+    inst = cf.Instance(cfg, stream=ctypes_stream(stream))
+    inst.init_fields(w["seed"] + rank, w["amp"], w["c_amp"])
+    inst.step_graph(args.warmup)
+    inst.sync()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        start.record(stream)
+        inst.step_graph(args.steps)
+        end.record(stream)
+        end.synchronize()
+        barrier()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pts = w["nx"] * w["ny"] * w["nz"]
+    substeps = 3 * args.steps
+    value = pts * substeps * world / (ms * 1e-3) / 1e6
+    ms_per_step = ms / args.steps
+
+    # per-kernel device times (CUDA events between the launch groups)
+    prof = inst.profile(3)
+    sub_ms = sum(prof.values()) / 3.0
+    peak, peak_kind = measured_peaks()
+    kernels = {}
+    for name, t in prof.items():
+        t1 = t / 3.0
+        nb = KERNEL_BYTES.get(name)
+        gbs = nb * pts / (t1 * 1e-3) / 1e9 if nb and t1 > 0 else None
+        kernels[name] = {"ms": round(t1, 4), "alg_bytes_per_pt": nb,
+                         "gbs": round(gbs, 1) if gbs else None,
+                         "frac": round(gbs / peak, 3) if gbs else None}
+    substep_ms = ms_per_step / 3.0
+    achieved = B_ALG * pts / (substep_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_per_substep.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("dram_bytes_per_substep_full_size")
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "whole RK3 substep (CUDA graph of 16 launches)",
+                "alg_bytes_per_unit": B_ALG, "unit_desc": "interior point-substep",
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "kernels": kernels, "profiled_substep_ms": round(sub_ms, 4)}
+
+    # end to end through the C ABI with host buffers: restart-style run of
+    # run_steps time steps, fields in and out in the reference layout
+    e2e = None
+    if not args.no_e2e:
+        shape = cfg.padded_shape()
+        host = {nm: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for nm in "uvwc"}
+        for nm in "uvwc":
+            inst.get_field(nm, out=host[nm])
+        nrun = w["run_steps"]
+        inst2 = cf.Instance(cfg, stream=ctypes_stream(stream))
+        barrier()
+        t0 = time.perf_counter()
+        for nm in "uvwc":
+            inst2.set_field(nm, host[nm])
+        inst2.step_graph(nrun)
+        for nm in "uvwc":
+            inst2.get_field(nm, out=host[nm])
+        barrier()
+        t_e2e = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([t_e2e], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        nbytes = 4 * host["u"].nbytes
+        e2e = {"value": round(pts * 3 * nrun * world / t_e2e / 1e6, 1), "unit": METRIC,
+               "h2d_bytes_per_step": nbytes // nrun, "d2h_bytes_per_step": nbytes // nrun,
+               "run_steps": nrun,
+               "how": "cf_set_field x4 (pinned host, reference padded layout) + cf_step_graph(run_steps) "
+                      "+ cf_get_field x4, wall clock, max over ranks"}
+        inst2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and ensure_reference():
+        v, nproc, sample, _ = cpu_reference(CPU_SAMPLE["substeps"], 1)
+        cpu = {"value": round(v, 3), "unit": METRIC, "cores": nproc, "kind": "reference", "sample": sample}
+
+    div = inst.max_divergence()
+    launches = inst.launches_per_substep() * substeps
+    inst.close()
+    result = {
+        "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["name"], "order": w["order"], "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
+                   "box": "2pi x pi x 2", "dt": w["dt"], "nu": w["nu"], "prandtl": w["prandtl"],
+                   "step": "one RK3 time step = 3 substeps",
+                   "l2": f"inputs larger than L2 ({pts * (w['nz'] + 6) // w['nz'] * 8 / 1e6:.0f} MB per field, "
+                         "4 fields read per kernel vs 126 MB L2); no flush",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single instance"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk.summary(), "max_divergence": div,
+    }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def ctypes_stream(torch_stream):
+    import ctypes
+    return ctypes.c_void_p(torch_stream.cuda_stream)
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    if not ensure_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "reference sources absent and oracle/_ref not built"}))
+        return
+    v, nproc, sample, tmax = cpu_reference(args.steps, args.warmup)
+    nx, ny = CPU_SAMPLE["nx"], CPU_SAMPLE["ny"]
+    ms_per_step = tmax / args.steps * 1e3
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": METRIC, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "order": WORKLOAD["order"], "nx": WORKLOAD["nx"], "ny": WORKLOAD["ny"],
+                   "nz": WORKLOAD["nz"], "step": f"one substep on each of {nproc} {nx}x{ny}x{WORKLOAD['nz']} "
+                   "sample instances in parallel"},
+        "cpu_baseline": {"value": round(v, 3), "unit": METRIC, "cores": nproc, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(v, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
+                    help="config2 (default) is the benchmark; the others serve profiling and checks")
+    args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.workload]
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

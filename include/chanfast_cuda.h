@@ -86,8 +86,9 @@ int cf_init_fields(cf_instance *inst, unsigned long long seed, double amp, doubl
  * right-hand sides persist across calls. */
 int cf_step(cf_instance *inst, int nsub);
 
-/* Same as cf_step, replaying a CUDA graph of one full RK3 step (3 substeps)
- * captured on first use; nsteps counts full steps. */
+/* Same as cf_step for nsteps full RK3 time steps, replaying a CUDA graph of
+ * two time steps (6 substeps) captured on first use; a leftover odd step and
+ * any substeps needed to reach the start of a time step run as cf_step. */
 int cf_step_graph(cf_instance *inst, int nsteps);
 
 /* Wait for all work of the instance. */
@@ -120,6 +121,16 @@ int cf_set_dt(cf_instance *inst, double dt);
  * for callers that keep data on the device. */
 int cf_device_field(cf_instance *inst, int field, double **dev_ptr, long long *n_elems);
 
+/* Run nsub substeps with CUDA events between the kernel groups on the
+ * instance stream and return the summed device time of each group (ms) in
+ * ms[CF_NKERNEL_GROUPS], in this order:
+ *   0 ghosts (apply_bc), 1 rhs, 2 solve u, 3 mass-flux control u, 4 solve v,
+ *   5 solve c, 6 scalar-mean control c, 7 solve w, 8 divergence + x FFT,
+ *   9 y FFT, 10 Poisson, 11 inverse y FFT, 12 inverse x FFT, 13 projection.
+ * Synchronises after every substep (timing only). */
+#define CF_NKERNEL_GROUPS 14
+int cf_profile(cf_instance *inst, int nsub, double *ms);
+
 /* Number of kernel launches the engine issues per substep. */
 int cf_launches_per_substep(const cf_instance *inst);
 
@@ -130,7 +141,7 @@ const char *cf_strerror(int status);
  * reference (chanfast.h:1-21, called at main.c:56-60); they read
  * outputdir/{u,v,w,c}_it<it>.dat, run nt - it time steps on the current
  * CUDA device, append outputdir/cfl.dat, pstat.dat and cstat.dat, and write
- * outputdir/{u,v,w,c,p}_it<N>.dat every istat steps.  p_row * p_col must be
+ * outputdir/{u,v,w,c}_it<N>.dat every istat steps.  p_row * p_col must be
  * 1.  The reference returns nothing and aborts on error; these print the
  * failing status to stderr and return.  chanfast2_status / chanfast4_status
  * return it instead.

@@ -25,6 +25,9 @@ CF_OK, CF_EINVAL, CF_ENOMEM, CF_ECUDA, CF_EPIVOT, CF_ENONFINITE, CF_EIO = 0, -1,
 FIELDS = {"u": 0, "v": 1, "w": 2, "c": 3, "p": 4}
 LAYOUT_PADDED, LAYOUT_INTERIOR = 0, 1
 LOG_COLS = 10
+KERNEL_GROUPS = ("ghosts", "rhs", "solve_u", "mass_u", "solve_v", "solve_c", "mass_c", "solve_w",
+                 "div_fftx", "ffty_fwd", "poisson", "ffty_bwd", "fftx_c2r", "project")
+NKERNEL_GROUPS = len(KERNEL_GROUPS)
 
 _lib = None
 _drv = None
@@ -93,6 +96,7 @@ def _bind(L):
     L.cf_set_dt.argtypes = [vp, ctypes.c_double]
     L.cf_device_field.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)]
     L.cf_launches_per_substep.argtypes = [vp]
+    L.cf_profile.argtypes = [vp, ip, dp]
     L.cf_strerror.restype = ctypes.c_char_p
     L.cf_strerror.argtypes = [ip]
     return L
@@ -173,9 +177,11 @@ class Instance:
         a = np.ascontiguousarray(array, dtype=np.float64).reshape(shape)
         _check(self.L.cf_set_field(self.h, FIELDS[name], _dp(a), layout), "cf_set_field")
 
-    def get_field(self, name, layout=LAYOUT_PADDED):
+    def get_field(self, name, layout=LAYOUT_PADDED, out=None):
         shape = self.cfg.padded_shape() if layout == LAYOUT_PADDED else self.cfg.interior_shape()
-        a = np.empty(shape)
+        a = np.empty(shape) if out is None else out
+        if a.shape != tuple(shape) or a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of the layout's shape")
         _check(self.L.cf_get_field(self.h, FIELDS[name], _dp(a), layout), "cf_get_field")
         return a
 
@@ -219,6 +225,12 @@ class Instance:
         n = ctypes.c_longlong()
         _check(self.L.cf_device_field(self.h, FIELDS[name], ctypes.byref(p), ctypes.byref(n)), "cf_device_field")
         return p.value, n.value
+
+    def profile(self, nsub):
+        """Per-kernel-group device time (ms, summed over nsub substeps)."""
+        ms = np.zeros(NKERNEL_GROUPS)
+        _check(self.L.cf_profile(self.h, nsub, _dp(ms)), "cf_profile")
+        return dict(zip(KERNEL_GROUPS, ms.tolist()))
 
     def launches_per_substep(self):
         return int(self.L.cf_launches_per_substep(self.h))

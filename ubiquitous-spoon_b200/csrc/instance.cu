@@ -405,7 +405,17 @@ PoissonArgs poisson_args(cf_instance* I, const PoissonOffsets& po, double pdt)
 // Divergence -> FFT -> Poisson -> inverse FFT -> projection with step `pdt`.
 // With `corr`, the lazily applied mass-flux corrections of substep set `s`
 // are folded in (divergence and projection read u + G_u * mdpdx, c + G_c * dcdt).
-void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr)
+// Optional per-kernel timing: events recorded after each launch group.
+struct Timeline {
+    cudaEvent_t ev[CF_NKERNEL_GROUPS + 1];
+    int n = 0;
+    void mark(cudaStream_t st) { cudaEventRecord(ev[n++], st); }
+};
+
+void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr,
+                       Timeline* tl = nullptr);
+void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr,
+                       Timeline* tl)
 {
     const Geo& G = I->geo;
     cudaStream_t st = I->stream;
@@ -413,13 +423,18 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     DivArgs D{I->u, I->v, I->w, corr ? b + I->set[s][0].green : nullptr, corr ? I->dscal : nullptr,
               I->spec, I->px, I->c8};
     launch_div_fftx(G, D, st);
+    if (tl) tl->mark(st);
     FftyArgs Y{I->spec, I->py, -1, GZ, I->c8};
     launch_ffty(G, Y, G.nz, st);
+    if (tl) tl->mark(st);
     launch_poisson(G, poisson_args(I, po, pdt), st);
+    if (tl) tl->mark(st);
     FftyArgs Yb{I->spec, I->py, +1, 0, I->c8};
     launch_ffty(G, Yb, G.n2, st);
+    if (tl) tl->mark(st);
     C2rArgs X{I->spec, I->p, I->px, I->c8};
     launch_fftx_c2r(G, X, st);
+    if (tl) tl->mark(st);
     ProjArgs P;
     P.u = I->u; P.v = I->v; P.w = I->w; P.c = I->c; P.p = I->p;
     P.gu = corr ? b + I->set[s][0].green : nullptr;
@@ -428,9 +443,10 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     P.mc = corr ? I->dscal + 1 : nullptr;
     P.dt = pdt;
     launch_project(G, P, st);
+    if (tl) tl->mark(st);
 }
 
-void enqueue_substep(cf_instance* I)
+void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
 {
     const cf_config& C = I->cfg;
     const Geo& G = I->geo;
@@ -447,11 +463,14 @@ void enqueue_substep(cf_instance* I)
     GA.bc_c_bot = -0.5;
     GA.bc_c_top = +0.5;
     GA.bc_w = 0.0;
+    if (tl) tl->mark(st);
     launch_ghosts(G, GA, st);
+    if (tl) tl->mark(st);
 
     RhsArgs R{I->u, I->v, I->w, I->c, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
               C.nu, C.nu / C.prandtl, C.betg_x, C.betg_y, C.betg_z};
     launch_rhs(G, R, st);
+    if (tl) tl->mark(st);
 
     const double nuadt = C.nu * RK3_ALP[s] * dt;
     const double gamdt = RK3_GAM[s] * dt;
@@ -479,6 +498,7 @@ void enqueue_substep(cf_instance* I)
         S.bct = is_w ? I->bc_wt : I->bc_ut;
         S.partial = stats ? I->partial : nullptr;
         launch_solve(G, S, is_w, S.gshift != nullptr, st);
+        if (tl) tl->mark(st);
         if (stats) {
             MassArgs M;
             M.avg = I->avg;
@@ -498,9 +518,10 @@ void enqueue_substep(cf_instance* I)
             M.col = q == 0 ? 0 : 5;
             M.advance = q == 2 ? 1 : 0;
             launch_mass(G, I->partial, I->avg, M, st);
+            if (tl) tl->mark(st);
         }
     }
-    pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true);
+    pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, tl);
     I->substep++;
 }
 
@@ -838,6 +859,32 @@ int cf_device_field(cf_instance* I, int field, double** dev_ptr, long long* n_el
     *dev_ptr = p;
     if (n_elems) *n_elems = I->geo.plane * I->geo.n2;
     return CF_OK;
+}
+
+int cf_profile(cf_instance* I, int nsub, double* ms)
+{
+    if (!I || !ms || nsub <= 0) return CF_EINVAL;
+    Timeline tl;
+    for (int g = 0; g <= CF_NKERNEL_GROUPS; g++) CF_CUDA(cudaEventCreate(&tl.ev[g]));
+    for (int g = 0; g < CF_NKERNEL_GROUPS; g++) ms[g] = 0.0;
+    int rc = CF_OK;
+    for (int q = 0; q < nsub && rc == CF_OK; q++) {
+        tl.n = 0;
+        enqueue_substep(I, &tl);
+        cudaError_t e = cudaStreamSynchronize(I->stream);
+        if (e != cudaSuccess || tl.n != CF_NKERNEL_GROUPS + 1) {
+            g_last_error = cudaGetErrorString(e);
+            rc = CF_ECUDA;
+            break;
+        }
+        for (int g = 0; g < CF_NKERNEL_GROUPS; g++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, tl.ev[g], tl.ev[g + 1]);
+            ms[g] += t;
+        }
+    }
+    for (int g = 0; g <= CF_NKERNEL_GROUPS; g++) cudaEventDestroy(tl.ev[g]);
+    return rc;
 }
 
 int cf_launches_per_substep(const cf_instance* I)
