@@ -39,7 +39,11 @@ struct Geo {
     const double* dzm3h;  // 0.5*(dz[k-2]+dz[k-1])
     const double* dydz;   // dy*dz[k]
     const double* dxdz;   // dx*dz[k]
+    const double* ivol;   // 1 / (dx*dy*dz[k])       cell volume
+    const double* ivolw;  // 1 / (dx*dy*dzp1h[k])    w-face volume
+    const double* idzp1h; // 1 / dzp1h[k]
     double dxdy;          // dx*dy
+    double idx, idy;      // 1/dx, 1/dy
 };
 
 // Line-solve factorisation on device (see host_band.h LineFactor).
@@ -54,9 +58,8 @@ struct SolveArgs {
     const double* f;      // current RHS
     const double* g;      // previous-stage RHS
     const double* gshift; // device scalar added to g (mass-flux lazily applied), or null
-    FactorD fac;
-    const double* hbc;    // [n2]
-    double nuadt, gamdt, zetdt;
+    FactorD fac;          // back-substitution multipliers P, Q, R; rows k0 .. k0+n-1
+    const double* rows;   // fused forward rows [n][fused_width] (host_band.h)
     double bc_bot, bc_top;
     WallRowsD bcb, bct;   // apply_bc closure rows for this field
     double* partial;      // per-warp row sums [nwarps][n2] or null
@@ -142,6 +145,7 @@ struct ProjArgs {
     const double *gu, *gc;          // Green's function columns (n2) or null
     const double *mu, *mc;          // device scalars mdpdx, dcdt or null
     double dt;                      // (alpha + beta) dt of the substep
+    double dtdx, dtdy;              // dt/dx, dt/dy
 };
 
 // ---------------------------------------------------------------- launchers
@@ -155,6 +159,7 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st);
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st);
 void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st);
 cudaError_t fft_set_smem_limits(int max_n);
+cudaError_t rhs_set_smem_limits();
 size_t fft_smem_bytes(int n);
 constexpr int FFT_MAX_N = 512;
 

@@ -3,6 +3,7 @@
 // evaluation order (x86-64 builds without FMA contraction).
 #include "host_band.h"
 
+#include <algorithm>
 #include <cmath>
 #include <stdexcept>
 
@@ -706,6 +707,43 @@ void solve_column(const ImplicitSet& s, const Metrics& m, bool is_w, std::vector
         else { u_fill_bot4(B, kb); u_fill_top4(B, kt); }
     }
     out = B.x;
+}
+
+std::vector<double> fused_rows(const Metrics& m, const ImplicitSet& s, bool is_w, double nuadt,
+                               double gamdt, double zetdt)
+{
+    const int H = m.order == 2 ? 1 : 3;
+    const int W = fused_width(m.order);
+    const int k0 = s.fac.k0, n = s.fac.n;
+    std::vector<double> L((size_t) n * (2 * H + 1), 0.0);
+    // The operator is linear: its coefficients are its response to unit columns.
+    std::vector<double> e(m.n2, 0.0), h(m.n2, 0.0);
+    for (int q = 0; q < m.n2; q++) {
+        std::fill(e.begin(), e.end(), 0.0);
+        std::fill(h.begin(), h.end(), 0.0);
+        e[q] = 1.0;
+        if (is_w) helmholtz_w_col(m, e, h, nuadt);
+        else helmholtz_u_col(m, e, h, nuadt);
+        for (int i = 0; i < n; i++) {
+            int k = k0 + i, off = q - k;
+            if (off >= -H && off <= H) L[(size_t) i * (2 * H + 1) + off + H] = h[k];
+        }
+    }
+    std::vector<double> rows((size_t) n * W, 0.0);
+    for (int i = 0; i < n; i++) {
+        int k = k0 + i;
+        double dvol = is_w ? 0.5 * (m.dz[k + 1] + m.dz[k]) : m.dz[k];
+        double iden = 1.0 / s.fac.DEN[i];
+        double* r = &rows[(size_t) i * W];
+        for (int t = 0; t < 2 * H + 1; t++) r[t] = dvol * L[(size_t) i * (2 * H + 1) + t] * iden;
+        r[2 * H + 1] = dvol * gamdt * iden;
+        r[2 * H + 2] = dvol * zetdt * iden;
+        r[2 * H + 3] = -dvol * s.hbc[k] * iden;
+        r[2 * H + 4] = s.fac.F1[i] * iden;
+        r[2 * H + 5] = s.fac.F2[i] * iden;
+        r[2 * H + 6] = s.fac.F3[i] * iden;
+    }
+    return rows;
 }
 
 PoissonSet make_poisson(const Metrics& m, double dt)

@@ -93,6 +93,15 @@ ImplicitSet make_implicit_u(const Metrics& m, double nubdt, double gamdt, double
                             double bc_top, double kappa, bool want_green);
 ImplicitSet make_implicit_w(const Metrics& m, double nubdt, double bc_bot, double bc_top);
 
+// Per-row coefficients of the fused forward sweep used on the device:
+//   s_i = sum_m cu_m x_{k+m} + cf f_k + cg g_k + c0 - f1 s_{i-1} - f2 s_{i-2} - f3 s_{i-3}
+// which is, up to rounding, ((H(nuadt) x + gamdt f + zetdt g - hbc) dvol - F.s) / DEN
+// (chanfast.c:469-482 with the forward half of tridag/heptdag).  Row i holds
+// [cu_{-H..H}, cf, cg, c0, f1, f2, f3] with H = 1 (order 2) or 3 (order 4).
+std::vector<double> fused_rows(const Metrics& m, const ImplicitSet& s, bool is_w, double nuadt,
+                               double gamdt, double zetdt);
+inline int fused_width(int order) { return (order == 2 ? 3 : 7) + 6; }
+
 // Solve one column with an ImplicitSet factorisation (host reference of the
 // device kernel; used for the Green's function and for tests).
 void solve_column(const ImplicitSet& s, const Metrics& m, bool is_w, std::vector<double>& rhs_h,

@@ -227,7 +227,7 @@ std::vector<int> fft_radices(int n)
 }  // namespace
 
 struct SetOffsets {
-    size_t F1, F2, F3, DEN, P, Q, R, hbc, green;
+    size_t F1, F2, F3, DEN, P, Q, R, hbc, green, rows;
     int k0, n;
     WallRowsD bot, top;
     double gstats[4];
@@ -298,7 +298,9 @@ int build_tables(cf_instance* I, double dt)
     const cf_config& C = I->cfg;
     const Metrics& m = I->m;
     Arena A;
-    auto addfac = [&](SetOffsets& so, const ImplicitSet& s) {
+    auto addfac = [&](SetOffsets& so, const ImplicitSet& s, bool is_w, double nuadt, double gamdt,
+                      double zetdt) {
+        so.rows = A.add(fused_rows(m, s, is_w, nuadt, gamdt, zetdt));
         so.k0 = s.fac.k0;
         so.n = s.fac.n;
         so.F1 = A.add(s.fac.F1); so.F2 = A.add(s.fac.F2); so.F3 = A.add(s.fac.F3);
@@ -319,10 +321,11 @@ int build_tables(cf_instance* I, double dt)
             ImplicitSet sv = make_implicit_u(m, nubdt, gamdt, 0.0 - vf, 0.0 - vf, C.nu, false);
             ImplicitSet sc = make_implicit_u(m, nubdt / C.prandtl, gamdt, -0.5, +0.5, C.nu / C.prandtl, true);
             ImplicitSet sw = make_implicit_w(m, nubdt, 0.0, 0.0);
-            addfac(I->set[s][0], su);
-            addfac(I->set[s][1], sv);
-            addfac(I->set[s][2], sc);
-            addfac(I->set[s][3], sw);
+            double nuadt = C.nu * RK3_ALP[s] * dt, zetdt = RK3_ZET[s] * dt;
+            addfac(I->set[s][0], su, false, nuadt, gamdt, zetdt);
+            addfac(I->set[s][1], sv, false, nuadt, gamdt, zetdt);
+            addfac(I->set[s][2], sc, false, nuadt / C.prandtl, gamdt, zetdt);
+            addfac(I->set[s][3], sw, true, nuadt, gamdt, zetdt);
         }
     } catch (const std::exception&) {
         g_last_error = "zero pivot in a line-solve factorisation";
@@ -349,8 +352,17 @@ int build_tables(cf_instance* I, double dt)
         dydz[k] = m.dy * m.dz[k];
         dxdz[k] = m.dx * m.dz[k];
     }
+    std::vector<double> ivol(n2, 0.0), ivolw(n2, 0.0), idzp1h(n2, 0.0);
+    for (int k = 0; k < n2; k++) {
+        ivol[k] = 1.0 / (m.dx * m.dy * m.dz[k]);
+        if (k + 1 < n2) {
+            ivolw[k] = 1.0 / (m.dx * m.dy * dzp1h[k]);
+            idzp1h[k] = 1.0 / dzp1h[k];
+        }
+    }
     size_t o_dz = A.add(m.dz), o_p1 = A.add(dzp1h), o_m1 = A.add(dzm1h), o_p3 = A.add(dzp3h),
-           o_m3 = A.add(dzm3h), o_dydz = A.add(dydz), o_dxdz = A.add(dxdz);
+           o_m3 = A.add(dzm3h), o_dydz = A.add(dydz), o_dxdz = A.add(dxdz), o_iv = A.add(ivol),
+           o_ivw = A.add(ivolw), o_idz = A.add(idzp1h);
     size_t o_zp = A.add(z_at_p(m));
 
     if (I->coef) { cudaFree(I->coef); I->coef = nullptr; }
@@ -359,7 +371,8 @@ int build_tables(cf_instance* I, double dt)
     double* b = I->coef;
     Geo& G = I->geo;
     G.dz = b + o_dz; G.dzp1h = b + o_p1; G.dzm1h = b + o_m1; G.dzp3h = b + o_p3; G.dzm3h = b + o_m3;
-    G.dydz = b + o_dydz; G.dxdz = b + o_dxdz;
+    G.dydz = b + o_dydz; G.dxdz = b + o_dxdz; G.ivol = b + o_iv; G.ivolw = b + o_ivw;
+    G.idzp1h = b + o_idz;
     I->lamx = b + o_lamx;
     I->lamy = b + o_lamy;
     I->zp = b + o_zp;
@@ -442,6 +455,8 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     P.mu = corr ? I->dscal : nullptr;
     P.mc = corr ? I->dscal + 1 : nullptr;
     P.dt = pdt;
+    P.dtdx = pdt / I->m.dx;
+    P.dtdy = pdt / I->m.dy;
     launch_project(G, P, st);
     if (tl) tl->mark(st);
 }
@@ -472,9 +487,6 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     launch_rhs(G, R, st);
     if (tl) tl->mark(st);
 
-    const double nuadt = C.nu * RK3_ALP[s] * dt;
-    const double gamdt = RK3_GAM[s] * dt;
-    const double zetdt = RK3_ZET[s] * dt;
     double* fields[4] = {I->u, I->v, I->c, I->w};
     const int fidx[4] = {0, 1, 3, 2};   // u, v, c, w -> f/g slots (u, v, w, c)
     double bcb[4] = {0.0 - C.setuframe, 0.0 - C.setvframe, -0.5, 0.0};
@@ -488,10 +500,7 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
         S.g = I->gbuf[fidx[q]];
         S.gshift = q == 0 ? I->dscal : (q == 2 ? I->dscal + 1 : nullptr);
         S.fac = factor_of(I, so);
-        S.hbc = I->coef + so.hbc;
-        S.nuadt = q == 2 ? nuadt / C.prandtl : nuadt;
-        S.gamdt = gamdt;
-        S.zetdt = zetdt;
+        S.rows = I->coef + so.rows;
         S.bc_bot = bcb[q];
         S.bc_top = bct[q];
         S.bcb = is_w ? I->bc_wb : I->bc_ub;
@@ -583,6 +592,8 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     G.dx = I->m.dx;
     G.dy = I->m.dy;
     G.dxdy = I->m.dx * I->m.dy;
+    G.idx = 1.0 / I->m.dx;
+    G.idy = 1.0 / I->m.dy;
     if (stream) {
         I->stream = (cudaStream_t) stream;
     } else {
@@ -632,6 +643,7 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     if (rc) return rc;
     I->c8 = std::cos(M_PI / 4.0);
     CF_CUDA(fft_set_smem_limits(std::max(C.nx, C.ny)));
+    CF_CUDA(rhs_set_smem_limits());
     I->bc_ub = to_dev(bc_rows_u(I->m, true));
     I->bc_ut = to_dev(bc_rows_u(I->m, false));
     I->bc_wb = to_dev(bc_rows_w(I->m, true));

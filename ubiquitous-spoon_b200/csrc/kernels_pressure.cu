@@ -341,20 +341,21 @@ __global__ void __launch_bounds__(128) k_poisson(Geo G, PoissonArgs A)
         double* gam = A.scratch;
         double cfv[7];
         coef(0, cfv);
-        double bet = cfv[3];
+        double ibet = 1.0 / cfv[3];
         double2 r0 = S(GZ);
-        double2 u = make_double2(r0.x * A.dvol[GZ] / bet, r0.y * A.dvol[GZ] / bet);
+        const double dv0 = A.dvol[GZ];
+        double2 u = make_double2(r0.x * dv0 * ibet, r0.y * dv0 * ibet);
         S(GZ) = u;
         double cprev = cfv[2];
         for (int i = 1; i < nz; i++) {
             const int k = GZ + i;
             coef(i, cfv);
-            double gm = cprev / bet;
-            bet = cfv[3] - cfv[0] * gm;
+            double gm = cprev * ibet;
+            ibet = 1.0 / (cfv[3] - cfv[0] * gm);
             gam[(long long) k * ncol + col] = gm;
             double2 r = S(k);
-            double rx = r.x * A.dvol[k], ry = r.y * A.dvol[k];
-            u = make_double2((rx - cfv[0] * u.x) / bet, (ry - cfv[0] * u.y) / bet);
+            const double dv = A.dvol[k];
+            u = make_double2((r.x * dv - cfv[0] * u.x) * ibet, (r.y * dv - cfv[0] * u.y) * ibet);
             S(k) = u;
             cprev = cfv[2];
         }
@@ -407,28 +408,33 @@ __global__ void __launch_bounds__(128) k_poisson(Geo G, PoissonArgs A)
         h.y = h.y * dv;
         double den, p, q, r;
         double2 s;
+        double iden;
         if (i == 0) {
             den = d;
-            p = e / den; q = f / den; r = g / den;
-            s = make_double2(h.x / den, h.y / den);
+            iden = 1.0 / den;
+            p = e * iden; q = f * iden; r = g * iden;
+            s = make_double2(h.x * iden, h.y * iden);
         } else if (i == 1) {
             den = d - c * p1;
-            p = (e - c * q1) / den; q = (f - c * r1) / den; r = (g) / den;
-            s = make_double2((h.x - c * s1.x) / den, (h.y - c * s1.y) / den);
+            iden = 1.0 / den;
+            p = (e - c * q1) * iden; q = (f - c * r1) * iden; r = g * iden;
+            s = make_double2((h.x - c * s1.x) * iden, (h.y - c * s1.y) * iden);
         } else if (i == 2) {
             double bet = c - b * p2;
             den = d - b * q2 - bet * p1;
-            p = (e - b * r2 - bet * q1) / den; q = (f - bet * r1) / den; r = (g) / den;
-            s = make_double2((h.x - b * s2.x - bet * s1.x) / den, (h.y - b * s2.y - bet * s1.y) / den);
+            iden = 1.0 / den;
+            p = (e - b * r2 - bet * q1) * iden; q = (f - bet * r1) * iden; r = g * iden;
+            s = make_double2((h.x - b * s2.x - bet * s1.x) * iden, (h.y - b * s2.y - bet * s1.y) * iden);
         } else {
             double alp = b - a * p3;
             double bet = c - a * q3 - alp * p2;
             den = d - a * r3 - alp * q2 - bet * p1;
-            p = (e - alp * r2 - bet * q1) / den;
-            q = (f - bet * r1) / den;
-            r = (g) / den;
-            s = make_double2((h.x - a * s3.x - alp * s2.x - bet * s1.x) / den,
-                             (h.y - a * s3.y - alp * s2.y - bet * s1.y) / den);
+            iden = 1.0 / den;
+            p = (e - alp * r2 - bet * q1) * iden;
+            q = (f - bet * r1) * iden;
+            r = g * iden;
+            s = make_double2((h.x - a * s3.x - alp * s2.x - bet * s1.x) * iden,
+                             (h.y - a * s3.y - alp * s2.y - bet * s1.y) * iden);
         }
         at(Pp, k) = p; at(Qp, k) = q; at(Rp, k) = r;
         S(k) = s;
@@ -493,18 +499,18 @@ __global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
         double up1h;
         if (ORDER == 2) up1h = __ldg(p + I(k, i + 1, j)) - __ldg(p + ijk);
         else up1h = A1 * (__ldg(p + I(k, i + 1, j)) - __ldg(p + ijk)) + A2 * (__ldg(p + I(k, i + 2, j)) - __ldg(p + I(k, i - 1, j)));
-        u = u - up1h * dt / G.dx;
+        u = u - up1h * A.dtdx;
         double vp1h;
         if (ORDER == 2) vp1h = __ldg(p + I(k, i, j + 1)) - __ldg(p + ijk);
         else vp1h = A1 * (__ldg(p + I(k, i, j + 1)) - __ldg(p + ijk)) + A2 * (__ldg(p + I(k, i, j + 2)) - __ldg(p + I(k, i, j - 1)));
-        A.v[ijk] = A.v[ijk] - vp1h * dt / G.dy;
+        A.v[ijk] = A.v[ijk] - vp1h * A.dtdy;
     }
     A.u[ijk] = u;
     if (k >= GZ - 1 && k < n2 - GZ) {
         double wp1h;
         if (ORDER == 2) wp1h = __ldg(p + I(k + 1, i, j)) - __ldg(p + ijk);
         else wp1h = A1 * (__ldg(p + I(k + 1, i, j)) - __ldg(p + ijk)) + A2 * (__ldg(p + I(k + 2, i, j)) - __ldg(p + I(k - 1, i, j)));
-        A.w[ijk] = A.w[ijk] - wp1h * dt / G.dzp1h[k];
+        A.w[ijk] = A.w[ijk] - wp1h * (dt * G.idzp1h[k]);
     }
     if (A.mc) A.c[ijk] = A.c[ijk] + A.gc[k] * (*A.mc);   // chanfast.c:603-606
 }

@@ -123,234 +123,257 @@ __global__ void k_ghosts(Geo G, GhostArgs A)
 }
 
 // --------------------------------------------------------------------- RHS
+//
+// One block owns an 8 (x) by 32 (y) column tile and marches up a chunk of
+// interior rows.  The 7 k-planes a row needs (k-3..k+3) of u, v, w, c, with a
+// 3-cell periodic halo in x and y, sit in a ring of 8 shared-memory slots;
+// the next plane streams in with cp.async while the current row is computed.
+// Every stencil value is read from shared memory.  Divisions by the grid
+// metrics are multiplications by their reciprocals (host tables), so results
+// agree with the reference to rounding, not bit for bit.
 
+constexpr int RT_I = 8, RT_J = 32, RT_H = 3, RT_SLOTS = 8;
+constexpr int RT_PI = RT_I + 2 * RT_H, RT_PJ = RT_J + 2 * RT_H;   // 14 x 38
+constexpr int RT_PLANE = RT_PI * RT_PJ;
+constexpr int RT_THREADS = RT_I * RT_J;
+constexpr int RT_KC = 64;   // interior rows per block
+
+size_t rhs_smem_bytes() { return (size_t) 4 * RT_SLOTS * RT_PLANE * sizeof(double); }
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src)
+{
+    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_rhs(Geo G, RhsArgs A)
+__global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = GZ + blockIdx.z;
-    if (j >= G.ny || i >= G.nx) return;
+    extern __shared__ double sm[];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RT_J + tx;
+    const int j0 = blockIdx.x * RT_J, i0 = blockIdx.y * RT_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
-    const double dx = G.dx, dy = G.dy, dxdy = G.dxdy;
-    const double* __restrict__ dz = G.dz;
+    const int kb = GZ + blockIdx.z * RT_KC;
+    const int ke = min(kb + RT_KC, GZ + G.nz);
+    const double* src[4] = {A.u, A.v, A.w, A.c};
+
+    auto load_plane = [&](int k) {
+        const int slot = k & (RT_SLOTS - 1);
+        for (int idx = tid; idx < 4 * RT_PLANE; idx += RT_THREADS) {
+            int f = idx / RT_PLANE, r = idx - f * RT_PLANE;
+            int ii = r / RT_PJ, jj = r - ii * RT_PJ;
+            int gi = (i0 + ii - RT_H) % nx; if (gi < 0) gi += nx;
+            int gj = (j0 + jj - RT_H) % ny; if (gj < 0) gj += ny;
+            cp_async8(sm + (f * RT_SLOTS + slot) * RT_PLANE + r, src[f] + ((long long) k * nx + gi) * ny + gj);
+        }
+        cp_async_commit();
+    };
+    for (int k = kb - 3; k <= kb + 3; k++) load_plane(k);
+    cp_async_wait_all();
+    __syncthreads();
+
+    const int i = i0 + ty, j = j0 + tx;
+    const bool out = i < nx && j < ny;
+    const double dxdy = G.dxdy, idx = G.idx, idy = G.idy;
     const double* __restrict__ dydz = G.dydz;
     const double* __restrict__ dxdz = G.dxdz;
+    const int kb_w = GZ - 1, kt_u = n2 - GZ;   // wall ghost rows of cell-centred fields
 
-    auto I = [&](int di, int dj, int dk) -> long long {
-        return ((long long) (k + dk) * nx + wrapi(i + di, nx)) * ny + wrapi(j + dj, ny);
-    };
-    auto U = [&](int di, int dj, int dk) { return __ldg(A.u + I(di, dj, dk)); };
-    auto V = [&](int di, int dj, int dk) { return __ldg(A.v + I(di, dj, dk)); };
-    auto W = [&](int di, int dj, int dk) { return __ldg(A.w + I(di, dj, dk)); };
-    auto C = [&](int di, int dj, int dk) { return __ldg(A.c + I(di, dj, dk)); };
-    const long long ijk = I(0, 0, 0);
-    const double vol = dx * dy * dz[k];
-    const bool do_w = k < n2 - GZ - 1;
-    const int kb = GZ - 1, kt = n2 - GZ;   // wall ghost rows of cell-centred fields
-
-    double fu, fv, fw = 0.0, fc;
-
-    if (ORDER == 2) {
-        // massflux{x,y,z}2 (advect.c:6-85) formed on the fly
-        auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
-        auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
-        auto mx_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)); };
-        auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
-        auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
-        auto my_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)); };
-        auto mz_u = [&](int di, int dj, int dk) { return 0.5 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1)); };
-        auto mz_v = [&](int di, int dj, int dk) { return 0.5 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1)); };
-        auto mz_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)); };
-
-        {   // advectu2 (advect.c:286-350)
-            double q0 = U(0, 0, 0);
-            double xph = mx_u(0, 0, 0) * 0.5 * (q0 + U(1, 0, 0));
-            double yph = mx_v(0, 0, 0) * 0.5 * (q0 + U(0, 1, 0));
-            double zph = mx_w(0, 0, 0) * 0.5 * (q0 + U(0, 0, 1));
-            double xmh = mx_u(-1, 0, 0) * 0.5 * (q0 + U(-1, 0, 0));
-            double ymh = mx_v(0, -1, 0) * 0.5 * (q0 + U(0, -1, 0));
-            double zmh = mx_w(0, 0, -1) * 0.5 * (q0 + U(0, 0, -1));
-            if (k == n2 - GZ - 1) zph = mx_w(0, 0, 0) * (0.5 * (U(0, 0, kt - 1 - k) + U(0, 0, kt - k)));
-            if (k == GZ) zmh = mx_w(0, 0, -1) * (0.5 * (U(0, 0, kb - k) + U(0, 0, kb + 1 - k)));
-            fu = -((xph - xmh) + (yph - ymh) + (zph - zmh)) / vol;
-        }
-        {   // advectv2 (advect.c:353-417)
-            double q0 = V(0, 0, 0);
-            double xph = my_u(0, 0, 0) * 0.5 * (q0 + V(1, 0, 0));
-            double yph = my_v(0, 0, 0) * 0.5 * (q0 + V(0, 1, 0));
-            double zph = my_w(0, 0, 0) * 0.5 * (q0 + V(0, 0, 1));
-            double xmh = my_u(-1, 0, 0) * 0.5 * (q0 + V(-1, 0, 0));
-            double ymh = my_v(0, -1, 0) * 0.5 * (q0 + V(0, -1, 0));
-            double zmh = my_w(0, 0, -1) * 0.5 * (q0 + V(0, 0, -1));
-            if (k == n2 - GZ - 1) zph = my_w(0, 0, 0) * (0.5 * (V(0, 0, kt - 1 - k) + V(0, 0, kt - k)));
-            if (k == GZ) zmh = my_w(0, 0, -1) * (0.5 * (V(0, 0, kb - k) + V(0, 0, kb + 1 - k)));
-            fv = -((xph - xmh) + (yph - ymh) + (zph - zmh)) / vol;
-        }
-        if (do_w) {   // advectw2 (advect.c:420-463)
-            double q0 = W(0, 0, 0);
-            double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
-            double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
-            double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
-            double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
-            double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
-            double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
-            fw = -((xph - xmh) + (yph - ymh) + (zph - zmh)) / (dx * dy * G.dzp1h[k]);
-        }
-        // add_laplacexy_operator_{u,w}2 (diffuseu.c:286-313, diffusew.c:290-317)
-        auto lap2 = [&](auto F, double nu) {
-            double q0 = F(0, 0, 0);
-            return nu * (((F(1, 0, 0) - q0) / dx - (q0 - F(-1, 0, 0)) / dx) / dx
-                         + ((F(0, 1, 0) - q0) / dy - (q0 - F(0, -1, 0)) / dy) / dy);
+    for (int k = kb; k < ke; k++) {
+        if (k + 4 <= ke + 2) load_plane(k + 4);
+        auto at = [&](int f, int di, int dj, int dk) -> double {
+            return sm[(f * RT_SLOTS + ((k + dk) & (RT_SLOTS - 1))) * RT_PLANE + (ty + RT_H + di) * RT_PJ + (tx + RT_H + dj)];
         };
-        fu += lap2(U, A.nu);
-        fv += lap2(V, A.nu);
-        if (do_w) fw += lap2(W, A.nu);
-    } else {
-        // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation
-        auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
-            return B1 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)) + B2 * (d * U(di - 1, dj, dk) + d * U(di + 2, dj, dk)); };
-        auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
-            return B1 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)) + B2 * (d * V(di - 1, dj, dk) + d * V(di + 2, dj, dk)); };
-        auto mx_w = [&](int di, int dj, int dk) {
-            return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
-        auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
-            return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
-        auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
-            return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
-        auto my_w = [&](int di, int dj, int dk) {
-            return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
-        auto mz_u = [&](int di, int dj, int dk) {
-            return B1 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1))
-                 + B2 * (dydz[k + dk - 1] * U(di, dj, dk - 1) + dydz[k + dk + 2] * U(di, dj, dk + 2)); };
-        auto mz_v = [&](int di, int dj, int dk) {
-            return B1 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1))
-                 + B2 * (dxdz[k + dk - 1] * V(di, dj, dk - 1) + dxdz[k + dk + 2] * V(di, dj, dk + 2)); };
-        auto mz_w = [&](int di, int dj, int dk) {
-            return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)) + B2 * (dxdy * W(di, dj, dk - 1) + dxdy * W(di, dj, dk + 2)); };
+        auto U = [&](int di, int dj, int dk) { return at(0, di, dj, dk); };
+        auto V = [&](int di, int dj, int dk) { return at(1, di, dj, dk); };
+        auto W = [&](int di, int dj, int dk) { return at(2, di, dj, dk); };
+        auto C = [&](int di, int dj, int dk) { return at(3, di, dj, dk); };
+        const double ivol = G.ivol[k];
+        const bool do_w = k < n2 - GZ - 1;
+        double fu, fv, fw = 0.0, fc;
 
-        // advectu4 / advectv4 share their structure (advect.c:466-669); the
-        // wall-adjacent z fluxes use the 4th-order wall value qbc.
-        auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {
-            double q0 = Q(0, 0, 0);
-            double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
-            double yph = MY(0, 0, 0) * 0.5 * (q0 + Q(0, 1, 0));
-            double zph = MZ(0, 0, 0) * 0.5 * (q0 + Q(0, 0, 1));
-            double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
-            double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
-            double zmh = MZ(0, 0, -1) * 0.5 * (q0 + Q(0, 0, -1));
-            double xp3 = MX(1, 0, 0) * 0.5 * (q0 + Q(3, 0, 0));
-            double yp3 = MY(0, 1, 0) * 0.5 * (q0 + Q(0, 3, 0));
-            double zp3 = MZ(0, 0, 1) * 0.5 * (q0 + Q(0, 0, 3));
-            double xm3 = MX(-2, 0, 0) * 0.5 * (q0 + Q(-3, 0, 0));
-            double ym3 = MY(0, -2, 0) * 0.5 * (q0 + Q(0, -3, 0));
-            double zm3 = MZ(0, 0, -2) * 0.5 * (q0 + Q(0, 0, -3));
-            if (k >= n2 - GZ - 2 || k <= GZ + 1) {
-                double qbot = 0.5 * A2 * (Q(0, 0, kb - 1 - k) + Q(0, 0, kb + 2 - k))
-                            + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kb - k) + Q(0, 0, kb + 1 - k));
-                double qtop = 0.5 * A2 * (Q(0, 0, kt - 2 - k) + Q(0, 0, kt + 1 - k))
-                            + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kt - 1 - k) + Q(0, 0, kt - k));
-                if (k == n2 - GZ - 1) {
-                    zph = MZ(0, 0, 0) * qtop;
-                    zp3 = -MZ(0, 0, -1) * 0.5 * (Q(0, 0, -2) + Q(0, 0, 1)) + 2.0 * MZ(0, 0, 0) * qtop;
-                }
-                if (k == n2 - GZ - 2) zp3 = MZ(0, 0, 1) * qtop;
-                if (k == GZ) {
-                    zmh = MZ(0, 0, -1) * qbot;
-                    zm3 = -MZ(0, 0, 0) * 0.5 * (Q(0, 0, 2) + Q(0, 0, -1)) + 2.0 * MZ(0, 0, -1) * qbot;
-                }
-                if (k == GZ + 1) zm3 = MZ(0, 0, -2) * qbot;
+        if (ORDER == 2) {
+            // massflux{x,y,z}2 (advect.c:6-85) formed on the fly
+            auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
+            auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
+            auto mx_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)); };
+            auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
+            auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
+            auto my_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)); };
+            auto mz_u = [&](int di, int dj, int dk) { return 0.5 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1)); };
+            auto mz_v = [&](int di, int dj, int dk) { return 0.5 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1)); };
+            auto mz_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)); };
+            auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {   // advectu2 / advectv2 (advect.c:286-417)
+                double q0 = Q(0, 0, 0);
+                double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
+                double yph = MY(0, 0, 0) * 0.5 * (q0 + Q(0, 1, 0));
+                double zph = MZ(0, 0, 0) * 0.5 * (q0 + Q(0, 0, 1));
+                double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
+                double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
+                double zmh = MZ(0, 0, -1) * 0.5 * (q0 + Q(0, 0, -1));
+                if (k == n2 - GZ - 1) zph = MZ(0, 0, 0) * (0.5 * (Q(0, 0, kt_u - 1 - k) + Q(0, 0, kt_u - k)));
+                if (k == GZ) zmh = MZ(0, 0, -1) * (0.5 * (Q(0, 0, kb_w - k) + Q(0, 0, kb_w + 1 - k)));
+                return -((xph - xmh) + (yph - ymh) + (zph - zmh)) * ivol;
+            };
+            fu = adv_cell(U, mx_u, mx_v, mx_w);
+            fv = adv_cell(V, my_u, my_v, my_w);
+            if (do_w) {   // advectw2 (advect.c:420-463)
+                double q0 = W(0, 0, 0);
+                double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
+                double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
+                double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
+                double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
+                double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
+                double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
+                fw = -((xph - xmh) + (yph - ymh) + (zph - zmh)) * G.ivolw[k];
             }
-            return -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
-                     + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) / vol;
-        };
-        fu = adv_cell(U, mx_u, mx_v, mx_w);
-        fv = adv_cell(V, my_u, my_v, my_w);
-        if (do_w) {   // advectw4 (advect.c:672-734)
-            double q0 = W(0, 0, 0);
-            double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
-            double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
-            double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
-            double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
-            double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
-            double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
-            double xp3 = mz_u(1, 0, 0) * 0.5 * (q0 + W(3, 0, 0));
-            double yp3 = mz_v(0, 1, 0) * 0.5 * (q0 + W(0, 3, 0));
-            double zp3 = mz_w(0, 0, 1) * 0.5 * (q0 + W(0, 0, 3));
-            double xm3 = mz_u(-2, 0, 0) * 0.5 * (q0 + W(-3, 0, 0));
-            double ym3 = mz_v(0, -2, 0) * 0.5 * (q0 + W(0, -3, 0));
-            double zm3 = mz_w(0, 0, -2) * 0.5 * (q0 + W(0, 0, -3));
-            fw = -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
-                   + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) / (dx * dy * G.dzp1h[k]);
-        }
-        // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363)
-        auto lap4 = [&](auto F, double nu) {
-            double q0 = F(0, 0, 0);
-            double up3h = A1 * (F(2, 0, 0) - F(1, 0, 0)) + A2 * (F(3, 0, 0) - q0);
-            double up1h = A1 * (F(1, 0, 0) - q0) + A2 * (F(2, 0, 0) - F(-1, 0, 0));
-            double um1h = A1 * (q0 - F(-1, 0, 0)) + A2 * (F(1, 0, 0) - F(-2, 0, 0));
-            double um3h = A1 * (F(-1, 0, 0) - F(-2, 0, 0)) + A2 * (q0 - F(-3, 0, 0));
-            double vp3h = A1 * (F(0, 2, 0) - F(0, 1, 0)) + A2 * (F(0, 3, 0) - q0);
-            double vp1h = A1 * (F(0, 1, 0) - q0) + A2 * (F(0, 2, 0) - F(0, -1, 0));
-            double vm1h = A1 * (q0 - F(0, -1, 0)) + A2 * (F(0, 1, 0) - F(0, -2, 0));
-            double vm3h = A1 * (F(0, -1, 0) - F(0, -2, 0)) + A2 * (q0 - F(0, -3, 0));
-            return nu * ((A1 * (up1h / dx - um1h / dx) + A2 * (up3h / dx - um3h / dx)) / dx
-                         + (A1 * (vp1h / dy - vm1h / dy) + A2 * (vp3h / dy - vm3h / dy)) / dy);
-        };
-        fu += lap4(U, A.nu);
-        fv += lap4(V, A.nu);
-        if (do_w) fw += lap4(W, A.nu);
-    }
+            // add_laplacexy_operator_{u,w}2 (diffuseu.c:286-313, diffusew.c:290-317)
+            auto lap2 = [&](auto F, double nu) {
+                double q0 = F(0, 0, 0);
+                return nu * (((F(1, 0, 0) - q0) * idx - (q0 - F(-1, 0, 0)) * idx) * idx
+                             + ((F(0, 1, 0) - q0) * idy - (q0 - F(0, -1, 0)) * idy) * idy);
+            };
+            fu += lap2(U, A.nu);
+            fv += lap2(V, A.nu);
+            if (do_w) fw += lap2(W, A.nu);
+            fc = lap2(C, A.kappa);
+        } else {
+            // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation
+            auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+                return B1 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)) + B2 * (d * U(di - 1, dj, dk) + d * U(di + 2, dj, dk)); };
+            auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+                return B1 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)) + B2 * (d * V(di - 1, dj, dk) + d * V(di + 2, dj, dk)); };
+            auto mx_w = [&](int di, int dj, int dk) {
+                return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
+            auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+                return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
+            auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+                return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
+            auto my_w = [&](int di, int dj, int dk) {
+                return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
+            auto mz_u = [&](int di, int dj, int dk) {
+                return B1 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1))
+                     + B2 * (dydz[k + dk - 1] * U(di, dj, dk - 1) + dydz[k + dk + 2] * U(di, dj, dk + 2)); };
+            auto mz_v = [&](int di, int dj, int dk) {
+                return B1 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1))
+                     + B2 * (dxdz[k + dk - 1] * V(di, dj, dk - 1) + dxdz[k + dk + 2] * V(di, dj, dk + 2)); };
+            auto mz_w = [&](int di, int dj, int dk) {
+                return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)) + B2 * (dxdy * W(di, dj, dk - 1) + dxdy * W(di, dj, dk + 2)); };
 
-    {   // flux_quick + advect_scalar (scalar.c:79-162), order independent
-        const double q = -0.125;
-        auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
-            double cph = 0.5 * (c0 + c1);
-            cph += m > 0.0 ? q * (c1 - 2.0 * c0 + cm1) : q * (c2 - 2.0 * c1 + c0);
-            return m * cph;
-        };
-        double c0 = C(0, 0, 0);
-        double fxp = quick(dydz[k] * U(0, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0), C(2, 0, 0));
-        double fxm = quick(dydz[k] * U(-1, 0, 0), C(-2, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0));
-        double fyp = quick(dxdz[k] * V(0, 0, 0), C(0, -1, 0), c0, C(0, 1, 0), C(0, 2, 0));
-        double fym = quick(dxdz[k] * V(0, -1, 0), C(0, -2, 0), C(0, -1, 0), c0, C(0, 1, 0));
-        double fzp = quick(dxdy * W(0, 0, 0), C(0, 0, -1), c0, C(0, 0, 1), C(0, 0, 2));
-        double fzm = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), c0, C(0, 0, 1));
-        fc = -((fxp - fxm) + (fyp - fym) + (fzp - fzm)) / vol;
-        if (ORDER == 2) {
-            double nu = A.kappa;
-            fc += nu * (((C(1, 0, 0) - c0) / dx - (c0 - C(-1, 0, 0)) / dx) / dx
-                        + ((C(0, 1, 0) - c0) / dy - (c0 - C(0, -1, 0)) / dy) / dy);
-        } else {
-            double up3h = A1 * (C(2, 0, 0) - C(1, 0, 0)) + A2 * (C(3, 0, 0) - c0);
-            double up1h = A1 * (C(1, 0, 0) - c0) + A2 * (C(2, 0, 0) - C(-1, 0, 0));
-            double um1h = A1 * (c0 - C(-1, 0, 0)) + A2 * (C(1, 0, 0) - C(-2, 0, 0));
-            double um3h = A1 * (C(-1, 0, 0) - C(-2, 0, 0)) + A2 * (c0 - C(-3, 0, 0));
-            double vp3h = A1 * (C(0, 2, 0) - C(0, 1, 0)) + A2 * (C(0, 3, 0) - c0);
-            double vp1h = A1 * (C(0, 1, 0) - c0) + A2 * (C(0, 2, 0) - C(0, -1, 0));
-            double vm1h = A1 * (c0 - C(0, -1, 0)) + A2 * (C(0, 1, 0) - C(0, -2, 0));
-            double vm3h = A1 * (C(0, -1, 0) - C(0, -2, 0)) + A2 * (c0 - C(0, -3, 0));
-            fc += A.kappa * ((A1 * (up1h / dx - um1h / dx) + A2 * (up3h / dx - um3h / dx)) / dx
-                             + (A1 * (vp1h / dy - vm1h / dy) + A2 * (vp3h / dy - vm3h / dy)) / dy);
+            // advectu4 / advectv4 (advect.c:466-669); the wall-adjacent z
+            // fluxes use the fourth-order wall value qbot / qtop.
+            auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {
+                double q0 = Q(0, 0, 0);
+                double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
+                double yph = MY(0, 0, 0) * 0.5 * (q0 + Q(0, 1, 0));
+                double zph = MZ(0, 0, 0) * 0.5 * (q0 + Q(0, 0, 1));
+                double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
+                double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
+                double zmh = MZ(0, 0, -1) * 0.5 * (q0 + Q(0, 0, -1));
+                double xp3 = MX(1, 0, 0) * 0.5 * (q0 + Q(3, 0, 0));
+                double yp3 = MY(0, 1, 0) * 0.5 * (q0 + Q(0, 3, 0));
+                double zp3 = MZ(0, 0, 1) * 0.5 * (q0 + Q(0, 0, 3));
+                double xm3 = MX(-2, 0, 0) * 0.5 * (q0 + Q(-3, 0, 0));
+                double ym3 = MY(0, -2, 0) * 0.5 * (q0 + Q(0, -3, 0));
+                double zm3 = MZ(0, 0, -2) * 0.5 * (q0 + Q(0, 0, -3));
+                if (k >= n2 - GZ - 2 || k <= GZ + 1) {
+                    double qbot = 0.5 * A2 * (Q(0, 0, kb_w - 1 - k) + Q(0, 0, kb_w + 2 - k))
+                                + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kb_w - k) + Q(0, 0, kb_w + 1 - k));
+                    double qtop = 0.5 * A2 * (Q(0, 0, kt_u - 2 - k) + Q(0, 0, kt_u + 1 - k))
+                                + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kt_u - 1 - k) + Q(0, 0, kt_u - k));
+                    if (k == n2 - GZ - 1) {
+                        zph = MZ(0, 0, 0) * qtop;
+                        zp3 = -MZ(0, 0, -1) * 0.5 * (Q(0, 0, -2) + Q(0, 0, 1)) + 2.0 * MZ(0, 0, 0) * qtop;
+                    }
+                    if (k == n2 - GZ - 2) zp3 = MZ(0, 0, 1) * qtop;
+                    if (k == GZ) {
+                        zmh = MZ(0, 0, -1) * qbot;
+                        zm3 = -MZ(0, 0, 0) * 0.5 * (Q(0, 0, 2) + Q(0, 0, -1)) + 2.0 * MZ(0, 0, -1) * qbot;
+                    }
+                    if (k == GZ + 1) zm3 = MZ(0, 0, -2) * qbot;
+                }
+                return -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
+                         + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) * ivol;
+            };
+            fu = adv_cell(U, mx_u, mx_v, mx_w);
+            fv = adv_cell(V, my_u, my_v, my_w);
+            if (do_w) {   // advectw4 (advect.c:672-734)
+                double q0 = W(0, 0, 0);
+                double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
+                double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
+                double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
+                double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
+                double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
+                double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
+                double xp3 = mz_u(1, 0, 0) * 0.5 * (q0 + W(3, 0, 0));
+                double yp3 = mz_v(0, 1, 0) * 0.5 * (q0 + W(0, 3, 0));
+                double zp3 = mz_w(0, 0, 1) * 0.5 * (q0 + W(0, 0, 3));
+                double xm3 = mz_u(-2, 0, 0) * 0.5 * (q0 + W(-3, 0, 0));
+                double ym3 = mz_v(0, -2, 0) * 0.5 * (q0 + W(0, -3, 0));
+                double zm3 = mz_w(0, 0, -2) * 0.5 * (q0 + W(0, 0, -3));
+                fw = -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
+                       + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) * G.ivolw[k];
+            }
+            // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363)
+            auto lap4 = [&](auto F, double nu) {
+                double q0 = F(0, 0, 0);
+                double up3h = A1 * (F(2, 0, 0) - F(1, 0, 0)) + A2 * (F(3, 0, 0) - q0);
+                double up1h = A1 * (F(1, 0, 0) - q0) + A2 * (F(2, 0, 0) - F(-1, 0, 0));
+                double um1h = A1 * (q0 - F(-1, 0, 0)) + A2 * (F(1, 0, 0) - F(-2, 0, 0));
+                double um3h = A1 * (F(-1, 0, 0) - F(-2, 0, 0)) + A2 * (q0 - F(-3, 0, 0));
+                double vp3h = A1 * (F(0, 2, 0) - F(0, 1, 0)) + A2 * (F(0, 3, 0) - q0);
+                double vp1h = A1 * (F(0, 1, 0) - q0) + A2 * (F(0, 2, 0) - F(0, -1, 0));
+                double vm1h = A1 * (q0 - F(0, -1, 0)) + A2 * (F(0, 1, 0) - F(0, -2, 0));
+                double vm3h = A1 * (F(0, -1, 0) - F(0, -2, 0)) + A2 * (q0 - F(0, -3, 0));
+                return nu * ((A1 * (up1h * idx - um1h * idx) + A2 * (up3h * idx - um3h * idx)) * idx
+                             + (A1 * (vp1h * idy - vm1h * idy) + A2 * (vp3h * idy - vm3h * idy)) * idy);
+            };
+            fu += lap4(U, A.nu);
+            fv += lap4(V, A.nu);
+            if (do_w) fw += lap4(W, A.nu);
+            fc = lap4(C, A.kappa);
         }
-        // add_buoyancy{2,4} (scalar.c:6-76)
-        if (ORDER == 2) {
-            fu += 0.5 * (c0 + C(1, 0, 0)) * A.betg_x;
-            fv += 0.5 * (c0 + C(0, 1, 0)) * A.betg_y;
-            if (do_w) fw += 0.5 * (c0 + C(0, 0, 1)) * A.betg_z;
-        } else {
-            double cphx = B1 * (c0 + C(1, 0, 0)) + B2 * (C(-1, 0, 0) + C(2, 0, 0));
-            double cphy = B1 * (c0 + C(0, 1, 0)) + B2 * (C(0, -1, 0) + C(0, 2, 0));
-            fu += cphx * A.betg_x;
-            fv += cphy * A.betg_y;
-            if (do_w) fw += (B1 * (c0 + C(0, 0, 1)) + B2 * (C(0, 0, -1) + C(0, 0, 2))) * A.betg_z;
+
+        {   // flux_quick + advect_scalar (scalar.c:79-162), order independent
+            const double q = -0.125;
+            auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
+                double cph = 0.5 * (c0 + c1);
+                cph += m > 0.0 ? q * (c1 - 2.0 * c0 + cm1) : q * (c2 - 2.0 * c1 + c0);
+                return m * cph;
+            };
+            double c0 = C(0, 0, 0);
+            double fxp = quick(dydz[k] * U(0, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0), C(2, 0, 0));
+            double fxm = quick(dydz[k] * U(-1, 0, 0), C(-2, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0));
+            double fyp = quick(dxdz[k] * V(0, 0, 0), C(0, -1, 0), c0, C(0, 1, 0), C(0, 2, 0));
+            double fym = quick(dxdz[k] * V(0, -1, 0), C(0, -2, 0), C(0, -1, 0), c0, C(0, 1, 0));
+            double fzp = quick(dxdy * W(0, 0, 0), C(0, 0, -1), c0, C(0, 0, 1), C(0, 0, 2));
+            double fzm = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), c0, C(0, 0, 1));
+            fc = -((fxp - fxm) + (fyp - fym) + (fzp - fzm)) * ivol + fc;
+            // add_buoyancy{2,4} (scalar.c:6-76)
+            if (ORDER == 2) {
+                fu += 0.5 * (c0 + C(1, 0, 0)) * A.betg_x;
+                fv += 0.5 * (c0 + C(0, 1, 0)) * A.betg_y;
+                if (do_w) fw += 0.5 * (c0 + C(0, 0, 1)) * A.betg_z;
+            } else {
+                double cphx = B1 * (c0 + C(1, 0, 0)) + B2 * (C(-1, 0, 0) + C(2, 0, 0));
+                double cphy = B1 * (c0 + C(0, 1, 0)) + B2 * (C(0, -1, 0) + C(0, 2, 0));
+                fu += cphx * A.betg_x;
+                fv += cphy * A.betg_y;
+                if (do_w) fw += (B1 * (c0 + C(0, 0, 1)) + B2 * (C(0, 0, -1) + C(0, 0, 2))) * A.betg_z;
+            }
         }
+        if (out) {
+            const long long ijk = ((long long) k * nx + i) * ny + j;
+            A.fu[ijk] = fu;
+            A.fv[ijk] = fv;
+            if (do_w) A.fw[ijk] = fw;
+            A.fc[ijk] = fc;
+        }
+        cp_async_wait_all();
+        __syncthreads();
     }
-    A.fu[ijk] = fu;
-    A.fv[ijk] = fv;
-    if (do_w) A.fw[ijk] = fw;
-    A.fc[ijk] = fc;
 }
 
 // ------------------------------------------------------------- launchers
@@ -365,10 +388,19 @@ void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st)
 
 void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st)
 {
-    dim3 blk(32, 4, 1);
-    dim3 grd((G.ny + 31) / 32, (G.nx + 3) / 4, G.nz);
-    if (G.order == 2) k_rhs<2><<<grd, blk, 0, st>>>(G, A);
-    else k_rhs<4><<<grd, blk, 0, st>>>(G, A);
+    dim3 blk(RT_J, RT_I, 1);
+    dim3 grd((G.ny + RT_J - 1) / RT_J, (G.nx + RT_I - 1) / RT_I, (G.nz + RT_KC - 1) / RT_KC);
+    size_t sm = rhs_smem_bytes();
+    if (G.order == 2) k_rhs<2><<<grd, blk, sm, st>>>(G, A);
+    else k_rhs<4><<<grd, blk, sm, st>>>(G, A);
+}
+
+cudaError_t rhs_set_smem_limits()
+{
+    int v = (int) rhs_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_rhs<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    return e;
 }
 
 }  // namespace cf

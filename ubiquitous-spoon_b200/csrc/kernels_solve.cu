@@ -5,11 +5,12 @@
 //   h  = helmholtz1d_operator(x, nuadt) + gamdt*f + zetdt*g - hbc
 //   x  = solve_helmholtz1d(h, -nubdt)       (tridag.c / heptdag.c)
 //   apply_bc(x)
-// The band matrix is the same for every column, so its factorisation
-// (forward multipliers F1..F3, pivots DEN, back multipliers P, Q, R) comes
-// precomputed from host_band.cpp and only the right-hand side streams.  The
-// forward-substituted vector s is kept in the field's own storage between
-// the two sweeps.  With `partial` set, each warp also writes the sum of its
+// The band matrix is the same for every column, so its factorisation comes
+// precomputed from host_band.cpp; the Helmholtz operator, the RK3 combination,
+// the cell volume and the pivot reciprocal are folded into one coefficient
+// row per k (fused_rows), so the forward sweep is a short dot product per row
+// and results agree with the reference to rounding.  The forward-substituted
+// vector s is kept in the field's own storage between the two sweeps.  With `partial` set, each warp also writes the sum of its
 // 32 columns for every row (input of get_xy_avg, get.c:281-302).
 #include "engine.cuh"
 #include "host_band.h"
@@ -91,7 +92,6 @@ __global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
     const int kt = IS_W ? n2 - GZ - 1 : n2 - GZ;    // top wall ghost row / face
     const int n = A.fac.n, k0 = A.fac.k0;
     double* __restrict__ x = A.x;
-    const double* __restrict__ dz = G.dz;
     const long long cc = active ? col : 0;
     auto ld = [&](const double* p, int k) { return p[(long long) k * P + cc]; };
 
@@ -112,42 +112,26 @@ __global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
     };
 
     constexpr int H = ORDER == 2 ? 1 : 3;
+    constexpr int W = 2 * H + 1 + 6;   // fused row width (host_band.h fused_rows)
     double win[2 * H + 1];  // old x at rows k-H .. k+H
 #pragma unroll
     for (int q = 0; q < 2 * H + 1; q++) win[q] = old(k0 - H + q);
 
+    // Forward sweep: helmholtz1d_operator + RK3 combination + boundary lifting
+    // + forward elimination of tridag/heptdag, one fused row per k.
     double s1 = 0.0, s2 = 0.0, s3 = 0.0;
     const double shift = SHIFT ? *A.gshift : 0.0;
+    const double* __restrict__ rows = A.rows;
     for (int i = 0; i < n; i++) {
         const int k = k0 + i;
-        double hv;
-        const double u0 = win[H];
-        if (ORDER == 2) {
-            if (!IS_W) {  // helmholtz1d_operator_u2 (diffuseu.c:121-131)
-                hv = u0 + A.nuadt * (((win[2] - u0) / G.dzp1h[k] - (u0 - win[0]) / G.dzm1h[k]) / dz[k]);
-            } else {      // helmholtz1d_operator_w2 (diffusew.c:121-132)
-                hv = u0 + A.nuadt * (((win[2] - u0) / dz[k + 1] - (u0 - win[0]) / dz[k]) / G.dzp1h[k]);
-            }
-        } else {
-            double wp3h = A1 * (win[5] - win[4]) + A2 * (win[6] - u0);
-            double wp1h = A1 * (win[4] - u0) + A2 * (win[5] - win[2]);
-            double wm1h = A1 * (u0 - win[2]) + A2 * (win[4] - win[1]);
-            double wm3h = A1 * (win[2] - win[1]) + A2 * (u0 - win[0]);
-            if (!IS_W)    // helmholtz1d_operator_u4 (diffuseu.c:149-169)
-                hv = u0 + A.nuadt * ((A1 * (wp1h / G.dzp1h[k] - wm1h / G.dzm1h[k])
-                                      + A2 * (wp3h / G.dzp3h[k] - wm3h / G.dzm3h[k])) / dz[k]);
-            else          // helmholtz1d_operator_w4 (diffusew.c:150-171)
-                hv = u0 + A.nuadt * ((A1 * (wp1h / dz[k + 1] - wm1h / dz[k])
-                                      + A2 * (wp3h / dz[k + 2] - wm3h / dz[k - 1])) / G.dzp1h[k]);
-        }
+        const double* r = rows + i * W;
         double gk = ld(A.g, k);
         if (SHIFT) gk = gk + shift;   // f += mdpdx of the previous substep (chanfast.c:516-519)
-        hv = hv + (A.gamdt * ld(A.f, k) + A.zetdt * gk);
-        hv = hv - A.hbc[k];
-        const double r = hv * (IS_W ? G.dzp1h[k] : dz[k]);
-        double s;
-        if (ORDER == 2) s = (r - A.fac.F1[i] * s1) / A.fac.DEN[i];
-        else s = (((r - A.fac.F3[i] * s3) - A.fac.F2[i] * s2) - A.fac.F1[i] * s1) / A.fac.DEN[i];
+        double s = __ldg(r + 2 * H + 3) + __ldg(r + 2 * H + 1) * ld(A.f, k) + __ldg(r + 2 * H + 2) * gk;
+#pragma unroll
+        for (int q = 0; q < 2 * H + 1; q++) s += __ldg(r + q) * win[q];
+        s -= __ldg(r + 2 * H + 4) * s1;
+        if (ORDER == 4) s -= __ldg(r + 2 * H + 5) * s2 + __ldg(r + 2 * H + 6) * s3;
         s3 = s2; s2 = s1; s1 = s;
         if (active) x[(long long) k * P + col] = s;
 #pragma unroll
@@ -164,8 +148,8 @@ __global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
         const int k = k0 + i;
         double s = active ? x[(long long) k * P + col] : 0.0;
         double y;
-        if (ORDER == 2) y = s - A.fac.P[i] * y1;
-        else y = ((s - A.fac.P[i] * y1) - A.fac.Q[i] * y2) - A.fac.R[i] * y3;
+        if (ORDER == 2) y = s - __ldg(A.fac.P + i) * y1;
+        else y = s - __ldg(A.fac.P + i) * y1 - __ldg(A.fac.Q + i) * y2 - __ldg(A.fac.R + i) * y3;
         y3 = y2; y2 = y1; y1 = y;
         if (active) x[(long long) k * P + col] = y;
         if (i >= n - 3) top[n - 1 - i] = y;
