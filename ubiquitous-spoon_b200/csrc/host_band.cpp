@@ -399,45 +399,51 @@ void apply_bc_w_col(const Metrics& m, std::vector<double>& x, double bc_bot, dou
     x = B.x;
 }
 
-void helmholtz_u_col(const Metrics& m, const std::vector<double>& u, std::vector<double>& h, double nudt)
+// One row of helmholtz1d_operator_u{2,4} (diffuseu.c:121-131 / 149-169).
+static double helmholtz_u_at(const Metrics& m, const double* u, int k, double nudt)
 {
     const auto& dz = m.dz;
-    for (int k = m.gz; k < m.n2 - m.gz; k++) {
-        if (m.order == 2) {  // diffuseu.c:121-131
-            double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-            double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-            h[k] = u[k] + nudt * (((u[k + 1] - u[k]) / dzp1h - (u[k] - u[k - 1]) / dzm1h) / dz[k]);
-        } else {  // diffuseu.c:149-169
-            double wp3h = A1 * (u[k + 2] - u[k + 1]) + A2 * (u[k + 3] - u[k]);
-            double wp1h = A1 * (u[k + 1] - u[k]) + A2 * (u[k + 2] - u[k - 1]);
-            double wm1h = A1 * (u[k] - u[k - 1]) + A2 * (u[k + 1] - u[k - 2]);
-            double wm3h = A1 * (u[k - 1] - u[k - 2]) + A2 * (u[k] - u[k - 3]);
-            double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
-            double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-            double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-            double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
-            h[k] = u[k] + nudt * ((A1 * (wp1h / dzp1h - wm1h / dzm1h) + A2 * (wp3h / dzp3h - wm3h / dzm3h)) / dz[k]);
-        }
+    if (m.order == 2) {
+        double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+        double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+        return u[k] + nudt * (((u[k + 1] - u[k]) / dzp1h - (u[k] - u[k - 1]) / dzm1h) / dz[k]);
     }
+    double wp3h = A1 * (u[k + 2] - u[k + 1]) + A2 * (u[k + 3] - u[k]);
+    double wp1h = A1 * (u[k + 1] - u[k]) + A2 * (u[k + 2] - u[k - 1]);
+    double wm1h = A1 * (u[k] - u[k - 1]) + A2 * (u[k + 1] - u[k - 2]);
+    double wm3h = A1 * (u[k - 1] - u[k - 2]) + A2 * (u[k] - u[k - 3]);
+    double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
+    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
+    double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
+    return u[k] + nudt * ((A1 * (wp1h / dzp1h - wm1h / dzm1h) + A2 * (wp3h / dzp3h - wm3h / dzm3h)) / dz[k]);
+}
+
+// One row of helmholtz1d_operator_w{2,4} (diffusew.c:121-132 / 150-171).
+static double helmholtz_w_at(const Metrics& m, const double* w, int k, double nudt)
+{
+    const auto& dz = m.dz;
+    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
+    if (m.order == 2) {
+        double dzp1 = dz[k + 1], dzm0 = dz[k];
+        return w[k] + nudt * (((w[k + 1] - w[k]) / dzp1 - (w[k] - w[k - 1]) / dzm0) / dzp1h);
+    }
+    double wp3h = A1 * (w[k + 2] - w[k + 1]) + A2 * (w[k + 3] - w[k]);
+    double wp1h = A1 * (w[k + 1] - w[k]) + A2 * (w[k + 2] - w[k - 1]);
+    double wm1h = A1 * (w[k] - w[k - 1]) + A2 * (w[k + 1] - w[k - 2]);
+    double wm3h = A1 * (w[k - 1] - w[k - 2]) + A2 * (w[k] - w[k - 3]);
+    double dzp2 = dz[k + 2], dzp1 = dz[k + 1], dzm0 = dz[k], dzm1 = dz[k - 1];
+    return w[k] + nudt * ((A1 * (wp1h / dzp1 - wm1h / dzm0) + A2 * (wp3h / dzp2 - wm3h / dzm1)) / dzp1h);
+}
+
+void helmholtz_u_col(const Metrics& m, const std::vector<double>& u, std::vector<double>& h, double nudt)
+{
+    for (int k = m.gz; k < m.n2 - m.gz; k++) h[k] = helmholtz_u_at(m, u.data(), k, nudt);
 }
 
 void helmholtz_w_col(const Metrics& m, const std::vector<double>& w, std::vector<double>& h, double nudt)
 {
-    const auto& dz = m.dz;
-    for (int k = m.gz; k < m.n2 - m.gz - 1; k++) {
-        double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-        if (m.order == 2) {  // diffusew.c:121-132
-            double dzp1 = dz[k + 1], dzm0 = dz[k];
-            h[k] = w[k] + nudt * (((w[k + 1] - w[k]) / dzp1 - (w[k] - w[k - 1]) / dzm0) / dzp1h);
-        } else {  // diffusew.c:150-171
-            double wp3h = A1 * (w[k + 2] - w[k + 1]) + A2 * (w[k + 3] - w[k]);
-            double wp1h = A1 * (w[k + 1] - w[k]) + A2 * (w[k + 2] - w[k - 1]);
-            double wm1h = A1 * (w[k] - w[k - 1]) + A2 * (w[k + 1] - w[k - 2]);
-            double wm3h = A1 * (w[k - 1] - w[k - 2]) + A2 * (w[k] - w[k - 3]);
-            double dzp2 = dz[k + 2], dzp1 = dz[k + 1], dzm0 = dz[k], dzm1 = dz[k - 1];
-            h[k] = w[k] + nudt * ((A1 * (wp1h / dzp1 - wm1h / dzm0) + A2 * (wp3h / dzp2 - wm3h / dzm1)) / dzp1h);
-        }
-    }
+    for (int k = m.gz; k < m.n2 - m.gz - 1; k++) h[k] = helmholtz_w_at(m, w.data(), k, nudt);
 }
 
 // ------------------------------------------------------- factorisation
@@ -717,16 +723,14 @@ std::vector<double> fused_rows(const Metrics& m, const ImplicitSet& s, bool is_w
     const int k0 = s.fac.k0, n = s.fac.n;
     std::vector<double> L((size_t) n * (2 * H + 1), 0.0);
     // The operator is linear: its coefficients are its response to unit columns.
-    std::vector<double> e(m.n2, 0.0), h(m.n2, 0.0);
-    for (int q = 0; q < m.n2; q++) {
-        std::fill(e.begin(), e.end(), 0.0);
-        std::fill(h.begin(), h.end(), 0.0);
-        e[q] = 1.0;
-        if (is_w) helmholtz_w_col(m, e, h, nuadt);
-        else helmholtz_u_col(m, e, h, nuadt);
-        for (int i = 0; i < n; i++) {
-            int k = k0 + i, off = q - k;
-            if (off >= -H && off <= H) L[(size_t) i * (2 * H + 1) + off + H] = h[k];
+    std::vector<double> e(m.n2, 0.0);
+    for (int i = 0; i < n; i++) {
+        int k = k0 + i;
+        for (int off = -H; off <= H; off++) {
+            e[k + off] = 1.0;
+            L[(size_t) i * (2 * H + 1) + off + H] = is_w ? helmholtz_w_at(m, e.data(), k, nuadt)
+                                                         : helmholtz_u_at(m, e.data(), k, nuadt);
+            e[k + off] = 0.0;
         }
     }
     std::vector<double> rows((size_t) n * W, 0.0);
