@@ -108,6 +108,23 @@ long cf_substeps_done(const cf_instance *inst);
  * divergence{2,4} (pressure.c:40-117), evaluated on the device. */
 int cf_max_divergence(cf_instance *inst, double *out);
 
+/* Same result as cf_max_divergence, without allocating anything.  It has no
+ * counterpart in the reference; it exists for callers that cannot call
+ * cudaMalloc or cudaFree at the point where they check the flow, e.g. a
+ * serving loop that has budgeted the whole device memory to resident
+ * instances (an allocation there can fail), or a monitor that runs between
+ * the steps of live instances on other streams (cudaFree synchronises the
+ * whole device and would stall them).  The partial maxima live in a
+ * file-scope device array of one double per interior k-plane, at most 8191
+ * planes: an instance with nz > 8191 is rejected with CF_EINVAL before any
+ * work is queued.  The array is shared by every call on a device,
+ * keeps the last call's contents and needs no zeroing (each call rewrites
+ * every entry it reads); calls that overlap on one GPU, e.g. for two
+ * instances on different streams, race on it.  The first call on each
+ * device looks up the array's device address with that device current;
+ * make that first call before any stream capture. */
+int cf_max_divergence_noalloc(cf_instance *inst, double *out);
+
 /* CFL number of the current velocity field for time step dt, as get_cfl
  * (get.c:390-416): max over interior cells of |u| dt/dx, |v| dt/dy,
  * |w| dt/dzph, evaluated on the device; synchronises the instance. */

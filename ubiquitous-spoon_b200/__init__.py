@@ -25,6 +25,7 @@ CF_OK, CF_EINVAL, CF_ENOMEM, CF_ECUDA, CF_EPIVOT, CF_ENONFINITE, CF_EIO = 0, -1,
 FIELDS = {"u": 0, "v": 1, "w": 2, "c": 3, "p": 4}
 LAYOUT_PADDED, LAYOUT_INTERIOR = 0, 1
 LOG_COLS = 10
+NOALLOC_MAX_ROWS = 8191   # scratch rows of cf_max_divergence_noalloc
 KERNEL_GROUPS = ("ghosts", "rhs", "solve_u", "mass_u", "solve_v", "solve_c", "mass_c", "solve_w",
                  "div_fftx", "ffty_fwd", "poisson", "ffty_bwd", "fftx_c2r", "project")
 NKERNEL_GROUPS = len(KERNEL_GROUPS)
@@ -92,6 +93,7 @@ def _bind(L):
     L.cf_substeps_done.restype = ll
     L.cf_substeps_done.argtypes = [vp]
     L.cf_max_divergence.argtypes = [vp, dp]
+    L.cf_max_divergence_noalloc.argtypes = [vp, dp]
     L.cf_cfl.argtypes = [vp, ctypes.c_double, dp]
     L.cf_set_dt.argtypes = [vp, ctypes.c_double]
     L.cf_device_field.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)]
@@ -210,6 +212,17 @@ class Instance:
     def max_divergence(self):
         d = ctypes.c_double()
         _check(self.L.cf_max_divergence(self.h, ctypes.byref(d)), "cf_max_divergence")
+        return d.value
+
+    def max_divergence_noalloc(self):
+        """max |div u| like max_divergence, through the entry point that
+        allocates no device memory (fixed scratch; nz <= 8191)."""
+        d = ctypes.c_double()
+        st = self.L.cf_max_divergence_noalloc(self.h, ctypes.byref(d))
+        if st == CF_EINVAL and self.cfg.nz > NOALLOC_MAX_ROWS:
+            raise ChanfastError(st, f"cf_max_divergence_noalloc: nz = {self.cfg.nz} exceeds its fixed "
+                                    f"scratch of {NOALLOC_MAX_ROWS} wall-normal planes")
+        _check(st, "cf_max_divergence_noalloc")
         return d.value
 
     def cfl(self, dt):

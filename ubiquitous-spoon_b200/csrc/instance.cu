@@ -183,6 +183,66 @@ __global__ void k_cfl(Geo G, const double* u, const double* v, const double* w, 
     if (threadIdx.x == 0) blockmax[blockIdx.x] = red[0];
 }
 
+// ---- cf_max_divergence_noalloc -------------------------------------------
+// Scratch of the allocation-free divergence check: one partial maximum per
+// interior k-plane plus one result slot, in file-scope device memory.  Every
+// GPU that loads this library holds these 64 KiB until the process exits.
+constexpr int CF_NOALLOC_MAX_ROWS = 8191;
+static __device__ __align__(256) double g_divmax_rows[CF_NOALLOC_MAX_ROWS + 1];
+
+// Same per-point operator as k_max_div (divergence{2,4}, pressure.c:40-117);
+// block b reduces interior plane k = GZ + b into rowmax[b].
+template <int ORDER>
+__global__ void k_max_div_rows(Geo G, const double* u, const double* v, const double* w, double* rowmax)
+{
+    __shared__ double red[256];
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const int k = GZ + blockIdx.x;
+    double m = 0.0;
+    for (long long t = threadIdx.x; t < G.plane; t += blockDim.x) {
+        int i = (int) (t / ny), j = (int) (t - (long long) i * ny);
+        auto I = [&](int kk, int ii, int jj) {
+            ii = ii < 0 ? ii + nx : (ii >= nx ? ii - nx : ii);
+            jj = jj < 0 ? jj + ny : (jj >= ny ? jj - ny : jj);
+            return ((long long) kk * nx + ii) * ny + jj;
+        };
+        double d;
+        if (ORDER == 2) {
+            d = (u[I(k, i, j)] - u[I(k, i - 1, j)]) / G.dx + (v[I(k, i, j)] - v[I(k, i, j - 1)]) / G.dy
+              + (w[I(k, i, j)] - w[I(k - 1, i, j)]) / G.dz[k];
+        } else {
+            const int kb = GZ - 1, kt = n2 - GZ - 1;
+            double wkm2 = (k - 2 == kb - 1) ? 2.0 * w[I(kb, i, j)] - w[I(kb + 1, i, j)] : w[I(k - 2, i, j)];
+            double wkp1 = (k + 1 == kt + 1) ? 2.0 * w[I(kt, i, j)] - w[I(kt - 1, i, j)] : w[I(k + 1, i, j)];
+            d = (A1 * (u[I(k, i, j)] - u[I(k, i - 1, j)]) + A2 * (u[I(k, i + 1, j)] - u[I(k, i - 2, j)])) / G.dx
+              + (A1 * (v[I(k, i, j)] - v[I(k, i, j - 1)]) + A2 * (v[I(k, i, j + 1)] - v[I(k, i, j - 2)])) / G.dy
+              + (A1 * (w[I(k, i, j)] - w[I(k - 1, i, j)]) + A2 * (wkp1 - wkm2)) / G.dz[k];
+        }
+        m = fmax(m, fabs(d));
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) rowmax[blockIdx.x] = red[0];
+}
+
+__global__ void k_max_rows_final(const double* rowmax, int n, double* result)
+{
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) m = fmax(m, rowmax[t]);
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *result = red[0];
+}
+
 __global__ void k_zero(double* p, long long n)
 {
     for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < n;
@@ -835,6 +895,51 @@ int cf_max_divergence(cf_instance* I, double* out)
     double m = 0.0;
     for (double x : h) m = std::fmax(m, x);
     *out = m;
+    return CF_OK;
+}
+
+// Device address of g_divmax_rows on each device, looked up once per device
+// (with that device current) by the first cf_max_divergence_noalloc call there.
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_rows[256] = {};
+
+int cf_max_divergence_noalloc(cf_instance* I, double* out)
+{
+    if (!I || !out) return CF_EINVAL;
+    if (I->cfg.nz > CF_NOALLOC_MAX_ROWS) {
+        g_last_error = "cf_max_divergence_noalloc: nz exceeds its fixed scratch of "
+                       + std::to_string(CF_NOALLOC_MAX_ROWS) + " rows";
+        return CF_EINVAL;
+    }
+    if (I->device < 0 || I->device >= 256) return CF_EINVAL;
+    int prev = 0;
+    CF_CUDA(cudaGetDevice(&prev));
+    if (prev != I->device) CF_CUDA(cudaSetDevice(I->device));
+    double* rows = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_rows[I->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_divmax_rows);
+            if (e != cudaSuccess) {
+                g_last_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                if (prev != I->device) cudaSetDevice(prev);
+                return CF_ECUDA;
+            }
+            g_noalloc_rows[I->device] = (double*) p;
+        }
+        rows = g_noalloc_rows[I->device];
+    }
+    const int nz = I->cfg.nz;
+    if (I->cfg.order == 2) k_max_div_rows<2><<<nz, 256, 0, I->stream>>>(I->geo, I->u, I->v, I->w, rows);
+    else k_max_div_rows<4><<<nz, 256, 0, I->stream>>>(I->geo, I->u, I->v, I->w, rows);
+    k_max_rows_final<<<1, 256, 0, I->stream>>>(rows, nz, rows + CF_NOALLOC_MAX_ROWS);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, rows + CF_NOALLOC_MAX_ROWS, sizeof(double), cudaMemcpyDeviceToHost, I->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(I->stream);
+    if (prev != I->device) cudaSetDevice(prev);
+    CF_CUDA(e);
     return CF_OK;
 }
 
