@@ -515,12 +515,264 @@ __global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
     if (A.mc) A.c[ijk] = A.c[ijk] + A.gc[k] * (*A.mc);   // chanfast.c:603-606
 }
 
+// ------------------------------------------------- power-of-two fast path
+// N = 64, 128, 256, 512.  Each thread holds 8 elements of one line, at
+// positions t + q*T (T = N/8, q = 0..7), in registers.  One leading radix-2
+// or radix-4 stage when log2(N) is not a multiple of 3, then radix-8 stages.
+// The leading stage reads the natural slots and the last radix-8 stage
+// (Ns = T) leaves output position t + r*T in slot r, so global loads and
+// stores are in natural order and coalesced.  Between stages the values go
+// through shared memory padded by one complex per 8 (no bank conflicts).
+
+__device__ __forceinline__ int pad8(int p) { return p + (p >> 3); }
+
+template <int R>
+__device__ __forceinline__ void bfly(double2* w, int s, double c8)
+{
+    if (R == 2) {
+        double2 a = w[0], b = w[1];
+        w[0] = cadd(a, b);
+        w[1] = csub(a, b);
+    } else if (R == 4) {
+        double2 t0 = cadd(w[0], w[2]), t1 = csub(w[0], w[2]);
+        double2 t2 = cadd(w[1], w[3]), t3 = cmul_si(csub(w[1], w[3]), s);
+        w[0] = cadd(t0, t2);
+        w[2] = csub(t0, t2);
+        w[1] = cadd(t1, t3);
+        w[3] = csub(t1, t3);
+    } else {
+        double2 e[4] = {w[0], w[2], w[4], w[6]}, o[4] = {w[1], w[3], w[5], w[7]};
+        bfly<4>(e, s, c8);
+        bfly<4>(o, s, c8);
+        double2 o1 = make_double2(c8 * (o[1].x - s * o[1].y), c8 * (o[1].y + s * o[1].x));
+        double2 o2 = cmul_si(o[2], s);
+        double2 o3 = make_double2(c8 * (-o[3].x - s * o[3].y), c8 * (-o[3].y + s * o[3].x));
+        w[0] = cadd(e[0], o[0]); w[4] = csub(e[0], o[0]);
+        w[1] = cadd(e[1], o1);   w[5] = csub(e[1], o1);
+        w[2] = cadd(e[2], o2);   w[6] = csub(e[2], o2);
+        w[3] = cadd(e[3], o3);   w[7] = csub(e[3], o3);
+    }
+}
+
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+
+// In-place transform of one line; every thread of the block must call it
+// (it synchronises the block).  sl: this line's padded shared buffer.
+template <int N>
+__device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* __restrict__ tw, int sign,
+                            double c8)
+{
+    constexpr int T = N / 8;
+    constexpr int LOG = ilog2c(N);
+    constexpr int R0 = LOG % 3 == 0 ? 8 : (LOG % 3 == 1 ? 2 : 4);
+    {   // leading stage, Ns = 1: no twiddles; output position j*R0 + r
+        constexpr int NB = 8 / R0;
+#pragma unroll
+        for (int m = 0; m < NB; m++) {
+            double2 w[R0];
+#pragma unroll
+            for (int r = 0; r < R0; r++) w[r] = v[m + r * NB];
+            bfly<R0>(w, sign, c8);
+            const int j = t + m * T;
+#pragma unroll
+            for (int r = 0; r < R0; r++) sl[pad8(j * R0 + r)] = w[r];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int Ns = R0; Ns < N; Ns *= 8) {
+        double2 w[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) w[r] = sl[pad8(t + r * T)];
+        __syncthreads();
+        const int k = t % Ns;
+        const int step = N / (Ns * 8);
+#pragma unroll
+        for (int r = 1; r < 8; r++) {
+            if (k) {
+                double2 c = __ldg(&tw[r * k * step]);
+                if (sign > 0) c.y = -c.y;
+                w[r] = cmul(w[r], c);
+            }
+        }
+        bfly<8>(w, sign, c8);
+        if (Ns * 8 == N) {
+#pragma unroll
+            for (int r = 0; r < 8; r++) v[r] = w[r];
+        } else {
+            const int base = (t / Ns) * Ns * 8 + k;
+#pragma unroll
+            for (int r = 0; r < 8; r++) sl[pad8(base + r * Ns)] = w[r];
+            __syncthreads();
+        }
+    }
+}
+
+// 256 threads per block: 2048 / N lines of N / 8 threads (x transforms: the
+// lines are consecutive j, so each load or store of a warp covers runs of
+// consecutive j; y transforms: the lines are consecutive kx)
+__host__ __device__ constexpr int p2_lines(int n) { return 2048 / n; }
+__host__ __device__ constexpr int p2_pad(int n) { return n + n / 8; }
+
+template <int ORDER>
+__device__ __forceinline__ double div_point(const Geo& G, const DivArgs& A, int k, int i, int j, double uc, bool corr)
+{
+    // divergence{2,4} (pressure.c:40-117), u read as u + G_u mdpdx
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const int kb = GZ - 1, kt = n2 - GZ - 1;
+    auto I = [&](int kk, int ii, int jj) { return ((long long) kk * nx + ii) * ny + jj; };
+    auto U = [&](int di) { double t = __ldg(A.u + I(k, wrapp(i + di, nx), j)); return corr ? t + uc : t; };
+    auto V = [&](int dj) { return __ldg(A.v + I(k, i, wrapp(j + dj, ny))); };
+    auto Wr = [&](int kk) { return __ldg(A.w + I(kk, i, j)); };
+    const double dzk = G.dz[k];
+    if (ORDER == 2)
+        return (U(0) - U(-1)) / G.dx + (V(0) - V(-1)) / G.dy + (Wr(k) - Wr(k - 1)) / dzk;
+    double wkm2 = (k - 2 == kb - 1) ? 2.0 * Wr(kb) - Wr(kb + 1) : Wr(k - 2);  // pressure.c:80-87
+    double wkp1 = (k + 1 == kt + 1) ? 2.0 * Wr(kt) - Wr(kt - 1) : Wr(k + 1);  // pressure.c:88-95
+    return (A1 * (U(0) - U(-1)) + A2 * (U(1) - U(-2))) / G.dx
+         + (A1 * (V(0) - V(-1)) + A2 * (V(1) - V(-2))) / G.dy
+         + (A1 * (Wr(k) - Wr(k - 1)) + A2 * (wkp1 - wkm2)) / dzk;
+}
+
+template <int ORDER, int N>
+__global__ void __launch_bounds__(256) k_div_fftx_p2(Geo G, DivArgs A)
+{
+    extern __shared__ double2 sbuf[];
+    constexpr int T = N / 8, L = p2_lines(N);
+    const int l = threadIdx.x % L, t = threadIdx.x / L;
+    const int k = GZ + blockIdx.y;
+    const int j = blockIdx.x * L + l;
+    const bool valid = j < G.ny;
+    const bool corr = A.mu != nullptr;
+    const double uc = corr ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+        v[q] = make_double2(valid ? div_point<ORDER>(G, A, k, t + q * T, j, uc, corr) : 0.0, 0.0);
+    fft_p2_line<N>(v, t, sbuf + l * p2_pad(N), A.px.tw, -1, A.c8);
+    const double scale = 1.0 / (double) N;
+    if (!valid) return;
+    const int nkx = G.nkx;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        int kx = t + q * T;
+        if (kx < nkx)
+            A.spec[((long long) k * nkx + kx) * G.ny + j] = make_double2(v[q].x * scale, v[q].y * scale);
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
+{
+    extern __shared__ double2 sbuf[];
+    constexpr int T = N / 8, L = p2_lines(N);
+    const int t = threadIdx.x % T, l = threadIdx.x / T;
+    const int k = A.kfirst + blockIdx.y;
+    const int kx = blockIdx.x * L + l;
+    const int nkx = G.nkx;
+    const bool valid = kx < nkx;
+    double2* base = A.spec + ((long long) k * nkx + (valid ? kx : 0)) * N;
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = valid ? base[t + q * T] : make_double2(0.0, 0.0);
+    fft_p2_line<N>(v, t, sbuf + l * p2_pad(N), A.py.tw, A.sign, A.c8);
+    if (!valid) return;
+    const double scale = 1.0 / (double) N;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        double2 x = v[q];
+        if (A.sign < 0) { x.x *= scale; x.y *= scale; }
+        base[t + q * T] = x;
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
+{
+    extern __shared__ double2 sbuf[];
+    constexpr int T = N / 8, L = p2_lines(N);
+    const int l = threadIdx.x % L, t = threadIdx.x / L;
+    const int k = blockIdx.y;
+    const int j = blockIdx.x * L + l;
+    const bool valid = j < G.ny;
+    const int nkx = G.nkx, ny = G.ny;
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        int p = t + q * T;
+        double2 x = make_double2(0.0, 0.0);
+        if (valid) {
+            if (p < nkx) {
+                x = A.spec[((long long) k * nkx + p) * ny + j];
+                if (p == 0 || 2 * p == N) x.y = 0.0;   // c2r ignores these imaginary parts
+            } else {
+                x = A.spec[((long long) k * nkx + (N - p)) * ny + j];
+                x.y = -x.y;
+            }
+        }
+        v[q] = x;
+    }
+    fft_p2_line<N>(v, t, sbuf + l * p2_pad(N), A.px.tw, +1, A.c8);
+    if (!valid) return;
+#pragma unroll
+    for (int q = 0; q < 8; q++) A.p[((long long) k * G.nx + (t + q * T)) * ny + j] = v[q].x;
+}
+
+static bool is_p2(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+
+template <int N>
+static size_t p2_smem_x() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(double2); }
+template <int N>
+static size_t p2_smem_y() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(double2); }
+
+template <int N>
+static void launch_div_fftx_p2(const Geo& G, const DivArgs& A, cudaStream_t st)
+{
+    constexpr int L = p2_lines(N);
+    dim3 grd((G.ny + L - 1) / L, G.nz);
+    if (G.order == 2) k_div_fftx_p2<2, N><<<grd, 256, p2_smem_x<N>(), st>>>(G, A);
+    else k_div_fftx_p2<4, N><<<grd, 256, p2_smem_x<N>(), st>>>(G, A);
+}
+
+template <int N>
+static void launch_ffty_p2(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st)
+{
+    constexpr int L = p2_lines(N);
+    dim3 grd((G.nkx + L - 1) / L, nrows);
+    k_ffty_p2<N><<<grd, 256, p2_smem_y<N>(), st>>>(G, A);
+}
+
+template <int N>
+static void launch_c2r_p2(const Geo& G, const C2rArgs& A, cudaStream_t st)
+{
+    constexpr int L = p2_lines(N);
+    dim3 grd((G.ny + L - 1) / L, G.n2);
+    k_fftx_c2r_p2<N><<<grd, 256, p2_smem_x<N>(), st>>>(G, A);
+}
+
+template <int N>
+static cudaError_t p2_set_smem()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_div_fftx_p2<2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N>());
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx_p2<4, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N>());
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N>());
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_y<N>());
+    return e;
+}
+
 // -------------------------------------------------------------- launchers
 
 size_t fft_smem_bytes(int n) { return (size_t) n * FFT_L * sizeof(double2); }
 
 void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st)
 {
+    switch (G.nx) {
+    case 64: return launch_div_fftx_p2<64>(G, A, st);
+    case 128: return launch_div_fftx_p2<128>(G, A, st);
+    case 256: return launch_div_fftx_p2<256>(G, A, st);
+    case 512: return launch_div_fftx_p2<512>(G, A, st);
+    default: break;
+    }
     dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.nz);
     size_t sm = fft_smem_bytes(G.nx);
     if (G.order == 2) k_div_fftx<2><<<grd, FFT_THREADS, sm, st>>>(G, A);
@@ -529,12 +781,26 @@ void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st)
 
 void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st)
 {
+    switch (G.ny) {
+    case 64: return launch_ffty_p2<64>(G, A, nrows, st);
+    case 128: return launch_ffty_p2<128>(G, A, nrows, st);
+    case 256: return launch_ffty_p2<256>(G, A, nrows, st);
+    case 512: return launch_ffty_p2<512>(G, A, nrows, st);
+    default: break;
+    }
     dim3 grd((G.nkx + FFT_L - 1) / FFT_L, nrows);
     k_ffty<<<grd, FFT_THREADS, fft_smem_bytes(G.ny), st>>>(G, A);
 }
 
 void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st)
 {
+    switch (G.nx) {
+    case 64: return launch_c2r_p2<64>(G, A, st);
+    case 128: return launch_c2r_p2<128>(G, A, st);
+    case 256: return launch_c2r_p2<256>(G, A, st);
+    case 512: return launch_c2r_p2<512>(G, A, st);
+    default: break;
+    }
     dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.n2);
     k_fftx_c2r<<<grd, FFT_THREADS, fft_smem_bytes(G.nx), st>>>(G, A);
 }
@@ -557,8 +823,11 @@ void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st)
 cudaError_t fft_set_smem_limits(int max_n)
 {
     size_t sm = fft_smem_bytes(max_n);
-    cudaError_t e = cudaSuccess;
-    if (sm > 48 * 1024) {
+    cudaError_t e = p2_set_smem<64>();
+    if (e == cudaSuccess) e = p2_set_smem<128>();
+    if (e == cudaSuccess) e = p2_set_smem<256>();
+    if (e == cudaSuccess) e = p2_set_smem<512>();
+    if (e == cudaSuccess && sm > 48 * 1024) {
         int v = (int) sm;
         e = cudaFuncSetAttribute(k_div_fftx<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
