@@ -671,7 +671,7 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     CF_CUDA(cudaMemsetAsync(I->spec, 0, (size_t) G.splane * G.n2 * sizeof(double2), I->stream));
     const int nscr = C.order == 4 ? 3 : 1;
     CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
-    const long long nwarps = ((G.plane + 127) / 128) * 4;   // per-warp partial sums of k_solve
+    const long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);   // per-warp partial sums of k_solve
     CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->avg, (size_t) G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->dscal, 8 * sizeof(double)));

@@ -613,6 +613,11 @@ __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* 
 // consecutive j; y transforms: the lines are consecutive kx)
 __host__ __device__ constexpr int p2_lines(int n) { return 2048 / n; }
 __host__ __device__ constexpr int p2_pad(int n) { return n + n / 8; }
+// Line stride of the x transforms, whose consecutive lanes are different
+// lines: a quarter-warp (8 lanes of 16 bytes) spans 8 lines at one position
+// (N <= 256; an odd stride in 16-byte units puts them in 8 distinct bank
+// groups) or 4 lines at two consecutive positions (N = 512; stride = 2 mod 8).
+__host__ __device__ constexpr int p2_stride_x(int n) { return p2_pad(n) + (p2_lines(n) >= 8 ? 1 : 2); }
 
 template <int ORDER>
 __device__ __forceinline__ double div_point(const Geo& G, const DivArgs& A, int k, int i, int j, double uc, bool corr)
@@ -649,7 +654,7 @@ __global__ void __launch_bounds__(256) k_div_fftx_p2(Geo G, DivArgs A)
 #pragma unroll
     for (int q = 0; q < 8; q++)
         v[q] = make_double2(valid ? div_point<ORDER>(G, A, k, t + q * T, j, uc, corr) : 0.0, 0.0);
-    fft_p2_line<N>(v, t, sbuf + l * p2_pad(N), A.px.tw, -1, A.c8);
+    fft_p2_line<N>(v, t, sbuf + l * p2_stride_x(N), A.px.tw, -1, A.c8);
     const double scale = 1.0 / (double) N;
     if (!valid) return;
     const int nkx = G.nkx;
@@ -712,16 +717,14 @@ __global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
         }
         v[q] = x;
     }
-    fft_p2_line<N>(v, t, sbuf + l * p2_pad(N), A.px.tw, +1, A.c8);
+    fft_p2_line<N>(v, t, sbuf + l * p2_stride_x(N), A.px.tw, +1, A.c8);
     if (!valid) return;
 #pragma unroll
     for (int q = 0; q < 8; q++) A.p[((long long) k * G.nx + (t + q * T)) * ny + j] = v[q].x;
 }
 
-static bool is_p2(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
-
 template <int N>
-static size_t p2_smem_x() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(double2); }
+static size_t p2_smem_x() { return (size_t) p2_lines(N) * p2_stride_x(N) * sizeof(double2); }
 template <int N>
 static size_t p2_smem_y() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(double2); }
 

@@ -7,9 +7,13 @@
 //            + flux_quick + advect_scalar + add_buoyancy
 //            (chanfast.c:420-452 / 1344-1376) for every interior point; mass
 //            fluxes are formed on the fly and never stored.  Expressions keep
-//            the reference's evaluation order (compiled with -fmad=false).
+//            the reference's evaluation order; this file is compiled with FMA
+//            contraction (its kernels are FP64-throughput bound), so results
+//            agree with the reference to rounding.
 #include "engine.cuh"
 #include "host_band.h"
+
+#include <type_traits>
 
 namespace cf {
 
@@ -137,8 +141,45 @@ constexpr int RT_PI = RT_I + 2 * RT_H, RT_PJ = RT_J + 2 * RT_H;   // 14 x 38
 constexpr int RT_PLANE = RT_PI * RT_PJ;
 constexpr int RT_THREADS = RT_I * RT_J;
 constexpr int RT_KC = 64;   // interior rows per block
+constexpr int RT_FIELD = RT_SLOTS * RT_PLANE;                      // one field's ring
+constexpr int RT_LOADS = (RT_PLANE + RT_THREADS - 1) / RT_THREADS;  // plane points per thread
 
 size_t rhs_smem_bytes() { return (size_t) 4 * RT_SLOTS * RT_PLANE * sizeof(double); }
+
+// z fluxes of one advected field (order 4), carried up the column.  With
+// F1(k) = MZ(k) (Q(k) + Q(k+1)) / 2 and F3(k) = MZ(k+1) (Q(k) + Q(k+3)) / 2,
+// row k needs zph = F1(k), zmh = F1(k-1), zp3 = F3(k), zm3 = F3(k-3)
+// (advect.c:466-734), so each row forms one new mass flux MZ(k+1) and two
+// fluxes and takes the others from earlier rows; prime() forms the earlier
+// ones directly for the first row of a chunk.
+struct ZQueue {
+    double f1m, f3m[3], mzc, mz1, f1, f3;
+
+    // State as if row k-1 had just been processed (called at row k).
+    template <class QF, class MF>
+    __device__ __forceinline__ void prime(QF Q, MF MZ)
+    {
+        mz1 = MZ(0, 0, 0);
+        f1 = MZ(0, 0, -1) * 0.5 * (Q(0, 0, -1) + Q(0, 0, 0));
+        f3m[1] = MZ(0, 0, -2) * 0.5 * (Q(0, 0, -3) + Q(0, 0, 0));
+        f3m[2] = MZ(0, 0, -1) * 0.5 * (Q(0, 0, -2) + Q(0, 0, 1));
+        f3 = mz1 * 0.5 * (Q(0, 0, -1) + Q(0, 0, 2));
+    }
+
+    template <class QF, class MF>
+    __device__ __forceinline__ void advance(QF Q, MF MZ)
+    {
+        f1m = f1;
+        f3m[0] = f3m[1];
+        f3m[1] = f3m[2];
+        f3m[2] = f3;
+        mzc = mz1;
+        mz1 = MZ(0, 0, 1);
+        const double q0 = Q(0, 0, 0);
+        f1 = mzc * 0.5 * (q0 + Q(0, 0, 1));
+        f3 = mz1 * 0.5 * (q0 + Q(0, 0, 3));
+    }
+};
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src)
 {
@@ -155,22 +196,38 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RT_J + tx;
     const int j0 = blockIdx.x * RT_J, i0 = blockIdx.y * RT_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const long long plane = (long long) nx * ny;
     const int kb = GZ + blockIdx.z * RT_KC;
     const int ke = min(kb + RT_KC, GZ + G.nz);
-    const double* src[4] = {A.u, A.v, A.w, A.c};
 
-    auto load_plane = [&](int k) {
-        const int slot = k & (RT_SLOTS - 1);
-        for (int idx = tid; idx < 4 * RT_PLANE; idx += RT_THREADS) {
-            int f = idx / RT_PLANE, r = idx - f * RT_PLANE;
-            int ii = r / RT_PJ, jj = r - ii * RT_PJ;
-            int gi = (i0 + ii - RT_H) % nx; if (gi < 0) gi += nx;
-            int gj = (j0 + jj - RT_H) % ny; if (gj < 0) gj += ny;
-            cp_async8(sm + (f * RT_SLOTS + slot) * RT_PLANE + r, src[f] + ((long long) k * nx + gi) * ny + gj);
+    // This thread's points of a haloed plane (same in every plane): their
+    // offsets within a field plane, computed once.
+    int goff[RT_LOADS];
+#pragma unroll
+    for (int m = 0; m < RT_LOADS; m++) {
+        const int r = tid + m * RT_THREADS;
+        const int ii = r / RT_PJ, jj = r - ii * RT_PJ;
+        int gi = (i0 + ii - RT_H) % nx; if (gi < 0) gi += nx;
+        int gj = (j0 + jj - RT_H) % ny; if (gj < 0) gj += ny;
+        goff[m] = gi * ny + gj;
+    }
+    auto load_plane = [&](int kk) {
+        const long long base = (long long) kk * plane;
+        double* d0 = sm + (kk & (RT_SLOTS - 1)) * RT_PLANE + tid;
+#pragma unroll
+        for (int m = 0; m < RT_LOADS; m++) {
+            if (tid + m * RT_THREADS < RT_PLANE) {
+                double* d = d0 + m * RT_THREADS;
+                const long long o = base + goff[m];
+                cp_async8(d, A.u + o);
+                cp_async8(d + RT_FIELD, A.v + o);
+                cp_async8(d + 2 * RT_FIELD, A.w + o);
+                cp_async8(d + 3 * RT_FIELD, A.c + o);
+            }
         }
         cp_async_commit();
     };
-    for (int k = kb - 3; k <= kb + 3; k++) load_plane(k);
+    for (int kk = kb - 3; kk <= kb + 3; kk++) load_plane(kk);
     cp_async_wait_all();
     __syncthreads();
 
@@ -181,30 +238,74 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     const double* __restrict__ dxdz = G.dxdz;
     const int kb_w = GZ - 1, kt_u = n2 - GZ;   // wall ghost rows of cell-centred fields
 
-    for (int k = kb; k < ke; k++) {
-        if (k + 4 <= ke + 2) load_plane(k + 4);
-        auto at = [&](int f, int di, int dj, int dk) -> double {
-            return sm[(f * RT_SLOTS + ((k + dk) & (RT_SLOTS - 1))) * RT_PLANE + (ty + RT_H + di) * RT_PJ + (tx + RT_H + dj)];
-        };
-        auto U = [&](int di, int dj, int dk) { return at(0, di, dj, dk); };
-        auto V = [&](int di, int dj, int dk) { return at(1, di, dj, dk); };
-        auto W = [&](int di, int dj, int dk) { return at(2, di, dj, dk); };
-        auto C = [&](int di, int dj, int dk) { return at(3, di, dj, dk); };
+    int k = kb;
+    auto at = [&](int f, int di, int dj, int dk) -> double {
+        return sm[f * RT_FIELD + ((k + dk) & (RT_SLOTS - 1)) * RT_PLANE + (ty + RT_H + di) * RT_PJ + (tx + RT_H + dj)];
+    };
+    auto U = [&](int di, int dj, int dk) { return at(0, di, dj, dk); };
+    auto V = [&](int di, int dj, int dk) { return at(1, di, dj, dk); };
+    auto W = [&](int di, int dj, int dk) { return at(2, di, dj, dk); };
+    auto C = [&](int di, int dj, int dk) { return at(3, di, dj, dk); };
+
+    // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation
+    auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+        return B1 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)) + B2 * (d * U(di - 1, dj, dk) + d * U(di + 2, dj, dk)); };
+    auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+        return B1 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)) + B2 * (d * V(di - 1, dj, dk) + d * V(di + 2, dj, dk)); };
+    auto mx_w = [&](int di, int dj, int dk) {
+        return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
+    auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+        return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
+    auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+        return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
+    auto my_w = [&](int di, int dj, int dk) {
+        return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
+    auto mz_u = [&](int di, int dj, int dk) {
+        return B1 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1))
+             + B2 * (dydz[k + dk - 1] * U(di, dj, dk - 1) + dydz[k + dk + 2] * U(di, dj, dk + 2)); };
+    auto mz_v = [&](int di, int dj, int dk) {
+        return B1 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1))
+             + B2 * (dxdz[k + dk - 1] * V(di, dj, dk - 1) + dxdz[k + dk + 2] * V(di, dj, dk + 2)); };
+    auto mz_w = [&](int di, int dj, int dk) {
+        return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)) + B2 * (dxdy * W(di, dj, dk - 1) + dxdy * W(di, dj, dk + 2)); };
+    // massflux{x,y,z}2 (advect.c:6-85)
+    auto mx_u2 = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
+    auto mx_v2 = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
+    auto mx_w2 = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)); };
+    auto my_u2 = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
+    auto my_v2 = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
+    auto my_w2 = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)); };
+    auto mz_u2 = [&](int di, int dj, int dk) { return 0.5 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1)); };
+    auto mz_v2 = [&](int di, int dj, int dk) { return 0.5 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1)); };
+    auto mz_w2 = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)); };
+
+    const double qk = -0.125;   // QUICK coefficient (scalar.c:79-162)
+    auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
+        double cph = 0.5 * (c0 + c1);
+        cph += m > 0.0 ? qk * (c1 - 2.0 * c0 + cm1) : qk * (c2 - 2.0 * c1 + c0);
+        return m * cph;
+    };
+
+    // z fluxes carried up the column: the queues and the scalar flux
+    // through the bottom face, primed for the first row.
+    ZQueue zq_u{}, zq_v{}, zq_w{};
+    if (ORDER == 4) {
+        zq_u.prime(U, mx_w);
+        zq_v.prime(V, my_w);
+        zq_w.prime(W, mz_w);
+    }
+    double fzp_prev = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), C(0, 0, 0), C(0, 0, 1));
+
+    // One row.  WALL: rows within two of a wall, whose z fluxes use the wall
+    // closures (and the top row has no w point); other rows take a
+    // branch-free path.
+    auto row = [&](auto wall_tag) {
+        constexpr bool WALL = decltype(wall_tag)::value;
         const double ivol = G.ivol[k];
-        const bool do_w = k < n2 - GZ - 1;
+        const bool do_w = !WALL || k < n2 - GZ - 1;
         double fu, fv, fw = 0.0, fc;
 
         if (ORDER == 2) {
-            // massflux{x,y,z}2 (advect.c:6-85) formed on the fly
-            auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
-            auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
-            auto mx_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)); };
-            auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
-            auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
-            auto my_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)); };
-            auto mz_u = [&](int di, int dj, int dk) { return 0.5 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1)); };
-            auto mz_v = [&](int di, int dj, int dk) { return 0.5 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1)); };
-            auto mz_w = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)); };
             auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {   // advectu2 / advectv2 (advect.c:286-417)
                 double q0 = Q(0, 0, 0);
                 double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
@@ -213,20 +314,22 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
                 double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
                 double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
                 double zmh = MZ(0, 0, -1) * 0.5 * (q0 + Q(0, 0, -1));
-                if (k == n2 - GZ - 1) zph = MZ(0, 0, 0) * (0.5 * (Q(0, 0, kt_u - 1 - k) + Q(0, 0, kt_u - k)));
-                if (k == GZ) zmh = MZ(0, 0, -1) * (0.5 * (Q(0, 0, kb_w - k) + Q(0, 0, kb_w + 1 - k)));
+                if (WALL) {
+                    if (k == n2 - GZ - 1) zph = MZ(0, 0, 0) * (0.5 * (Q(0, 0, kt_u - 1 - k) + Q(0, 0, kt_u - k)));
+                    if (k == GZ) zmh = MZ(0, 0, -1) * (0.5 * (Q(0, 0, kb_w - k) + Q(0, 0, kb_w + 1 - k)));
+                }
                 return -((xph - xmh) + (yph - ymh) + (zph - zmh)) * ivol;
             };
-            fu = adv_cell(U, mx_u, mx_v, mx_w);
-            fv = adv_cell(V, my_u, my_v, my_w);
+            fu = adv_cell(U, mx_u2, mx_v2, mx_w2);
+            fv = adv_cell(V, my_u2, my_v2, my_w2);
             if (do_w) {   // advectw2 (advect.c:420-463)
                 double q0 = W(0, 0, 0);
-                double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
-                double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
-                double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
-                double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
-                double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
-                double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
+                double xph = mz_u2(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
+                double yph = mz_v2(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
+                double zph = mz_w2(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
+                double xmh = mz_u2(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
+                double ymh = mz_v2(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
+                double zmh = mz_w2(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
                 fw = -((xph - xmh) + (yph - ymh) + (zph - zmh)) * G.ivolw[k];
             }
             // add_laplacexy_operator_{u,w}2 (diffuseu.c:286-313, diffusew.c:290-317)
@@ -240,45 +343,21 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
             if (do_w) fw += lap2(W, A.nu);
             fc = lap2(C, A.kappa);
         } else {
-            // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation
-            auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
-                return B1 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)) + B2 * (d * U(di - 1, dj, dk) + d * U(di + 2, dj, dk)); };
-            auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
-                return B1 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)) + B2 * (d * V(di - 1, dj, dk) + d * V(di + 2, dj, dk)); };
-            auto mx_w = [&](int di, int dj, int dk) {
-                return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
-            auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
-                return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
-            auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
-                return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
-            auto my_w = [&](int di, int dj, int dk) {
-                return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
-            auto mz_u = [&](int di, int dj, int dk) {
-                return B1 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1))
-                     + B2 * (dydz[k + dk - 1] * U(di, dj, dk - 1) + dydz[k + dk + 2] * U(di, dj, dk + 2)); };
-            auto mz_v = [&](int di, int dj, int dk) {
-                return B1 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1))
-                     + B2 * (dxdz[k + dk - 1] * V(di, dj, dk - 1) + dxdz[k + dk + 2] * V(di, dj, dk + 2)); };
-            auto mz_w = [&](int di, int dj, int dk) {
-                return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)) + B2 * (dxdy * W(di, dj, dk - 1) + dxdy * W(di, dj, dk + 2)); };
-
             // advectu4 / advectv4 (advect.c:466-669); the wall-adjacent z
-            // fluxes use the fourth-order wall value qbot / qtop.
-            auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {
+            // fluxes use the fourth-order wall value qbot / qtop.  The z
+            // fluxes come from the per-field queue (zph / zp3 of this row,
+            // zmh / zm3 = zph of row k-1 / zp3 of row k-3).
+            auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ, double zph, double zmh, double zp3, double zm3) {
                 double q0 = Q(0, 0, 0);
                 double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
                 double yph = MY(0, 0, 0) * 0.5 * (q0 + Q(0, 1, 0));
-                double zph = MZ(0, 0, 0) * 0.5 * (q0 + Q(0, 0, 1));
                 double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
                 double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
-                double zmh = MZ(0, 0, -1) * 0.5 * (q0 + Q(0, 0, -1));
                 double xp3 = MX(1, 0, 0) * 0.5 * (q0 + Q(3, 0, 0));
                 double yp3 = MY(0, 1, 0) * 0.5 * (q0 + Q(0, 3, 0));
-                double zp3 = MZ(0, 0, 1) * 0.5 * (q0 + Q(0, 0, 3));
                 double xm3 = MX(-2, 0, 0) * 0.5 * (q0 + Q(-3, 0, 0));
                 double ym3 = MY(0, -2, 0) * 0.5 * (q0 + Q(0, -3, 0));
-                double zm3 = MZ(0, 0, -2) * 0.5 * (q0 + Q(0, 0, -3));
-                if (k >= n2 - GZ - 2 || k <= GZ + 1) {
+                if (WALL) {
                     double qbot = 0.5 * A2 * (Q(0, 0, kb_w - 1 - k) + Q(0, 0, kb_w + 2 - k))
                                 + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kb_w - k) + Q(0, 0, kb_w + 1 - k));
                     double qtop = 0.5 * A2 * (Q(0, 0, kt_u - 2 - k) + Q(0, 0, kt_u + 1 - k))
@@ -297,24 +376,23 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
                 return -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
                          + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) * ivol;
             };
-            fu = adv_cell(U, mx_u, mx_v, mx_w);
-            fv = adv_cell(V, my_u, my_v, my_w);
+            zq_u.advance(U, mx_w);
+            zq_v.advance(V, my_w);
+            fu = adv_cell(U, mx_u, mx_v, mx_w, zq_u.f1, zq_u.f1m, zq_u.f3, zq_u.f3m[0]);
+            fv = adv_cell(V, my_u, my_v, my_w, zq_v.f1, zq_v.f1m, zq_v.f3, zq_v.f3m[0]);
             if (do_w) {   // advectw4 (advect.c:672-734)
+                zq_w.advance(W, mz_w);
                 double q0 = W(0, 0, 0);
                 double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
                 double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
-                double zph = mz_w(0, 0, 0) * 0.5 * (q0 + W(0, 0, 1));
                 double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
                 double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
-                double zmh = mz_w(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
                 double xp3 = mz_u(1, 0, 0) * 0.5 * (q0 + W(3, 0, 0));
                 double yp3 = mz_v(0, 1, 0) * 0.5 * (q0 + W(0, 3, 0));
-                double zp3 = mz_w(0, 0, 1) * 0.5 * (q0 + W(0, 0, 3));
                 double xm3 = mz_u(-2, 0, 0) * 0.5 * (q0 + W(-3, 0, 0));
                 double ym3 = mz_v(0, -2, 0) * 0.5 * (q0 + W(0, -3, 0));
-                double zm3 = mz_w(0, 0, -2) * 0.5 * (q0 + W(0, 0, -3));
                 fw = -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
-                       + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) * G.ivolw[k];
+                       + (A1 * (zq_w.f1 - zq_w.f1m) + A2 * (zq_w.f3 - zq_w.f3m[0]))) * G.ivolw[k];
             }
             // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363)
             auto lap4 = [&](auto F, double nu) {
@@ -337,19 +415,14 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
         }
 
         {   // flux_quick + advect_scalar (scalar.c:79-162), order independent
-            const double q = -0.125;
-            auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
-                double cph = 0.5 * (c0 + c1);
-                cph += m > 0.0 ? q * (c1 - 2.0 * c0 + cm1) : q * (c2 - 2.0 * c1 + c0);
-                return m * cph;
-            };
             double c0 = C(0, 0, 0);
             double fxp = quick(dydz[k] * U(0, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0), C(2, 0, 0));
             double fxm = quick(dydz[k] * U(-1, 0, 0), C(-2, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0));
             double fyp = quick(dxdz[k] * V(0, 0, 0), C(0, -1, 0), c0, C(0, 1, 0), C(0, 2, 0));
             double fym = quick(dxdz[k] * V(0, -1, 0), C(0, -2, 0), C(0, -1, 0), c0, C(0, 1, 0));
             double fzp = quick(dxdy * W(0, 0, 0), C(0, 0, -1), c0, C(0, 0, 1), C(0, 0, 2));
-            double fzm = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), c0, C(0, 0, 1));
+            double fzm = fzp_prev;   // the top-face flux of row k-1
+            fzp_prev = fzp;
             fc = -((fxp - fxm) + (fyp - fym) + (fzp - fzm)) * ivol + fc;
             // add_buoyancy{2,4} (scalar.c:6-76)
             if (ORDER == 2) {
@@ -365,12 +438,18 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
             }
         }
         if (out) {
-            const long long ijk = ((long long) k * nx + i) * ny + j;
+            const long long ijk = (long long) k * plane + (long long) i * ny + j;
             A.fu[ijk] = fu;
             A.fv[ijk] = fv;
             if (do_w) A.fw[ijk] = fw;
             A.fc[ijk] = fc;
         }
+    };
+
+    for (; k < ke; k++) {
+        if (k + 4 <= ke + 2) load_plane(k + 4);
+        if (k <= GZ + 1 || k >= n2 - GZ - 2) row(std::true_type{});
+        else row(std::false_type{});
         cp_async_wait_all();
         __syncthreads();
     }

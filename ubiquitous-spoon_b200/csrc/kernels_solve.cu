@@ -75,6 +75,18 @@ __device__ __forceinline__ void bcw_top(const WallRowsD& R, double bc, double x0
     }
 }
 
+// Async 8-byte global -> shared copies whose issue is ordered with the
+// thread's other memory accesses ("memory" clobber): the ring slot a copy
+// overwrites was read just before.
+__device__ __forceinline__ void cp_async8_ordered(double* dst, const double* src)
+{
+    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_ordered() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_ordered() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 __device__ __forceinline__ double warp_sum(double v)
 {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -82,7 +94,7 @@ __device__ __forceinline__ double warp_sum(double v)
 }
 
 template <int ORDER, bool IS_W, bool SHIFT>
-__global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
+__global__ void __launch_bounds__(SOLVE_THREADS, 10) k_solve(Geo G, SolveArgs A)
 {
     const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = col < G.plane;
@@ -98,15 +110,18 @@ __global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
     // Old ghost values: cell fields carry apply_bc values already (k_ghosts);
     // face fields recompute apply_bc_w here (k_ghosts stored the massflux4
     // extrapolation there instead).
-    double gb[3], gt[3];
+    double gb0 = 0.0, gb1 = 0.0, gb2 = 0.0, gt0 = 0.0, gt1 = 0.0, gt2 = 0.0;
     if (IS_W) {
-        bcw_bot<ORDER>(A.bcb, A.bc_bot, ld(x, kb + 1), ld(x, kb + 2), gb[0], gb[1], gb[2]);
-        bcw_top<ORDER>(A.bct, A.bc_top, ld(x, kt - 1), ld(x, kt - 2), gt[0], gt[1], gt[2]);
+        bcw_bot<ORDER>(A.bcb, A.bc_bot, ld(x, kb + 1), ld(x, kb + 2), gb0, gb1, gb2);
+        bcw_top<ORDER>(A.bct, A.bc_top, ld(x, kt - 1), ld(x, kt - 2), gt0, gt1, gt2);
     }
+    // ghost value d rows beyond the bottom / top wall row
+    auto gbot = [&](int d) { return d == 0 ? gb0 : (d == 1 ? gb1 : gb2); };
+    auto gtop = [&](int d) { return d == 0 ? gt0 : (d == 1 ? gt1 : gt2); };
     auto old = [&](int k) -> double {
         if (IS_W) {
-            if (k <= kb) return gb[kb - k];
-            if (k >= kt) return gt[k - kt];
+            if (k <= kb) return gbot(kb - k);
+            if (k >= kt) return gtop(k - kt);
         }
         return ld(x, k);
     };
@@ -118,16 +133,38 @@ __global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
     for (int q = 0; q < 2 * H + 1; q++) win[q] = old(k0 - H + q);
 
     // Forward sweep: helmholtz1d_operator + RK3 combination + boundary lifting
-    // + forward elimination of tridag/heptdag, one fused row per k.
+    // + forward elimination of tridag/heptdag, one fused row per k.  The f, g
+    // and next-window values of the coming SOLVE_PF rows are in flight as
+    // cp.async copies into this thread's slots of a shared-memory ring (no
+    // registers held); none of those rows has been overwritten yet (row i
+    // writes only x[k0 + i]).
+    extern __shared__ double ring[];   // [SOLVE_PF][3][SOLVE_THREADS]
+    auto slot = [&](int i, int fld) { return ring + ((i % SOLVE_PF) * 3 + fld) * SOLVE_THREADS + threadIdx.x; };
+    auto fetch = [&](int i) {
+        if (i < n) {
+            const int k = k0 + i;
+            const int kn = min(k + H + 1, n2 - 1);   // window row entering after row i
+            cp_async8_ordered(slot(i, 0), A.f + (long long) k * P + cc);
+            cp_async8_ordered(slot(i, 1), A.g + (long long) k * P + cc);
+            cp_async8_ordered(slot(i, 2), x + (long long) kn * P + cc);
+        }
+        cp_async_commit_ordered();
+    };
+    for (int i = 0; i < SOLVE_PF; i++) fetch(i);
     double s1 = 0.0, s2 = 0.0, s3 = 0.0;
     const double shift = SHIFT ? *A.gshift : 0.0;
     const double* __restrict__ rows = A.rows;
     for (int i = 0; i < n; i++) {
         const int k = k0 + i;
         const double* r = rows + i * W;
-        double gk = ld(A.g, k);
+        cp_async_wait_ordered<SOLVE_PF - 1>();   // row i's copies have landed
+        const double fk = *slot(i, 0);
+        double gk = *slot(i, 1);
+        double xn = *slot(i, 2);
+        fetch(i + SOLVE_PF);
+        if (IS_W && k + H + 1 >= kt) xn = gtop(k + H + 1 - kt);
         if (SHIFT) gk = gk + shift;   // f += mdpdx of the previous substep (chanfast.c:516-519)
-        double s = __ldg(r + 2 * H + 3) + __ldg(r + 2 * H + 1) * ld(A.f, k) + __ldg(r + 2 * H + 2) * gk;
+        double s = __ldg(r + 2 * H + 3) + __ldg(r + 2 * H + 1) * fk + __ldg(r + 2 * H + 2) * gk;
 #pragma unroll
         for (int q = 0; q < 2 * H + 1; q++) s += __ldg(r + q) * win[q];
         s -= __ldg(r + 2 * H + 4) * s1;
@@ -136,38 +173,57 @@ __global__ void __launch_bounds__(128) k_solve(Geo G, SolveArgs A)
         if (active) x[(long long) k * P + col] = s;
 #pragma unroll
         for (int q = 0; q < 2 * H; q++) win[q] = win[q + 1];
-        win[2 * H] = (i + 1 < n) ? old(k + H + 1) : 0.0;
+        win[2 * H] = (i + 1 < n) ? xn : 0.0;
     }
+    cp_async_wait_ordered<0>();
 
-    // back substitution
+    constexpr int PD = 4;   // back-substitution rows loaded ahead
+    // Back substitution, reading s PD rows ahead (below) the row being written.
+    double ps[PD];
+    auto fetch_s = [&](int i, int slot) {
+        if (i >= 0) ps[slot] = ld(x, k0 + i);
+    };
+#pragma unroll
+    for (int u = 0; u < PD; u++) fetch_s(n - 1 - u, u);
     double y1 = 0.0, y2 = 0.0, y3 = 0.0;
-    double top[3] = {0, 0, 0}, bot[3] = {0, 0, 0};
+    double top0 = 0.0, top1 = 0.0, top2 = 0.0, bot0 = 0.0, bot1 = 0.0, bot2 = 0.0;
     const bool stats = A.partial != nullptr;
     const long long wrow = ((long long) blockIdx.x * blockDim.x + threadIdx.x) / 32;
-    for (int i = n - 1; i >= 0; i--) {
-        const int k = k0 + i;
-        double s = active ? x[(long long) k * P + col] : 0.0;
-        double y;
-        if (ORDER == 2) y = s - __ldg(A.fac.P + i) * y1;
-        else y = s - __ldg(A.fac.P + i) * y1 - __ldg(A.fac.Q + i) * y2 - __ldg(A.fac.R + i) * y3;
-        y3 = y2; y2 = y1; y1 = y;
-        if (active) x[(long long) k * P + col] = y;
-        if (i >= n - 3) top[n - 1 - i] = y;
-        if (i < 3) bot[i] = y;
-        if (stats) {
-            double t = warp_sum(active ? y : 0.0);
-            if ((threadIdx.x & 31) == 0) A.partial[wrow * n2 + k] = t;
+    for (int i0 = n - 1; i0 >= 0; i0 -= PD) {
+#pragma unroll
+        for (int u = 0; u < PD; u++) {
+            const int i = i0 - u;
+            if (i >= 0) {
+                const int k = k0 + i;
+                const double s = ps[u];
+                fetch_s(i - PD, u);
+                double y;
+                if (ORDER == 2) y = s - __ldg(A.fac.P + i) * y1;
+                else y = s - __ldg(A.fac.P + i) * y1 - __ldg(A.fac.Q + i) * y2 - __ldg(A.fac.R + i) * y3;
+                y3 = y2; y2 = y1; y1 = y;
+                if (active) x[(long long) k * P + col] = y;
+                if (i == n - 1) top0 = y;
+                if (i == n - 2) top1 = y;
+                if (i == n - 3) top2 = y;
+                if (i == 0) bot0 = y;
+                if (i == 1) bot1 = y;
+                if (i == 2) bot2 = y;
+                if (stats) {
+                    double t = warp_sum(active ? y : 0.0);
+                    if ((threadIdx.x & 31) == 0) A.partial[wrow * n2 + k] = t;
+                }
+            }
         }
     }
 
     // apply_bc after the solve (chanfast.c:481-482)
     double b1, b2, b3, t1, t2, t3;
     if (IS_W) {
-        bcw_bot<ORDER>(A.bcb, A.bc_bot, bot[0], bot[1], b1, b2, b3);
-        bcw_top<ORDER>(A.bct, A.bc_top, top[0], top[1], t1, t2, t3);
+        bcw_bot<ORDER>(A.bcb, A.bc_bot, bot0, bot1, b1, b2, b3);
+        bcw_top<ORDER>(A.bct, A.bc_top, top0, top1, t1, t2, t3);
     } else {
-        bcu_bot<ORDER>(A.bcb, A.bc_bot, bot[0], bot[1], bot[2], b1, b2, b3);
-        bcu_top<ORDER>(A.bct, A.bc_top, top[0], top[1], top[2], t1, t2, t3);
+        bcu_bot<ORDER>(A.bcb, A.bc_bot, bot0, bot1, bot2, b1, b2, b3);
+        bcu_top<ORDER>(A.bct, A.bc_top, top0, top1, top2, t1, t2, t3);
     }
     if (active) {
         x[(long long) kb * P + col] = b1;
@@ -256,9 +312,8 @@ __global__ void k_mass_control(MassArgs A)
 
 void launch_solve(const Geo& G, const SolveArgs& A, bool is_w, bool shift, cudaStream_t st)
 {
-    int th = 128;
-    unsigned nb = (unsigned) ((G.plane + th - 1) / th);
-#define CF_SOLVE(O, W, S) k_solve<O, W, S><<<nb, th, 0, st>>>(G, A)
+    unsigned nb = (unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS);
+#define CF_SOLVE(O, W, S) k_solve<O, W, S><<<nb, SOLVE_THREADS, solve_smem_bytes(), st>>>(G, A)
     if (G.order == 2) {
         if (is_w) CF_SOLVE(2, true, false);
         else if (shift) CF_SOLVE(2, false, true);
@@ -273,7 +328,7 @@ void launch_solve(const Geo& G, const SolveArgs& A, bool is_w, bool shift, cudaS
 
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st)
 {
-    long long nwarps = ((G.plane + 127) / 128) * 4;   // k_solve launches 128-thread blocks
+    long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);
     double scale = 1.0 / ((double) G.nx * (double) G.ny);
     k_row_average<<<G.n2, 256, 0, st>>>(partial, nwarps, G.n2, scale, avg);
     k_mass_control<<<1, 32, 0, st>>>(M);
