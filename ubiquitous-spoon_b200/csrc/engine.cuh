@@ -133,11 +133,17 @@ struct PoissonArgs {
     double2* spec;
     double* scratch;          // width 3: 1 x [n2][ncol]; width 7: 3 x [n2][ncol]
     const double *a, *b, *c, *e, *f, *g, *dpart, *dvol, *lamx, *lamy;
+    const double *cx, *cy;    // dvol dt / dx^2, dvol dt / dy^2 per row
     double red[2][6][7];
     double dsub[2][6][3];
     WallRowsD bot[2], top;
     double dt, dxdx, dydy;
 };
+
+constexpr int POIS_THREADS = 128;  // k_poisson block: one thread per (kx, ky) column
+constexpr int POIS_PF = 8;         // forward rows in flight per thread
+constexpr int POIS_PB = 2;         // back-substitution rows loaded ahead (registers)
+inline size_t pois_smem_bytes() { return (size_t) POIS_PF * POIS_THREADS * 16; }
 
 struct ProjArgs {
     double *u, *v, *w, *c;

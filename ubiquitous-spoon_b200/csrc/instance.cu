@@ -294,7 +294,7 @@ struct SetOffsets {
 };
 
 struct PoissonOffsets {
-    size_t a, b, c, e, f, g, dpart, dvol;
+    size_t a, b, c, e, f, g, dpart, dvol, cx, cy;
     PoissonSet host;
 };
 
@@ -396,6 +396,13 @@ int build_tables(cf_instance* I, double dt)
         po.a = A.add(po.host.a); po.b = A.add(po.host.b); po.c = A.add(po.host.c);
         po.e = A.add(po.host.e); po.f = A.add(po.host.f); po.g = A.add(po.host.g);
         po.dpart = A.add(po.host.dpart); po.dvol = A.add(po.host.dvol);
+        // diagonal factors of the wavenumber terms (pressure.c:326-327, 414-415)
+        std::vector<double> cx(po.host.dvol.size()), cy(po.host.dvol.size());
+        for (size_t k = 0; k < cx.size(); k++) {
+            cx[k] = po.host.dvol[k] * pdt / (m.dx * m.dx);
+            cy[k] = po.host.dvol[k] * pdt / (m.dy * m.dy);
+        }
+        po.cx = A.add(cx); po.cy = A.add(cy);
     };
     for (int s = 0; s < 3; s++) addpois(I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt);
     addpois(I->pois_init, 1.0);
@@ -462,6 +469,7 @@ PoissonArgs poisson_args(cf_instance* I, const PoissonOffsets& po, double pdt)
     A.scratch = I->scratch;
     A.a = b + po.a; A.b = b + po.b; A.c = b + po.c; A.e = b + po.e; A.f = b + po.f; A.g = b + po.g;
     A.dpart = b + po.dpart; A.dvol = b + po.dvol;
+    A.cx = b + po.cx; A.cy = b + po.cy;
     A.lamx = I->lamx;
     A.lamy = I->lamy;
     std::memcpy(A.red, po.host.red, sizeof(A.red));

@@ -273,6 +273,17 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
 
 // ------------------------------------------------------------ Poisson in z
 
+// Async global -> shared copies ordered with the thread's other memory
+// accesses ("memory" clobber): a ring slot is refilled right after it is read.
+__device__ __forceinline__ void cp_async16_ordered(double2* dst, const double2* src)
+{
+    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_ordered() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_ordered() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 
 template <int ORDER>
 __device__ __forceinline__ void fill_bot(const WallRowsD& R, double x0, double x1, double x2,
@@ -307,7 +318,7 @@ __device__ __forceinline__ void fill_top(const WallRowsD& R, double x0, double x
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_poisson(Geo G, PoissonArgs A)
+__global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs A)
 {
     const long long ncol = G.splane;
     const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
@@ -324,8 +335,7 @@ __global__ void __launch_bounds__(128) k_poisson(Geo G, PoissonArgs A)
     auto coef = [&](int i, double* cf) {
         const int k = GZ + i;
         const int q = bq(i);
-        const double dv = A.dvol[k];
-        double d = (A.dpart[k] - lamx * dv * A.dt / A.dxdx) - lamy * dv * A.dt / A.dydy;
+        double d = (A.dpart[k] - lamx * A.cx[k]) - lamy * A.cy[k];   // cx = dv dt / dx^2, cy = dv dt / dy^2
         if (q >= 0) {
             d = ((d - A.dsub[var][q][0]) - A.dsub[var][q][1]) - A.dsub[var][q][2];
             for (int t = 0; t < 7; t++) cf[t] = A.red[var][q][t];
@@ -390,78 +400,89 @@ __global__ void __launch_bounds__(128) k_poisson(Geo G, PoissonArgs A)
         return;
     }
 
-    // heptdag.c:5-61 with per-column pivots; p, q, r spill to scratch
+    // heptdag.c:5-61 with per-column pivots; p, q, r spill to scratch.  One
+    // elimination formula serves every row: with zero history (p, q, r, s of
+    // rows -3..-1) it reduces exactly to the special forms of rows 0..2.
+    // In the forward sweep each thread keeps the spectrum values of the next
+    // POIS_PF rows in flight as cp.async copies into its own slots of a
+    // shared-memory ring; none of those rows has been rewritten yet.
     double* Pp = A.scratch;
     double* Qp = A.scratch + (long long) n2 * ncol;
     double* Rp = A.scratch + 2 * (long long) n2 * ncol;
     auto at = [&](double* base, int k) -> double& { return base[(long long) k * ncol + col]; };
+    extern __shared__ double2 pring[];
+    const int t = threadIdx.x;
+    auto fslot = [&](int i) { return pring + (i % POIS_PF) * POIS_THREADS + t; };
+    auto ffetch = [&](int i) {
+        if (i < nz) cp_async16_ordered(fslot(i), &S(GZ + i));
+        cp_async_commit_ordered();
+    };
+    for (int i = 0; i < POIS_PF; i++) ffetch(i);
     double p3 = 0, q3 = 0, r3 = 0, p2 = 0, q2 = 0, r2 = 0, p1 = 0, q1 = 0, r1 = 0;   // rows i-3, i-2, i-1
     double2 s3 = make_double2(0, 0), s2 = s3, s1 = s3;
     double cf[7];
     for (int i = 0; i < nz; i++) {
         const int k = GZ + i;
+        cp_async_wait_ordered<POIS_PF - 1>();
+        double2 h = *fslot(i);
+        ffetch(i + POIS_PF);
         coef(i, cf);
         const double a = cf[0], b = cf[1], c = cf[2], d = cf[3], e = cf[4], f = cf[5], g = cf[6];
-        double2 h = S(k);
         const double dv = A.dvol[k];
         h.x = h.x * dv;
         h.y = h.y * dv;
-        double den, p, q, r;
-        double2 s;
-        double iden;
-        if (i == 0) {
-            den = d;
-            iden = 1.0 / den;
-            p = e * iden; q = f * iden; r = g * iden;
-            s = make_double2(h.x * iden, h.y * iden);
-        } else if (i == 1) {
-            den = d - c * p1;
-            iden = 1.0 / den;
-            p = (e - c * q1) * iden; q = (f - c * r1) * iden; r = g * iden;
-            s = make_double2((h.x - c * s1.x) * iden, (h.y - c * s1.y) * iden);
-        } else if (i == 2) {
-            double bet = c - b * p2;
-            den = d - b * q2 - bet * p1;
-            iden = 1.0 / den;
-            p = (e - b * r2 - bet * q1) * iden; q = (f - bet * r1) * iden; r = g * iden;
-            s = make_double2((h.x - b * s2.x - bet * s1.x) * iden, (h.y - b * s2.y - bet * s1.y) * iden);
-        } else {
-            double alp = b - a * p3;
-            double bet = c - a * q3 - alp * p2;
-            den = d - a * r3 - alp * q2 - bet * p1;
-            iden = 1.0 / den;
-            p = (e - alp * r2 - bet * q1) * iden;
-            q = (f - bet * r1) * iden;
-            r = g * iden;
-            s = make_double2((h.x - a * s3.x - alp * s2.x - bet * s1.x) * iden,
-                             (h.y - a * s3.y - alp * s2.y - bet * s1.y) * iden);
-        }
+        const double alp = b - a * p3;
+        const double bet = c - a * q3 - alp * p2;
+        const double den = d - a * r3 - alp * q2 - bet * p1;
+        const double iden = 1.0 / den;
+        const double p = (e - alp * r2 - bet * q1) * iden;
+        const double q = (f - bet * r1) * iden;
+        const double r = g * iden;
+        const double2 sv = make_double2((h.x - a * s3.x - alp * s2.x - bet * s1.x) * iden,
+                                        (h.y - a * s3.y - alp * s2.y - bet * s1.y) * iden);
         at(Pp, k) = p; at(Qp, k) = q; at(Rp, k) = r;
-        S(k) = s;
+        S(k) = sv;
         p3 = p2; q3 = q2; r3 = r2; p2 = p1; q2 = q1; r2 = r1; p1 = p; q1 = q; r1 = r;
-        s3 = s2; s2 = s1; s1 = s;
+        s3 = s2; s2 = s1; s1 = sv;
     }
-    // back substitution (heptdag.c:50-55)
-    double2 x1 = S(GZ + nz - 1), x2 = make_double2(0, 0), x3 = x2;
-    double2 tp[3], bt[3];
-    tp[0] = x1;
-    for (int i = nz - 2; i >= 0; i--) {
-        const int k = GZ + i;
-        double2 sv = S(k);
-        double p = at(Pp, k), q = at(Qp, k), r = at(Rp, k);
-        double2 xv;
-        if (i == nz - 2) {
-            xv = make_double2(sv.x - p * x1.x, sv.y - p * x1.y);
-        } else if (i == nz - 3) {
-            xv = make_double2(sv.x - p * x1.x - q * x2.x, sv.y - p * x1.y - q * x2.y);
-        } else {
-            xv = make_double2(sv.x - p * x1.x - q * x2.x - r * x3.x, sv.y - p * x1.y - q * x2.y - r * x3.y);
+    cp_async_wait_ordered<0>();
+
+    // back substitution (heptdag.c:50-55), same general form (x2 = x3 = 0 at
+    // the top).  s, p, q, r of row i - POIS_PB are loaded into registers while
+    // row i is computed (plain loads: these rows were stored by this thread).
+    double2 ls[POIS_PB];
+    double lp[POIS_PB], lq[POIS_PB], lr[POIS_PB];
+    auto bload = [&](int i, int u) {
+        if (i >= 0) {
+            const int k = GZ + i;
+            ls[u] = S(k); lp[u] = at(Pp, k); lq[u] = at(Qp, k); lr[u] = at(Rp, k);
         }
-        S(k) = xv;
-        x3 = x2; x2 = x1; x1 = xv;
-        if (i >= nz - 3) tp[nz - 1 - i] = xv;
-        if (i < 3) bt[i] = xv;
+    };
+#pragma unroll
+    for (int u = 0; u < POIS_PB; u++) bload(nz - 2 - u, u);
+    double2 x1 = S(GZ + nz - 1), x2 = make_double2(0, 0), x3 = x2;
+    for (int i0 = nz - 2; i0 >= 0; i0 -= POIS_PB) {
+#pragma unroll
+        for (int u = 0; u < POIS_PB; u++) {
+            const int i = i0 - u;
+            if (i >= 0) {
+                const double2 sv = ls[u];
+                const double p = lp[u], q = lq[u], r = lr[u];
+                bload(i - POIS_PB, u);
+                const double2 xv = make_double2(sv.x - p * x1.x - q * x2.x - r * x3.x,
+                                                sv.y - p * x1.y - q * x2.y - r * x3.y);
+                S(GZ + i) = xv;
+                x3 = x2; x2 = x1; x1 = xv;
+            }
+        }
     }
+    // wall rows of the solution: bottom rows 0..2 are the last three results,
+    // top rows nz-1..nz-3 are read back
+    double2 bt[3] = {x1, x2, x3};
+    if (nz < 3)
+        for (int i = 0; i < 3; i++) bt[i] = i < nz ? S(GZ + i) : make_double2(0.0, 0.0);
+    double2 tp[3];
+    for (int i = 0; i < 3; i++) tp[i] = nz - 1 - i >= 0 ? S(GZ + nz - 1 - i) : make_double2(0.0, 0.0);
     double g1, g2, g3, h1, h2, h3;
     fill_bot<4>(A.bot[var], bt[0].x, bt[1].x, bt[2].x, g1, g2, g3);
     fill_bot<4>(A.bot[var], bt[0].y, bt[1].y, bt[2].y, h1, h2, h3);
@@ -810,9 +831,9 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st)
 
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
 {
-    unsigned nb = (unsigned) ((G.splane + 127) / 128);
-    if (G.order == 2) k_poisson<2><<<nb, 128, 0, st>>>(G, A);
-    else k_poisson<4><<<nb, 128, 0, st>>>(G, A);
+    unsigned nb = (unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS);
+    if (G.order == 2) k_poisson<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
+    else k_poisson<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
 }
 
 void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st)
