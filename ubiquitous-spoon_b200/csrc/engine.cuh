@@ -42,6 +42,7 @@ struct Geo {
     const double* ivol;   // 1 / (dx*dy*dz[k])       cell volume
     const double* ivolw;  // 1 / (dx*dy*dzp1h[k])    w-face volume
     const double* idzp1h; // 1 / dzp1h[k]
+    const double* idz;    // 1 / dz[k]
     double dxdy;          // dx*dy
     double idx, idy;      // 1/dx, 1/dy
 };

@@ -419,9 +419,10 @@ int build_tables(cf_instance* I, double dt)
         dydz[k] = m.dy * m.dz[k];
         dxdz[k] = m.dx * m.dz[k];
     }
-    std::vector<double> ivol(n2, 0.0), ivolw(n2, 0.0), idzp1h(n2, 0.0);
+    std::vector<double> ivol(n2, 0.0), ivolw(n2, 0.0), idzp1h(n2, 0.0), idz(n2, 0.0);
     for (int k = 0; k < n2; k++) {
         ivol[k] = 1.0 / (m.dx * m.dy * m.dz[k]);
+        idz[k] = 1.0 / m.dz[k];
         if (k + 1 < n2) {
             ivolw[k] = 1.0 / (m.dx * m.dy * dzp1h[k]);
             idzp1h[k] = 1.0 / dzp1h[k];
@@ -429,7 +430,7 @@ int build_tables(cf_instance* I, double dt)
     }
     size_t o_dz = A.add(m.dz), o_p1 = A.add(dzp1h), o_m1 = A.add(dzm1h), o_p3 = A.add(dzp3h),
            o_m3 = A.add(dzm3h), o_dydz = A.add(dydz), o_dxdz = A.add(dxdz), o_iv = A.add(ivol),
-           o_ivw = A.add(ivolw), o_idz = A.add(idzp1h);
+           o_ivw = A.add(ivolw), o_idz = A.add(idzp1h), o_idzc = A.add(idz);
     size_t o_zp = A.add(z_at_p(m));
 
     if (I->coef) { cudaFree(I->coef); I->coef = nullptr; }
@@ -440,6 +441,7 @@ int build_tables(cf_instance* I, double dt)
     G.dz = b + o_dz; G.dzp1h = b + o_p1; G.dzm1h = b + o_m1; G.dzp3h = b + o_p3; G.dzm3h = b + o_m3;
     G.dydz = b + o_dydz; G.dxdz = b + o_dxdz; G.ivol = b + o_iv; G.ivolw = b + o_ivw;
     G.idzp1h = b + o_idz;
+    G.idz = b + o_idzc;
     I->lamx = b + o_lamx;
     I->lamy = b + o_lamy;
     I->zp = b + o_zp;

@@ -650,14 +650,15 @@ __device__ __forceinline__ double div_point(const Geo& G, const DivArgs& A, int 
     auto U = [&](int di) { double t = __ldg(A.u + I(k, wrapp(i + di, nx), j)); return corr ? t + uc : t; };
     auto V = [&](int dj) { return __ldg(A.v + I(k, i, wrapp(j + dj, ny))); };
     auto Wr = [&](int kk) { return __ldg(A.w + I(kk, i, j)); };
-    const double dzk = G.dz[k];
+    // divisions by the metrics are multiplications by their reciprocals
+    const double idzk = G.idz[k];
     if (ORDER == 2)
-        return (U(0) - U(-1)) / G.dx + (V(0) - V(-1)) / G.dy + (Wr(k) - Wr(k - 1)) / dzk;
+        return (U(0) - U(-1)) * G.idx + (V(0) - V(-1)) * G.idy + (Wr(k) - Wr(k - 1)) * idzk;
     double wkm2 = (k - 2 == kb - 1) ? 2.0 * Wr(kb) - Wr(kb + 1) : Wr(k - 2);  // pressure.c:80-87
     double wkp1 = (k + 1 == kt + 1) ? 2.0 * Wr(kt) - Wr(kt - 1) : Wr(k + 1);  // pressure.c:88-95
-    return (A1 * (U(0) - U(-1)) + A2 * (U(1) - U(-2))) / G.dx
-         + (A1 * (V(0) - V(-1)) + A2 * (V(1) - V(-2))) / G.dy
-         + (A1 * (Wr(k) - Wr(k - 1)) + A2 * (wkp1 - wkm2)) / dzk;
+    return (A1 * (U(0) - U(-1)) + A2 * (U(1) - U(-2))) * G.idx
+         + (A1 * (V(0) - V(-1)) + A2 * (V(1) - V(-2))) * G.idy
+         + (A1 * (Wr(k) - Wr(k - 1)) + A2 * (wkp1 - wkm2)) * idzk;
 }
 
 template <int ORDER, int N>
