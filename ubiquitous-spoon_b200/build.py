@@ -6,10 +6,11 @@ Produces libchanfast_cuda.so (device engine + cf_* C ABI) and libchanfast.so
 (drop-in chanfast2/chanfast4 drivers in C) in this directory.  Device code is
 compiled with -fmad=false so that multiply-add sequences round like the
 reference CPU build (x86-64, no FMA contraction), except the files listed in
-FMA_SOURCES: their kernels are FP64-throughput bound, and contracting a
-multiply and an add into one fused operation (one rounding instead of two)
-cuts their instruction count; results then differ from the reference by
-rounding only.
+FMA_SOURCES (the substep kernels): contracting a multiply and an add into
+one fused operation (one rounding instead of two) cuts their FP64 instruction
+count and the latency of their recurrences; results then differ from the
+reference by rounding only.  instance.cu keeps -fmad=false: its seeded
+initial state must equal the reference's bit for bit.
 """
 from __future__ import annotations
 
@@ -26,7 +27,7 @@ CC = os.environ.get("CC", "gcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["host_band.cpp", "kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu", "instance.cu"]
-FMA_SOURCES = {"kernels_rhs.cu"}
+FMA_SOURCES = {"kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu"}
 LIB_CUDA = os.path.join(HERE, "libchanfast_cuda.so")
 LIB_DRIVER = os.path.join(HERE, "libchanfast.so")
 

@@ -723,21 +723,18 @@ __global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
     const int j = blockIdx.x * L + l;
     const bool valid = j < G.ny;
     const int nkx = G.nkx, ny = G.ny;
+    // Hermitian completion: position p > N/2 holds conj(spec[N - p]); all
+    // eight loads are issued unconditionally (a row of this plane) so they
+    // are in flight together
+    const double2* base = A.spec + (long long) k * nkx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-        int p = t + q * T;
-        double2 x = make_double2(0.0, 0.0);
-        if (valid) {
-            if (p < nkx) {
-                x = A.spec[((long long) k * nkx + p) * ny + j];
-                if (p == 0 || 2 * p == N) x.y = 0.0;   // c2r ignores these imaginary parts
-            } else {
-                x = A.spec[((long long) k * nkx + (N - p)) * ny + j];
-                x.y = -x.y;
-            }
-        }
-        v[q] = x;
+        const int p = t + q * T;
+        const bool lo = p < nkx;
+        v[q] = __ldg(base + (long long) (lo ? p : N - p) * ny);
+        if (!lo) v[q].y = -v[q].y;
+        if (p == 0 || 2 * p == N) v[q].y = 0.0;   // c2r ignores these imaginary parts
     }
     fft_p2_line<N>(v, t, sbuf + l * p2_stride_x(N), A.px.tw, +1, A.c8);
     if (!valid) return;
