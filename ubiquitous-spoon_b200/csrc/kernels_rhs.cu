@@ -141,6 +141,10 @@ constexpr int RT_PI = RT_I + 2 * RT_H, RT_PJ = RT_J + 2 * RT_H;   // 14 x 38
 constexpr int RT_PLANE = RT_PI * RT_PJ;
 constexpr int RT_THREADS = RT_I * RT_J;
 constexpr int RT_KC = 64;   // interior rows per block
+constexpr double B1h = 0.5 * B1, B2h = 0.5 * B2;   // halved interpolation weights (exact)
+// 7-point form of the fourth-order staggered second difference:
+// A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) = L1 (F1+F-1-2F0) + L2 (F2+F-2-2F0) + L3 (F3+F-3-2F0)
+constexpr double L1 = A1 * A1 - 2.0 * A1 * A2, L2 = 2.0 * A1 * A2, L3 = A2 * A2;
 constexpr int RT_FIELD = RT_SLOTS * RT_PLANE;                      // one field's ring
 constexpr int RT_LOADS = (RT_PLANE + RT_THREADS - 1) / RT_THREADS;  // plane points per thread
 
@@ -234,6 +238,7 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     const int i = i0 + ty, j = j0 + tx;
     const bool out = i < nx && j < ny;
     const double dxdy = G.dxdy, idx = G.idx, idy = G.idy;
+    const double idx2 = idx * idx, idy2 = idy * idy;
     const double* __restrict__ dydz = G.dydz;
     const double* __restrict__ dxdz = G.dxdz;
     const int kb_w = GZ - 1, kt_u = n2 - GZ;   // wall ghost rows of cell-centred fields
@@ -343,20 +348,31 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
             if (do_w) fw += lap2(W, A.nu);
             fc = lap2(C, A.kappa);
         } else {
-            // advectu4 / advectv4 (advect.c:466-669); the wall-adjacent z
-            // fluxes use the fourth-order wall value qbot / qtop.  The z
-            // fluxes come from the per-field queue (zph / zp3 of this row,
-            // zmh / zm3 = zph of row k-1 / zp3 of row k-3).
-            auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ, double zph, double zmh, double zp3, double zm3) {
-                double q0 = Q(0, 0, 0);
-                double xph = MX(0, 0, 0) * 0.5 * (q0 + Q(1, 0, 0));
-                double yph = MY(0, 0, 0) * 0.5 * (q0 + Q(0, 1, 0));
-                double xmh = MX(-1, 0, 0) * 0.5 * (q0 + Q(-1, 0, 0));
-                double ymh = MY(0, -1, 0) * 0.5 * (q0 + Q(0, -1, 0));
-                double xp3 = MX(1, 0, 0) * 0.5 * (q0 + Q(3, 0, 0));
-                double yp3 = MY(0, 1, 0) * 0.5 * (q0 + Q(0, 3, 0));
-                double xm3 = MX(-2, 0, 0) * 0.5 * (q0 + Q(-3, 0, 0));
-                double ym3 = MY(0, -2, 0) * 0.5 * (q0 + Q(0, -3, 0));
+            // advectu4 / advectv4 / advectw4 (advect.c:466-734).  Within one
+            // cell every x-direction mass flux carries the same metric
+            // (dydz[k] for the u-flux, dxdz[k] for the v-flux), so it is
+            // factored out of the x and y flux sums; the halved interpolation
+            // weights B1h, B2h absorb the 0.5 of the face value (an exact
+            // scaling).  Mathematically the reference's sums; they round
+            // differently.  The wall-adjacent z fluxes use the fourth-order
+            // wall value qbot / qtop; the z fluxes come from the per-field
+            // queue (zph / zp3 of this row, zmh / zm3 = zph of row k-1 / zp3
+            // of row k-3).
+            auto ix = [&](auto F, int di, int dj) {   // x interpolation to the face i+di+1/2
+                return B1h * (F(di, dj, 0) + F(di + 1, dj, 0)) + B2h * (F(di - 1, dj, 0) + F(di + 2, dj, 0));
+            };
+            auto iy = [&](auto F, int di, int dj) {   // y interpolation to the face j+dj+1/2
+                return B1h * (F(di, dj, 0) + F(di, dj + 1, 0)) + B2h * (F(di, dj - 1, 0) + F(di, dj + 2, 0));
+            };
+            auto xflux = [&](auto Q, auto M, double q0) {   // A1 (xph - xmh) + A2 (xp3 - xm3), metric factored out
+                return A1 * (M(0, 0) * (q0 + Q(1, 0, 0)) - M(-1, 0) * (q0 + Q(-1, 0, 0)))
+                     + A2 * (M(1, 0) * (q0 + Q(3, 0, 0)) - M(-2, 0) * (q0 + Q(-3, 0, 0)));
+            };
+            auto yflux = [&](auto Q, auto M, double q0) {
+                return A1 * (M(0, 0) * (q0 + Q(0, 1, 0)) - M(0, -1) * (q0 + Q(0, -1, 0)))
+                     + A2 * (M(0, 1) * (q0 + Q(0, 3, 0)) - M(0, -2) * (q0 + Q(0, -3, 0)));
+            };
+            auto zsum = [&](auto Q, auto MZ, double zph, double zmh, double zp3, double zm3) {
                 if (WALL) {
                     double qbot = 0.5 * A2 * (Q(0, 0, kb_w - 1 - k) + Q(0, 0, kb_w + 2 - k))
                                 + 0.5 * (A1 + 2.0 * A2) * (Q(0, 0, kb_w - k) + Q(0, 0, kb_w + 1 - k));
@@ -373,40 +389,52 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
                     }
                     if (k == GZ + 1) zm3 = MZ(0, 0, -2) * qbot;
                 }
-                return -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
-                         + (A1 * (zph - zmh) + A2 * (zp3 - zm3))) * ivol;
+                return A1 * (zph - zmh) + A2 * (zp3 - zm3);
             };
+            const double mdy = dydz[k], mdx = dxdz[k];
             zq_u.advance(U, mx_w);
             zq_v.advance(V, my_w);
-            fu = adv_cell(U, mx_u, mx_v, mx_w, zq_u.f1, zq_u.f1m, zq_u.f3, zq_u.f3m[0]);
-            fv = adv_cell(V, my_u, my_v, my_w, zq_v.f1, zq_v.f1m, zq_v.f3, zq_v.f3m[0]);
-            if (do_w) {   // advectw4 (advect.c:672-734)
+            {
+                const double q0 = U(0, 0, 0);
+                auto mu = [&](int di, int dj) { return ix(U, di, dj); };
+                auto mv = [&](int di, int dj) { return ix(V, di, dj); };
+                fu = -((mdy * xflux(U, mu, q0) + mdx * yflux(U, mv, q0))
+                       + zsum(U, mx_w, zq_u.f1, zq_u.f1m, zq_u.f3, zq_u.f3m[0])) * ivol;
+            }
+            {
+                const double q0 = V(0, 0, 0);
+                auto mu = [&](int di, int dj) { return iy(U, di, dj); };
+                auto mv = [&](int di, int dj) { return iy(V, di, dj); };
+                fv = -((mdy * xflux(V, mu, q0) + mdx * yflux(V, mv, q0))
+                       + zsum(V, my_w, zq_v.f1, zq_v.f1m, zq_v.f3, zq_v.f3m[0])) * ivol;
+            }
+            if (do_w) {
                 zq_w.advance(W, mz_w);
-                double q0 = W(0, 0, 0);
-                double xph = mz_u(0, 0, 0) * 0.5 * (q0 + W(1, 0, 0));
-                double yph = mz_v(0, 0, 0) * 0.5 * (q0 + W(0, 1, 0));
-                double xmh = mz_u(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
-                double ymh = mz_v(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
-                double xp3 = mz_u(1, 0, 0) * 0.5 * (q0 + W(3, 0, 0));
-                double yp3 = mz_v(0, 1, 0) * 0.5 * (q0 + W(0, 3, 0));
-                double xm3 = mz_u(-2, 0, 0) * 0.5 * (q0 + W(-3, 0, 0));
-                double ym3 = mz_v(0, -2, 0) * 0.5 * (q0 + W(0, -3, 0));
-                fw = -((A1 * (xph - xmh) + A2 * (xp3 - xm3)) + (A1 * (yph - ymh) + A2 * (yp3 - ym3))
+                // z interpolation of the u / v mass fluxes to the w face: the
+                // metric differs per plane, folded into four row constants
+                const double cu0 = B1h * dydz[k], cu1 = B1h * dydz[k + 1], cum = B2h * dydz[k - 1], cu2 = B2h * dydz[k + 2];
+                const double cv0 = B1h * dxdz[k], cv1 = B1h * dxdz[k + 1], cvm = B2h * dxdz[k - 1], cv2 = B2h * dxdz[k + 2];
+                auto mu = [&](int di, int dj) {
+                    return (cu0 * U(di, dj, 0) + cu1 * U(di, dj, 1)) + (cum * U(di, dj, -1) + cu2 * U(di, dj, 2));
+                };
+                auto mv = [&](int di, int dj) {
+                    return (cv0 * V(di, dj, 0) + cv1 * V(di, dj, 1)) + (cvm * V(di, dj, -1) + cv2 * V(di, dj, 2));
+                };
+                const double q0 = W(0, 0, 0);
+                fw = -((xflux(W, mu, q0) + yflux(W, mv, q0))
                        + (A1 * (zq_w.f1 - zq_w.f1m) + A2 * (zq_w.f3 - zq_w.f3m[0]))) * G.ivolw[k];
             }
-            // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363)
+            // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363):
+            // A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) of the staggered first
+            // differences is the 7-point stencil L1, L2, L3 on differences
+            // from the centre value (mathematically the same; rounds differently)
             auto lap4 = [&](auto F, double nu) {
-                double q0 = F(0, 0, 0);
-                double up3h = A1 * (F(2, 0, 0) - F(1, 0, 0)) + A2 * (F(3, 0, 0) - q0);
-                double up1h = A1 * (F(1, 0, 0) - q0) + A2 * (F(2, 0, 0) - F(-1, 0, 0));
-                double um1h = A1 * (q0 - F(-1, 0, 0)) + A2 * (F(1, 0, 0) - F(-2, 0, 0));
-                double um3h = A1 * (F(-1, 0, 0) - F(-2, 0, 0)) + A2 * (q0 - F(-3, 0, 0));
-                double vp3h = A1 * (F(0, 2, 0) - F(0, 1, 0)) + A2 * (F(0, 3, 0) - q0);
-                double vp1h = A1 * (F(0, 1, 0) - q0) + A2 * (F(0, 2, 0) - F(0, -1, 0));
-                double vm1h = A1 * (q0 - F(0, -1, 0)) + A2 * (F(0, 1, 0) - F(0, -2, 0));
-                double vm3h = A1 * (F(0, -1, 0) - F(0, -2, 0)) + A2 * (q0 - F(0, -3, 0));
-                return nu * ((A1 * (up1h * idx - um1h * idx) + A2 * (up3h * idx - um3h * idx)) * idx
-                             + (A1 * (vp1h * idy - vm1h * idy) + A2 * (vp3h * idy - vm3h * idy)) * idy);
+                const double q0 = F(0, 0, 0);
+                const double lx = L3 * ((F(3, 0, 0) - q0) + (F(-3, 0, 0) - q0)) + L2 * ((F(2, 0, 0) - q0) + (F(-2, 0, 0) - q0))
+                                + L1 * ((F(1, 0, 0) - q0) + (F(-1, 0, 0) - q0));
+                const double ly = L3 * ((F(0, 3, 0) - q0) + (F(0, -3, 0) - q0)) + L2 * ((F(0, 2, 0) - q0) + (F(0, -2, 0) - q0))
+                                + L1 * ((F(0, 1, 0) - q0) + (F(0, -1, 0) - q0));
+                return nu * (lx * idx2 + ly * idy2);
             };
             fu += lap4(U, A.nu);
             fv += lap4(V, A.nu);
