@@ -57,7 +57,7 @@ WORKLOAD = WORKLOADS["config2"]
 B_ALG = 240.0            # algorithmic HBM bytes per point-substep (whole substep)
 METRIC = "FP64 Mpt-substeps/s"
 # Minimal bytes per interior point of each kernel group (own inputs + outputs)
-KERNEL_BYTES = {"rhs": 64.0, "solve_u": 32.0, "solve_v": 32.0, "solve_c": 32.0, "solve_w": 32.0,
+KERNEL_BYTES = {"rhs": 64.0, "solve": 128.0,
                 "div_fftx": 32.0, "ffty_fwd": 16.0, "poisson": 16.0, "ffty_bwd": 16.0,
                 "fftx_c2r": 16.0, "project": 72.0}
 # CPU-baseline sample: same order / nz / dt / viscosity, fewer x-y points per process
@@ -258,7 +258,7 @@ def run_ours(args):
             traffic = json.load(f).get("dram_bytes_per_substep_full_size")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "whole RK3 substep (CUDA graph of 16 launches)",
+                "kernel": f"whole RK3 substep (CUDA graph of {inst.launches_per_substep()} launches)",
                 "alg_bytes_per_unit": B_ALG, "unit_desc": "interior point-substep",
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "kernels": kernels, "profiled_substep_ms": round(sub_ms, 4)}

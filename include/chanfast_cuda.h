@@ -141,11 +141,12 @@ int cf_device_field(cf_instance *inst, int field, double **dev_ptr, long long *n
 /* Run nsub substeps with CUDA events between the kernel groups on the
  * instance stream and return the summed device time of each group (ms) in
  * ms[CF_NKERNEL_GROUPS], in this order:
- *   0 ghosts (apply_bc), 1 rhs, 2 solve u, 3 mass-flux control u, 4 solve v,
- *   5 solve c, 6 scalar-mean control c, 7 solve w, 8 divergence + x FFT,
- *   9 y FFT, 10 Poisson, 11 inverse y FFT, 12 inverse x FFT, 13 projection.
+ *   0 ghosts (apply_bc), 1 rhs, 2 implicit solves of u, v, c and w (one
+ *   launch), 3 mass-flux control u, 4 scalar-mean control c, 5 divergence +
+ *   x FFT, 6 y FFT, 7 Poisson, 8 inverse y FFT, 9 inverse x FFT,
+ *   10 projection.
  * Synchronises after every substep (timing only). */
-#define CF_NKERNEL_GROUPS 14
+#define CF_NKERNEL_GROUPS 11
 int cf_profile(cf_instance *inst, int nsub, double *ms);
 
 /* Number of kernel launches the engine issues per substep. */

@@ -26,8 +26,8 @@ FIELDS = {"u": 0, "v": 1, "w": 2, "c": 3, "p": 4}
 LAYOUT_PADDED, LAYOUT_INTERIOR = 0, 1
 LOG_COLS = 10
 NOALLOC_MAX_ROWS = 8191   # scratch rows of cf_max_divergence_noalloc
-KERNEL_GROUPS = ("ghosts", "rhs", "solve_u", "mass_u", "solve_v", "solve_c", "mass_c", "solve_w",
-                 "div_fftx", "ffty_fwd", "poisson", "ffty_bwd", "fftx_c2r", "project")
+KERNEL_GROUPS = ("ghosts", "rhs", "solve", "mass_u", "mass_c", "div_fftx", "ffty_fwd", "poisson", "ffty_bwd",
+                 "fftx_c2r", "project")
 NKERNEL_GROUPS = len(KERNEL_GROUPS)
 
 _lib = None

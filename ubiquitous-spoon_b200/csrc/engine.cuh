@@ -161,7 +161,10 @@ void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st);
 constexpr int SOLVE_THREADS = 128;   // k_solve block: one thread per column
 constexpr int SOLVE_PF = 6;          // forward-sweep rows in flight per thread
 inline size_t solve_smem_bytes() { return (size_t) SOLVE_PF * 3 * SOLVE_THREADS * sizeof(double); }
-void launch_solve(const Geo& G, const SolveArgs& A, bool is_w, bool shift, cudaStream_t st);
+struct SolveBatch {
+    SolveArgs a[4];   // u, v, c, w
+};
+void launch_solve4(const Geo& G, const SolveBatch& B, cudaStream_t st);
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st);
 void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st);
 void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st);

@@ -243,13 +243,6 @@ __global__ void k_max_rows_final(const double* rowmax, int n, double* result)
     if (threadIdx.x == 0) *result = red[0];
 }
 
-__global__ void k_zero(double* p, long long n)
-{
-    for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (long long) gridDim.x * blockDim.x)
-        p[t] = 0.0;
-}
-
 // ------------------------------------------------------------ host helpers
 
 // Packs host vectors into one device allocation.
@@ -310,7 +303,8 @@ struct cf_instance {
     double* gbuf[4] = {nullptr, nullptr, nullptr, nullptr};
     double2* spec = nullptr;
     double* scratch = nullptr;
-    double* partial = nullptr;
+    double* partial = nullptr;     // per-warp row sums of the u solve
+    double* partial_c = nullptr;   // and of the c solve
     double* avg = nullptr;
     double* dscal = nullptr;        // [0] mdpdx, [1] dcdt
     long long* dcount = nullptr;    // device substep counter (log row)
@@ -561,13 +555,16 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     const int fidx[4] = {0, 1, 3, 2};   // u, v, c, w -> f/g slots (u, v, w, c)
     double bcb[4] = {0.0 - C.setuframe, 0.0 - C.setvframe, -0.5, 0.0};
     double bct[4] = {0.0 - C.setuframe, 0.0 - C.setvframe, +0.5, 0.0};
+    double* partial[4] = {I->partial, nullptr, I->partial_c, nullptr};
+    SolveBatch SB;
     for (int q = 0; q < 4; q++) {
         const SetOffsets& so = I->set[s][q];
-        const bool is_w = q == 3, stats = q == 0 || q == 2;
-        SolveArgs S;
+        const bool is_w = q == 3;
+        SolveArgs& S = SB.a[q];
         S.x = fields[q];
         S.f = I->fbuf[fidx[q]];
         S.g = I->gbuf[fidx[q]];
+        // u and c: f += mdpdx / dcdt of the previous substep's control step
         S.gshift = q == 0 ? I->dscal : (q == 2 ? I->dscal + 1 : nullptr);
         S.fac = factor_of(I, so);
         S.rows = I->coef + so.rows;
@@ -575,10 +572,13 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
         S.bc_top = bct[q];
         S.bcb = is_w ? I->bc_wb : I->bc_ub;
         S.bct = is_w ? I->bc_wt : I->bc_ut;
-        S.partial = stats ? I->partial : nullptr;
-        launch_solve(G, S, is_w, S.gshift != nullptr, st);
-        if (tl) tl->mark(st);
-        if (stats) {
+        S.partial = partial[q];
+    }
+    launch_solve4(G, SB, st);
+    if (tl) tl->mark(st);
+    for (int q = 0; q < 4; q += 2) {   // mass-flux control (u), scalar-mean control (c)
+        const SetOffsets& so = I->set[s][q];
+        {
             MassArgs M;
             M.avg = I->avg;
             M.dz = G.dz;
@@ -596,7 +596,7 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
             M.log_cap = I->log_cap;
             M.col = q == 0 ? 0 : 5;
             M.advance = q == 2 ? 1 : 0;
-            launch_mass(G, I->partial, I->avg, M, st);
+            launch_mass(G, partial[q], I->avg, M, st);
             if (tl) tl->mark(st);
         }
     }
@@ -634,7 +634,7 @@ int cf_destroy(cf_instance* I)
     if (I->gexec) cudaGraphExecDestroy(I->gexec);
     if (I->graph) cudaGraphDestroy(I->graph);
     void* bufs[] = {I->u, I->v, I->w, I->c, I->p, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
-                    I->gbuf[0], I->gbuf[1], I->gbuf[2], I->gbuf[3], I->spec, I->scratch, I->partial,
+                    I->gbuf[0], I->gbuf[1], I->gbuf[2], I->gbuf[3], I->spec, I->scratch, I->partial, I->partial_c,
                     I->avg, I->dscal, I->dcount, I->dlog, I->staging, I->coef, I->twx, I->twy};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -683,6 +683,7 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
     const long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);   // per-warp partial sums of k_solve
     CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
+    CF_CUDA(cudaMalloc(&I->partial_c, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->avg, (size_t) G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->dscal, 8 * sizeof(double)));
     CF_CUDA(cudaMemsetAsync(I->dscal, 0, 8 * sizeof(double), I->stream));
@@ -1016,9 +1017,9 @@ int cf_profile(cf_instance* I, int nsub, double* ms)
 
 int cf_launches_per_substep(const cf_instance* I)
 {
-    // ghosts, rhs, 4 solves, 2 x (row average + mass control), div+fftx,
-    // ffty, poisson, ffty, fftx_c2r, project
-    return I ? 16 : CF_EINVAL;
+    // ghosts, rhs, the four solves, 2 x (row average + mass control),
+    // div+fftx, ffty, poisson, ffty, fftx_c2r, project
+    return I ? 13 : CF_EINVAL;
 }
 
 }  // extern "C"

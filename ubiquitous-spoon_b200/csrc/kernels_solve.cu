@@ -93,8 +93,9 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// One column of one field; every thread of the block calls it.
 template <int ORDER, bool IS_W, bool SHIFT>
-__global__ void __launch_bounds__(SOLVE_THREADS, 10) k_solve(Geo G, SolveArgs A)
+__device__ __forceinline__ void solve_column(const Geo& G, const SolveArgs& A)
 {
     const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = col < G.plane;
@@ -310,20 +311,27 @@ __global__ void k_mass_control(MassArgs A)
     }
 }
 
-void launch_solve(const Geo& G, const SolveArgs& A, bool is_w, bool shift, cudaStream_t st)
+// The four implicit solves of a substep in one launch (they are independent:
+// the mass-flux corrections of u and c are applied lazily, and the control
+// kernels that read the u and c row sums run after it).  blockIdx.y selects
+// the field: 0 u, 1 v, 2 c (u and c carry the shift of the previous control
+// step), 3 w.
+template <int ORDER>
+__global__ void __launch_bounds__(SOLVE_THREADS, 9) k_solve4(Geo G, SolveBatch B)
 {
-    unsigned nb = (unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS);
-#define CF_SOLVE(O, W, S) k_solve<O, W, S><<<nb, SOLVE_THREADS, solve_smem_bytes(), st>>>(G, A)
-    if (G.order == 2) {
-        if (is_w) CF_SOLVE(2, true, false);
-        else if (shift) CF_SOLVE(2, false, true);
-        else CF_SOLVE(2, false, false);
-    } else {
-        if (is_w) CF_SOLVE(4, true, false);
-        else if (shift) CF_SOLVE(4, false, true);
-        else CF_SOLVE(4, false, false);
+    switch (blockIdx.y) {
+    case 0: solve_column<ORDER, false, true>(G, B.a[0]); break;
+    case 1: solve_column<ORDER, false, false>(G, B.a[1]); break;
+    case 2: solve_column<ORDER, false, true>(G, B.a[2]); break;
+    default: solve_column<ORDER, true, false>(G, B.a[3]); break;
     }
-#undef CF_SOLVE
+}
+
+void launch_solve4(const Geo& G, const SolveBatch& B, cudaStream_t st)
+{
+    dim3 grd((unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS), 4);
+    if (G.order == 2) k_solve4<2><<<grd, SOLVE_THREADS, solve_smem_bytes(), st>>>(G, B);
+    else k_solve4<4><<<grd, SOLVE_THREADS, solve_smem_bytes(), st>>>(G, B);
 }
 
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st)
