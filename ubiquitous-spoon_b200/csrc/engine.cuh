@@ -113,6 +113,7 @@ struct DivArgs {
     double2* spec;         // [n2][nkx][ny]
     FftPlan px;
     double c8;
+    double* dv;            // real divergence field [n2][nx][ny] (power-of-two nx path)
 };
 
 struct FftyArgs {

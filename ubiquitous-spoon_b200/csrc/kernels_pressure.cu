@@ -578,10 +578,11 @@ __device__ __forceinline__ void bfly(double2* w, int s, double c8)
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
 // In-place transform of one line; every thread of the block must call it
-// (it synchronises the block).  sl: this line's padded shared buffer.
+// (it synchronises the block).  sl: this line's padded shared buffer; tw:
+// exp(-2 pi i m / (tws N)), read with stride tws.
 template <int N>
 __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* __restrict__ tw, int sign,
-                            double c8)
+                            double c8, int tws = 1)
 {
     constexpr int T = N / 8;
     constexpr int LOG = ilog2c(N);
@@ -611,7 +612,7 @@ __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* 
 #pragma unroll
         for (int r = 1; r < 8; r++) {
             if (k) {
-                double2 c = __ldg(&tw[r * k * step]);
+                double2 c = __ldg(&tw[tws * r * k * step]);
                 if (sign > 0) c.y = -c.y;
                 w[r] = cmul(w[r], c);
             }
@@ -661,30 +662,68 @@ __device__ __forceinline__ double div_point(const Geo& G, const DivArgs& A, int 
          + (A1 * (Wr(k) - Wr(k - 1)) + A2 * (wkp1 - wkm2)) * idzk;
 }
 
-template <int ORDER, int N>
-__global__ void __launch_bounds__(256) k_div_fftx_p2(Geo G, DivArgs A)
+// Divergence of the power-of-two path as its own streaming kernel (one
+// thread per point, rows of 32 consecutive j); the x transform then reads
+// it as a real field.
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_div(Geo G, DivArgs A)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = GZ + blockIdx.z;
+    if (j >= G.ny || i >= G.nx) return;
+    const bool corr = A.mu != nullptr;
+    const double uc = corr ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
+    A.dv[((long long) k * G.nx + i) * G.ny + j] = div_point<ORDER>(G, A, k, i, j, uc, corr);
+}
+
+// Real-to-complex x transform (fftx_d2c, pressure.c:122-160, scaled by 1/N)
+// as a complex transform of half length: z[m] = x[2m] + i x[2m+1], Z = FFT(z),
+// X[k] = E[k] + exp(-2 pi i k/N) O[k] with E, O the transforms of the even and
+// odd samples, E = (Z[k] + conj Z[M-k]) / 2, O = (Z[k] - conj Z[M-k]) / 2i.
+// A line is M = N/2 points, 8 per thread; 256 / (M/8) lines of consecutive j
+// per block.
+template <int N>
+__global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, DivArgs A)
 {
     extern __shared__ double2 sbuf[];
-    constexpr int T = N / 8, L = p2_lines(N);
+    constexpr int M = N / 2, T = M / 8, L = p2_lines(M);
     const int l = threadIdx.x % L, t = threadIdx.x / L;
     const int k = GZ + blockIdx.y;
     const int j = blockIdx.x * L + l;
     const bool valid = j < G.ny;
-    const bool corr = A.mu != nullptr;
-    const double uc = corr ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
+    const int ny = G.ny;
+    const double* row = A.dv + (long long) k * G.nx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
-    for (int q = 0; q < 8; q++)
-        v[q] = make_double2(valid ? div_point<ORDER>(G, A, k, t + q * T, j, uc, corr) : 0.0, 0.0);
-    fft_p2_line<N>(v, t, sbuf + l * p2_stride_x(N), A.px.tw, -1, A.c8);
-    const double scale = 1.0 / (double) N;
+    for (int q = 0; q < 8; q++) {
+        const int m = t + q * T;
+        v[q] = make_double2(__ldg(row + (long long) (2 * m) * ny), __ldg(row + (long long) (2 * m + 1) * ny));
+    }
+    double2* sl = sbuf + l * p2_stride_x(M);
+    fft_p2_line<M>(v, t, sl, A.px.tw, -1, A.c8, 2);
+    // Z in natural order through this line's buffer (the transform's last
+    // reads of it are behind its final barrier)
+#pragma unroll
+    for (int r = 0; r < 8; r++) sl[pad8(t + r * T)] = v[r];
+    __syncthreads();
     if (!valid) return;
-    const int nkx = G.nkx;
+    const double scale = 1.0 / (double) N;
+    double2* out = A.spec + (long long) k * G.nkx * ny + j;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-        int kx = t + q * T;
-        if (kx < nkx)
-            A.spec[((long long) k * nkx + kx) * G.ny + j] = make_double2(v[q].x * scale, v[q].y * scale);
+        const int kx = t + q * T;
+        const double2 a = sl[pad8(kx)];
+        const double2 zb = sl[pad8((M - kx) & (M - 1))];
+        const double er = 0.5 * (a.x + zb.x), ei = 0.5 * (a.y - zb.y);   // E
+        const double orr = 0.5 * (a.y + zb.y), oi = -0.5 * (a.x - zb.x); // O
+        const double2 w = __ldg(&A.px.tw[kx]);                            // exp(-2 pi i kx/N)
+        out[(long long) kx * ny] = make_double2((er + (w.x * orr - w.y * oi)) * scale,
+                                                (ei + (w.x * oi + w.y * orr)) * scale);
+    }
+    if (t == 0) {   // Nyquist: X[N/2] = E[0] - O[0], real
+        const double2 z0 = sl[pad8(0)];
+        out[(long long) M * ny] = make_double2((z0.x - z0.y) * scale, 0.0);
     }
 }
 
@@ -713,33 +752,44 @@ __global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
     }
 }
 
+// Complex-to-real x transform (fftx_c2d, pressure.c:163-200) as an inverse
+// complex transform of half length: with X[0] and X[N/2] taken real (as
+// FFTW's c2r does), Z[k] = (X[k] + conj X[M-k]) + i exp(2 pi i k/N)
+// (X[k] - conj X[M-k]) for k < M, z = IFFT(Z) unnormalised, and
+// x[2m] = Re z[m], x[2m+1] = Im z[m].
 template <int N>
 __global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
 {
     extern __shared__ double2 sbuf[];
-    constexpr int T = N / 8, L = p2_lines(N);
+    constexpr int M = N / 2, T = M / 8, L = p2_lines(M);
     const int l = threadIdx.x % L, t = threadIdx.x / L;
     const int k = blockIdx.y;
     const int j = blockIdx.x * L + l;
     const bool valid = j < G.ny;
-    const int nkx = G.nkx, ny = G.ny;
-    // Hermitian completion: position p > N/2 holds conj(spec[N - p]); all
-    // eight loads are issued unconditionally (a row of this plane) so they
-    // are in flight together
-    const double2* base = A.spec + (long long) k * nkx * ny + (valid ? j : 0);
+    const int ny = G.ny;
+    const double2* base = A.spec + (long long) k * G.nkx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-        const int p = t + q * T;
-        const bool lo = p < nkx;
-        v[q] = __ldg(base + (long long) (lo ? p : N - p) * ny);
-        if (!lo) v[q].y = -v[q].y;
-        if (p == 0 || 2 * p == N) v[q].y = 0.0;   // c2r ignores these imaginary parts
+        const int kx = t + q * T;
+        double2 a = __ldg(base + (long long) kx * ny);
+        double2 b = __ldg(base + (long long) (M - kx) * ny);
+        if (kx == 0) { a.y = 0.0; b.y = 0.0; }   // imaginary parts of X[0], X[N/2] ignored
+        const double sr = a.x + b.x, si = a.y - b.y;   // X[k] + conj X[M-k]
+        const double dr = a.x - b.x, di = a.y + b.y;   // X[k] - conj X[M-k]
+        const double2 w = __ldg(&A.px.tw[kx]);          // conj of exp(2 pi i kx/N)
+        const double tr = w.x * dr + w.y * di, ti = w.x * di - w.y * dr;
+        v[q] = make_double2(sr - ti, si + tr);
     }
-    fft_p2_line<N>(v, t, sbuf + l * p2_stride_x(N), A.px.tw, +1, A.c8);
+    fft_p2_line<M>(v, t, sbuf + l * p2_stride_x(M), A.px.tw, +1, A.c8, 2);
     if (!valid) return;
+    double* out = A.p + (long long) k * G.nx * ny + j;
 #pragma unroll
-    for (int q = 0; q < 8; q++) A.p[((long long) k * G.nx + (t + q * T)) * ny + j] = v[q].x;
+    for (int q = 0; q < 8; q++) {
+        const int m = t + q * T;
+        out[(long long) (2 * m) * ny] = v[q].x;
+        out[(long long) (2 * m + 1) * ny] = v[q].y;
+    }
 }
 
 template <int N>
@@ -750,10 +800,11 @@ static size_t p2_smem_y() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(dou
 template <int N>
 static void launch_div_fftx_p2(const Geo& G, const DivArgs& A, cudaStream_t st)
 {
-    constexpr int L = p2_lines(N);
-    dim3 grd((G.ny + L - 1) / L, G.nz);
-    if (G.order == 2) k_div_fftx_p2<2, N><<<grd, 256, p2_smem_x<N>(), st>>>(G, A);
-    else k_div_fftx_p2<4, N><<<grd, 256, p2_smem_x<N>(), st>>>(G, A);
+    dim3 blk(32, 4, 1), grd((G.ny + 31) / 32, (G.nx + 3) / 4, G.nz);
+    if (G.order == 2) k_div<2><<<grd, blk, 0, st>>>(G, A);
+    else k_div<4><<<grd, blk, 0, st>>>(G, A);
+    constexpr int L = p2_lines(N / 2);
+    k_fftx_r2c_p2<N><<<dim3((G.ny + L - 1) / L, G.nz), 256, p2_smem_x<N / 2>(), st>>>(G, A);
 }
 
 template <int N>
@@ -767,17 +818,16 @@ static void launch_ffty_p2(const Geo& G, const FftyArgs& A, int nrows, cudaStrea
 template <int N>
 static void launch_c2r_p2(const Geo& G, const C2rArgs& A, cudaStream_t st)
 {
-    constexpr int L = p2_lines(N);
+    constexpr int L = p2_lines(N / 2);
     dim3 grd((G.ny + L - 1) / L, G.n2);
-    k_fftx_c2r_p2<N><<<grd, 256, p2_smem_x<N>(), st>>>(G, A);
+    k_fftx_c2r_p2<N><<<grd, 256, p2_smem_x<N / 2>(), st>>>(G, A);
 }
 
 template <int N>
 static cudaError_t p2_set_smem()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_div_fftx_p2<2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N>());
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx_p2<4, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N>());
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N>());
+    cudaError_t e = cudaFuncSetAttribute(k_fftx_r2c_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N / 2>());
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N / 2>());
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_y<N>());
     return e;
 }
