@@ -56,8 +56,10 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS["config2"]
 B_ALG = 240.0            # algorithmic HBM bytes per point-substep (whole substep)
 METRIC = "FP64 Mpt-substeps/s"
-# Minimal bytes per interior point of each kernel group (own inputs + outputs)
-KERNEL_BYTES = {"rhs": 64.0, "solve": 128.0,
+# Minimal bytes per interior point of each kernel group (own inputs + outputs):
+# rhs = RHS + forward sweeps (read u,v,w,c,g x4; write f x4, s x4), solve = back
+# substitution (read s x4, write x x4)
+KERNEL_BYTES = {"rhs": 128.0, "solve": 64.0,
                 "div_fftx": 32.0, "ffty_fwd": 16.0, "poisson": 16.0, "ffty_bwd": 16.0,
                 "fftx_c2r": 16.0, "project": 72.0}
 # CPU-baseline sample: same order / nz / dt / viscosity, fewer x-y points per process

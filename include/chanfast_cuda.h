@@ -141,10 +141,10 @@ int cf_device_field(cf_instance *inst, int field, double **dev_ptr, long long *n
 /* Run nsub substeps with CUDA events between the kernel groups on the
  * instance stream and return the summed device time of each group (ms) in
  * ms[CF_NKERNEL_GROUPS], in this order:
- *   0 ghosts (apply_bc), 1 rhs, 2 implicit solves of u, v, c and w (one
- *   launch), 3 mass-flux control u, 4 scalar-mean control c, 5 divergence +
- *   x FFT, 6 y FFT, 7 Poisson, 8 inverse y FFT, 9 inverse x FFT,
- *   10 projection.
+ *   0 ghosts (apply_bc), 1 rhs with the forward sweeps of the implicit
+ *   solves, 2 back substitution of u, v, c and w (one launch), 3 mass-flux
+ *   control u, 4 scalar-mean control c, 5 divergence + x FFT, 6 y FFT,
+ *   7 Poisson, 8 inverse y FFT, 9 inverse x FFT, 10 projection.
  * Synchronises after every substep (timing only). */
 #define CF_NKERNEL_GROUPS 11
 int cf_profile(cf_instance *inst, int nsub, double *ms);

@@ -53,14 +53,11 @@ struct FactorD {
     const double *F1, *F2, *F3, *DEN, *P, *Q, *R;
 };
 
-// Arguments of one implicit solve launch.
+// Back substitution of one implicit solve (its forward sweep runs in k_rhs).
 struct SolveArgs {
-    double* x;            // field (in: old value, out: new value)
-    const double* f;      // current RHS
-    const double* g;      // previous-stage RHS
-    const double* gshift; // device scalar added to g (mass-flux lazily applied), or null
+    double* x;            // field: out, the new value (all n2 rows)
+    const double* s;      // forward-substituted vector, rows k0 .. k0+n-1
     FactorD fac;          // back-substitution multipliers P, Q, R; rows k0 .. k0+n-1
-    const double* rows;   // fused forward rows [n][fused_width] (host_band.h)
     double bc_bot, bc_top;
     WallRowsD bcb, bct;   // apply_bc closure rows for this field
     double* partial;      // per-warp row sums [nwarps][n2] or null
@@ -82,11 +79,22 @@ struct GhostArgs {
     double bc_u, bc_v, bc_c_bot, bc_c_top, bc_w;
 };
 
+// Forward sweep of one implicit solve, fused into k_rhs (see host_band.h
+// fused_rows): s_i = sum cu_m x_{k+m} + cf f_k + cg g_k + c0 - f1 s_{i-1} - ...
+struct FwdSweep {
+    double* g;             // in: previous-stage RHS g; out: the forward-substituted s (same rows)
+    const double* gshift;  // device scalar added to g (mass-flux lazily applied), or null
+    const double* rows;    // fused forward rows [n][fused_width]
+};
+
 struct RhsArgs {
     const double *u, *v, *w, *c;
     double *fu, *fv, *fw, *fc;
     double nu, kappa;              // nu and nu/prandtl
     double betg_x, betg_y, betg_z;
+    FwdSweep sw[4];                // u, v, w, c
+    WallRowsD wbot, wtop;          // apply_bc_w closure rows (ghost values of the old w)
+    double wbc_bot, wbc_top;
 };
 
 struct MassArgs {
@@ -159,13 +167,11 @@ struct ProjArgs {
 // ---------------------------------------------------------------- launchers
 void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st);
 void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st);
-constexpr int SOLVE_THREADS = 128;   // k_solve block: one thread per column
-constexpr int SOLVE_PF = 6;          // forward-sweep rows in flight per thread
-inline size_t solve_smem_bytes() { return (size_t) SOLVE_PF * 3 * SOLVE_THREADS * sizeof(double); }
+constexpr int SOLVE_THREADS = 128;   // k_back4 block: one thread per column
 struct SolveBatch {
     SolveArgs a[4];   // u, v, c, w
 };
-void launch_solve4(const Geo& G, const SolveBatch& B, cudaStream_t st);
+void launch_back4(const Geo& G, const SolveBatch& B, cudaStream_t st);
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st);
 void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st);
 void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st);

@@ -548,8 +548,21 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     launch_ghosts(G, GA, st);
     if (tl) tl->mark(st);
 
+    // RHS + forward sweeps; set index of each f slot (u, v, w, c) among the
+    // implicit-solve sets (u, v, c, w)
     RhsArgs R{I->u, I->v, I->w, I->c, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
               C.nu, C.nu / C.prandtl, C.betg_x, C.betg_y, C.betg_z};
+    const int set_of_slot[4] = {0, 1, 3, 2};
+    for (int f = 0; f < 4; f++) {
+        R.sw[f].g = I->gbuf[f];
+        // u and c: f += mdpdx / dcdt of the previous substep's control step
+        R.sw[f].gshift = f == 0 ? I->dscal : (f == 3 ? I->dscal + 1 : nullptr);
+        R.sw[f].rows = I->coef + I->set[s][set_of_slot[f]].rows;
+    }
+    R.wbot = I->bc_wb;
+    R.wtop = I->bc_wt;
+    R.wbc_bot = 0.0;
+    R.wbc_top = 0.0;
     launch_rhs(G, R, st);
     if (tl) tl->mark(st);
 
@@ -564,19 +577,15 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
         const bool is_w = q == 3;
         SolveArgs& S = SB.a[q];
         S.x = fields[q];
-        S.f = I->fbuf[fidx[q]];
-        S.g = I->gbuf[fidx[q]];
-        // u and c: f += mdpdx / dcdt of the previous substep's control step
-        S.gshift = q == 0 ? I->dscal : (q == 2 ? I->dscal + 1 : nullptr);
+        S.s = I->gbuf[fidx[q]];   // the forward sweep in k_rhs left s there
         S.fac = factor_of(I, so);
-        S.rows = I->coef + so.rows;
         S.bc_bot = bcb[q];
         S.bc_top = bct[q];
         S.bcb = is_w ? I->bc_wb : I->bc_ub;
         S.bct = is_w ? I->bc_wt : I->bc_ut;
         S.partial = partial[q];
     }
-    launch_solve4(G, SB, st);
+    launch_back4(G, SB, st);
     if (tl) tl->mark(st);
     for (int q = 0; q < 4; q += 2) {   // mass-flux control (u), scalar-mean control (c)
         const SetOffsets& so = I->set[s][q];
@@ -683,7 +692,7 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     CF_CUDA(cudaMemsetAsync(I->spec, 0, (size_t) G.splane * G.n2 * sizeof(double2), I->stream));
     const int nscr = C.order == 4 ? 3 : 1;
     CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
-    const long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);   // per-warp partial sums of k_solve
+    const long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);   // per-warp partial sums of k_back4
     CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->partial_c, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->avg, (size_t) G.n2 * sizeof(double)));
@@ -1019,7 +1028,7 @@ int cf_profile(cf_instance* I, int nsub, double* ms)
 
 int cf_launches_per_substep(const cf_instance* I)
 {
-    // ghosts, rhs, the four solves, 2 x (row average + mass control),
+    // ghosts, rhs + forward sweeps, the four back substitutions, 2 x (row average + mass control),
     // div+fftx (two launches for power-of-two nx), ffty, poisson, ffty,
     // fftx_c2r, project
     if (!I) return CF_EINVAL;

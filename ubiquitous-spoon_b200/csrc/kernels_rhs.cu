@@ -128,19 +128,24 @@ __global__ void k_ghosts(Geo G, GhostArgs A)
 
 // --------------------------------------------------------------------- RHS
 //
-// One block owns an 8 (x) by 32 (y) column tile and marches up a chunk of
-// interior rows.  The 7 k-planes a row needs (k-3..k+3) of u, v, w, c, with a
-// 3-cell periodic halo in x and y, sit in a ring of 8 shared-memory slots;
-// the next plane streams in with cp.async while the current row is computed.
-// Every stencil value is read from shared memory.  Divisions by the grid
-// metrics are multiplications by their reciprocals (host tables), so results
-// agree with the reference to rounding, not bit for bit.
+// One block owns an 8 (x) by 32 (y) column tile and marches up all interior
+// rows.  The 7 k-planes a row needs (k-3..k+3) of u, v, w, c, with a 3-cell
+// periodic halo in x and y, sit in a ring of 8 shared-memory slots; the next
+// plane streams in with cp.async while the current row is computed.  Every
+// stencil value is read from shared memory.  Divisions by the grid metrics
+// are multiplications by their reciprocals (host tables), so results agree
+// with the reference to rounding, not bit for bit.
+//
+// After a row's four right-hand sides the same thread runs that row of the
+// forward sweeps of the four implicit solves (chanfast.c:459-482 with the
+// forward half of tridag/heptdag): the old field window x_{k-H..k+H} is in
+// the ring, f was just computed, g is read and overwritten by s.  The back
+// substitution follows in k_back4 (kernels_solve.cu).
 
 constexpr int RT_I = 8, RT_J = 32, RT_H = 3, RT_SLOTS = 8;
 constexpr int RT_PI = RT_I + 2 * RT_H, RT_PJ = RT_J + 2 * RT_H;   // 14 x 38
 constexpr int RT_PLANE = RT_PI * RT_PJ;
 constexpr int RT_THREADS = RT_I * RT_J;
-constexpr int RT_KC = 64;   // interior rows per block
 constexpr double B1h = 0.5 * B1, B2h = 0.5 * B2;   // halved interpolation weights (exact)
 // 7-point form of the fourth-order staggered second difference:
 // A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) = L1 (F1+F-1-2F0) + L2 (F2+F-2-2F0) + L3 (F3+F-3-2F0)
@@ -148,7 +153,13 @@ constexpr double L1 = A1 * A1 - 2.0 * A1 * A2, L2 = 2.0 * A1 * A2, L3 = A2 * A2;
 constexpr int RT_FIELD = RT_SLOTS * RT_PLANE;                      // one field's ring
 constexpr int RT_LOADS = (RT_PLANE + RT_THREADS - 1) / RT_THREADS;  // plane points per thread
 
-size_t rhs_smem_bytes() { return (size_t) 4 * RT_SLOTS * RT_PLANE * sizeof(double); }
+constexpr int RT_FWMAX = 13;   // widest fused forward row (order 4)
+// ring of haloed planes + two rows of each thread's g values + two rows of
+// the four fused coefficient rows
+size_t rhs_smem_bytes()
+{
+    return (size_t) (4 * RT_SLOTS * RT_PLANE + 2 * 4 * RT_THREADS + 2 * 4 * RT_FWMAX) * sizeof(double);
+}
 
 // z fluxes of one advected field (order 4), carried up the column.  With
 // F1(k) = MZ(k) (Q(k) + Q(k+1)) / 2 and F3(k) = MZ(k+1) (Q(k) + Q(k+3)) / 2,
@@ -201,8 +212,7 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     const int j0 = blockIdx.x * RT_J, i0 = blockIdx.y * RT_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
     const long long plane = (long long) nx * ny;
-    const int kb = GZ + blockIdx.z * RT_KC;
-    const int ke = min(kb + RT_KC, GZ + G.nz);
+    const int kb = GZ, ke = GZ + G.nz;   // all interior rows: the forward sweeps run in order
 
     // This thread's points of a haloed plane (same in every plane): their
     // offsets within a field plane, computed once.
@@ -231,6 +241,24 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
         }
         cp_async_commit();
     };
+    // g values (per thread) and fused coefficient rows (per block) of row kk,
+    // staged one row ahead so the sweeps never wait on global memory
+    double* gst = sm + 4 * RT_FIELD;              // [2][4][RT_THREADS]
+    double* cst = gst + 2 * 4 * RT_THREADS;       // [2][4][RT_FWMAX]
+    constexpr int FWR = (ORDER == 2 ? 3 : 7) + 6; // fused row width (host_band.h fused_rows)
+    const long long gij = (i0 + ty < nx && j0 + tx < ny) ? (long long) (i0 + ty) * ny + (j0 + tx) : 0;
+    auto load_extras = [&](int kk) {
+        const long long o = (long long) kk * plane + gij;
+        double* d = gst + (kk & 1) * 4 * RT_THREADS + tid;
+#pragma unroll
+        for (int f = 0; f < 4; f++) cp_async8(d + f * RT_THREADS, A.sw[f].g + o);
+        if (tid < 4 * FWR) {
+            const int f = tid / FWR, e = tid - f * FWR;
+            if (!(f == 2 && kk - GZ >= G.nz - 1))   // the w solve has nz - 1 rows
+                cp_async8(cst + ((kk & 1) * 4 + f) * RT_FWMAX + e, A.sw[f].rows + (kk - GZ) * FWR + e);
+        }
+    };
+    load_extras(kb);
     for (int kk = kb - 3; kk <= kb + 3; kk++) load_plane(kk);
     cp_async_wait_all();
     __syncthreads();
@@ -301,13 +329,40 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     }
     double fzp_prev = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), C(0, 0, 0), C(0, 0, 1));
 
+    // Forward-sweep state: s of rows k-1, k-2, k-3 per field, the lazily
+    // applied shifts of g (u: mdpdx, c: dcdt of the previous control step),
+    // and the ghost values of the old w below / above its wall faces
+    // (apply_bc_w; the ring holds the massflux4 extrapolation there instead).
+    constexpr int H = ORDER == 2 ? 1 : 3;
+    double su1 = 0.0, su2 = 0.0, su3 = 0.0, sv1 = 0.0, sv2 = 0.0, sv3 = 0.0;
+    double sw1 = 0.0, sw2 = 0.0, sw3 = 0.0, sc1 = 0.0, sc2 = 0.0, sc3 = 0.0;
+    const double shift_u = A.sw[0].gshift ? *A.sw[0].gshift : 0.0;
+    const double shift_c = A.sw[3].gshift ? *A.sw[3].gshift : 0.0;
+    double gb0, gb1, gb2, gt0 = 0.0, gt1 = 0.0, gt2 = 0.0;
+    bc_w_bot<ORDER>(A.wbot, A.wbc_bot, W(0, 0, 0), W(0, 0, 1), gb0, gb1, gb2);
+    (void) gb0;
+    auto sweep = [&](int f, auto X, double fk, double gk, double& s1, double& s2, double& s3) {
+        const double* r = cst + ((k & 1) * 4 + f) * RT_FWMAX;   // staged coefficient row
+        double sk = r[2 * H + 3] + r[2 * H + 1] * fk + r[2 * H + 2] * gk;
+#pragma unroll
+        for (int q = 0; q < 2 * H + 1; q++) sk += r[q] * X(q - H);
+        sk -= r[2 * H + 4] * s1;
+        if (ORDER == 4) sk -= r[2 * H + 5] * s2 + r[2 * H + 6] * s3;
+        s3 = s2; s2 = s1; s1 = sk;
+        return sk;
+    };
+
     // One row.  WALL: rows within two of a wall, whose z fluxes use the wall
-    // closures (and the top row has no w point); other rows take a
-    // branch-free path.
+    // closures (and the top row has no w point), and the row whose w-solve
+    // window reaches above the top face; other rows take a branch-free path.
     auto row = [&](auto wall_tag) {
         constexpr bool WALL = decltype(wall_tag)::value;
         const double ivol = G.ivol[k];
         const bool do_w = !WALL || k < n2 - GZ - 1;
+        const long long ijk = (long long) k * plane + gij;
+        const double* gk = gst + (k & 1) * 4 * RT_THREADS + tid;   // g of this row (staged)
+        const double gu = gk[0] + shift_u, gv = gk[RT_THREADS];
+        const double gw = gk[2 * RT_THREADS], gc = gk[3 * RT_THREADS] + shift_c;
         double fu, fv, fw = 0.0, fc;
 
         if (ORDER == 2) {
@@ -465,18 +520,43 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
                 if (do_w) fw += (B1 * (c0 + C(0, 0, 1)) + B2 * (C(0, 0, -1) + C(0, 0, 2))) * A.betg_z;
             }
         }
+
+        // forward sweeps of the implicit solves, rows k0 = GZ .. (u, v, c: nz
+        // rows; w: nz - 1 faces)
+        if (WALL && k >= n2 - GZ - 3)   // old w above the top face (apply_bc_w)
+            bc_w_top<ORDER>(A.wtop, A.wbc_top, W(0, 0, n2 - GZ - 2 - k), W(0, 0, n2 - GZ - 3 - k), gt0, gt1, gt2);
+        auto XW = [&](int dk) -> double {
+            if (WALL) {
+                const int kk = k + dk;
+                if (kk < GZ - 1) return kk == GZ - 2 ? gb1 : gb2;
+                if (kk > n2 - GZ - 1) return kk == n2 - GZ ? gt1 : gt2;
+            }
+            return W(0, 0, dk);
+        };
+        (void) gt0;
+        const double s_u = sweep(0, [&](int dk) { return U(0, 0, dk); }, fu, gu, su1, su2, su3);
+        const double s_v = sweep(1, [&](int dk) { return V(0, 0, dk); }, fv, gv, sv1, sv2, sv3);
+        const double s_w = do_w ? sweep(2, XW, fw, gw, sw1, sw2, sw3) : 0.0;
+        const double s_c = sweep(3, [&](int dk) { return C(0, 0, dk); }, fc, gc, sc1, sc2, sc3);
         if (out) {
-            const long long ijk = (long long) k * plane + (long long) i * ny + j;
             A.fu[ijk] = fu;
             A.fv[ijk] = fv;
-            if (do_w) A.fw[ijk] = fw;
             A.fc[ijk] = fc;
+            A.sw[0].g[ijk] = s_u;
+            A.sw[1].g[ijk] = s_v;
+            A.sw[3].g[ijk] = s_c;
+            if (do_w) {
+                A.fw[ijk] = fw;
+                A.sw[2].g[ijk] = s_w;
+            }
         }
     };
 
     for (; k < ke; k++) {
+        if (k + 1 < ke) load_extras(k + 1);
         if (k + 4 <= ke + 2) load_plane(k + 4);
-        if (k <= GZ + 1 || k >= n2 - GZ - 2) row(std::true_type{});
+        else cp_async_commit();
+        if (k <= GZ + 1 || k >= n2 - GZ - 3) row(std::true_type{});
         else row(std::false_type{});
         cp_async_wait_all();
         __syncthreads();
@@ -496,7 +576,7 @@ void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st)
 void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st)
 {
     dim3 blk(RT_J, RT_I, 1);
-    dim3 grd((G.ny + RT_J - 1) / RT_J, (G.nx + RT_I - 1) / RT_I, (G.nz + RT_KC - 1) / RT_KC);
+    dim3 grd((G.ny + RT_J - 1) / RT_J, (G.nx + RT_I - 1) / RT_I, 1);
     size_t sm = rhs_smem_bytes();
     if (G.order == 2) k_rhs<2><<<grd, blk, sm, st>>>(G, A);
     else k_rhs<4><<<grd, blk, sm, st>>>(G, A);

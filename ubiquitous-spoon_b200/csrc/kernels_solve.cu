@@ -1,6 +1,6 @@
-// Implicit wall-normal diffusion: one thread per column.
+// Implicit wall-normal diffusion, second half: one thread per column.
 //
-// Per column this kernel does what chanfast.c:459-482 does for one field
+// Per column the substep does what chanfast.c:459-482 does for one field
 // (order 2; :1383-1406 order 4):
 //   h  = helmholtz1d_operator(x, nuadt) + gamdt*f + zetdt*g - hbc
 //   x  = solve_helmholtz1d(h, -nubdt)       (tridag.c / heptdag.c)
@@ -8,10 +8,12 @@
 // The band matrix is the same for every column, so its factorisation comes
 // precomputed from host_band.cpp; the Helmholtz operator, the RK3 combination,
 // the cell volume and the pivot reciprocal are folded into one coefficient
-// row per k (fused_rows), so the forward sweep is a short dot product per row
-// and results agree with the reference to rounding.  The forward-substituted
-// vector s is kept in the field's own storage between the two sweeps.  With `partial` set, each warp also writes the sum of its
-// 32 columns for every row (input of get_xy_avg, get.c:281-302).
+// row per k (fused_rows), and the forward sweep runs inside k_rhs
+// (kernels_rhs.cu) right after each row's right-hand side, leaving the
+// forward-substituted vector s in the g buffer.  This file does the back
+// substitution and apply_bc of the four fields in one launch; with `partial`
+// set, each warp also writes the sum of its 32 columns for every row (input
+// of get_xy_avg, get.c:281-302).
 #include "engine.cuh"
 #include "host_band.h"
 
@@ -75,27 +77,15 @@ __device__ __forceinline__ void bcw_top(const WallRowsD& R, double bc, double x0
     }
 }
 
-// Async 8-byte global -> shared copies whose issue is ordered with the
-// thread's other memory accesses ("memory" clobber): the ring slot a copy
-// overwrites was read just before.
-__device__ __forceinline__ void cp_async8_ordered(double* dst, const double* src)
-{
-    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit_ordered() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_ordered() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
 __device__ __forceinline__ double warp_sum(double v)
 {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
 
-// One column of one field; every thread of the block calls it.
-template <int ORDER, bool IS_W, bool SHIFT>
-__device__ __forceinline__ void solve_column(const Geo& G, const SolveArgs& A)
+// Back substitution and apply_bc of one column of one field.
+template <int ORDER, bool IS_W>
+__device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A)
 {
     const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = col < G.plane;
@@ -105,84 +95,15 @@ __device__ __forceinline__ void solve_column(const Geo& G, const SolveArgs& A)
     const int kt = IS_W ? n2 - GZ - 1 : n2 - GZ;    // top wall ghost row / face
     const int n = A.fac.n, k0 = A.fac.k0;
     double* __restrict__ x = A.x;
+    const double* __restrict__ sv = A.s;
     const long long cc = active ? col : 0;
-    auto ld = [&](const double* p, int k) { return p[(long long) k * P + cc]; };
 
-    // Old ghost values: cell fields carry apply_bc values already (k_ghosts);
-    // face fields recompute apply_bc_w here (k_ghosts stored the massflux4
-    // extrapolation there instead).
-    double gb0 = 0.0, gb1 = 0.0, gb2 = 0.0, gt0 = 0.0, gt1 = 0.0, gt2 = 0.0;
-    if (IS_W) {
-        bcw_bot<ORDER>(A.bcb, A.bc_bot, ld(x, kb + 1), ld(x, kb + 2), gb0, gb1, gb2);
-        bcw_top<ORDER>(A.bct, A.bc_top, ld(x, kt - 1), ld(x, kt - 2), gt0, gt1, gt2);
-    }
-    // ghost value d rows beyond the bottom / top wall row
-    auto gbot = [&](int d) { return d == 0 ? gb0 : (d == 1 ? gb1 : gb2); };
-    auto gtop = [&](int d) { return d == 0 ? gt0 : (d == 1 ? gt1 : gt2); };
-    auto old = [&](int k) -> double {
-        if (IS_W) {
-            if (k <= kb) return gbot(kb - k);
-            if (k >= kt) return gtop(k - kt);
-        }
-        return ld(x, k);
-    };
-
-    constexpr int H = ORDER == 2 ? 1 : 3;
-    constexpr int W = 2 * H + 1 + 6;   // fused row width (host_band.h fused_rows)
-    double win[2 * H + 1];  // old x at rows k-H .. k+H
-#pragma unroll
-    for (int q = 0; q < 2 * H + 1; q++) win[q] = old(k0 - H + q);
-
-    // Forward sweep: helmholtz1d_operator + RK3 combination + boundary lifting
-    // + forward elimination of tridag/heptdag, one fused row per k.  The f, g
-    // and next-window values of the coming SOLVE_PF rows are in flight as
-    // cp.async copies into this thread's slots of a shared-memory ring (no
-    // registers held); none of those rows has been overwritten yet (row i
-    // writes only x[k0 + i]).
-    extern __shared__ double ring[];   // [SOLVE_PF][3][SOLVE_THREADS]
-    auto slot = [&](int i, int fld) { return ring + ((i % SOLVE_PF) * 3 + fld) * SOLVE_THREADS + threadIdx.x; };
-    auto fetch = [&](int i) {
-        if (i < n) {
-            const int k = k0 + i;
-            const int kn = min(k + H + 1, n2 - 1);   // window row entering after row i
-            cp_async8_ordered(slot(i, 0), A.f + (long long) k * P + cc);
-            cp_async8_ordered(slot(i, 1), A.g + (long long) k * P + cc);
-            cp_async8_ordered(slot(i, 2), x + (long long) kn * P + cc);
-        }
-        cp_async_commit_ordered();
-    };
-    for (int i = 0; i < SOLVE_PF; i++) fetch(i);
-    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    const double shift = SHIFT ? *A.gshift : 0.0;
-    const double* __restrict__ rows = A.rows;
-    for (int i = 0; i < n; i++) {
-        const int k = k0 + i;
-        const double* r = rows + i * W;
-        cp_async_wait_ordered<SOLVE_PF - 1>();   // row i's copies have landed
-        const double fk = *slot(i, 0);
-        double gk = *slot(i, 1);
-        double xn = *slot(i, 2);
-        fetch(i + SOLVE_PF);
-        if (IS_W && k + H + 1 >= kt) xn = gtop(k + H + 1 - kt);
-        if (SHIFT) gk = gk + shift;   // f += mdpdx of the previous substep (chanfast.c:516-519)
-        double s = __ldg(r + 2 * H + 3) + __ldg(r + 2 * H + 1) * fk + __ldg(r + 2 * H + 2) * gk;
-#pragma unroll
-        for (int q = 0; q < 2 * H + 1; q++) s += __ldg(r + q) * win[q];
-        s -= __ldg(r + 2 * H + 4) * s1;
-        if (ORDER == 4) s -= __ldg(r + 2 * H + 5) * s2 + __ldg(r + 2 * H + 6) * s3;
-        s3 = s2; s2 = s1; s1 = s;
-        if (active) x[(long long) k * P + col] = s;
-#pragma unroll
-        for (int q = 0; q < 2 * H; q++) win[q] = win[q + 1];
-        win[2 * H] = (i + 1 < n) ? xn : 0.0;
-    }
-    cp_async_wait_ordered<0>();
-
-    constexpr int PD = 4;   // back-substitution rows loaded ahead
-    // Back substitution, reading s PD rows ahead (below) the row being written.
+    // x_i = ((s_i - P_i x_{i+1}) - Q_i x_{i+2}) - R_i x_{i+3}, s of row
+    // i - PD loaded into registers while row i is computed.
+    constexpr int PD = 4;
     double ps[PD];
     auto fetch_s = [&](int i, int slot) {
-        if (i >= 0) ps[slot] = ld(x, k0 + i);
+        if (i >= 0) ps[slot] = sv[(long long) (k0 + i) * P + cc];
     };
 #pragma unroll
     for (int u = 0; u < PD; u++) fetch_s(n - 1 - u, u);
@@ -311,27 +232,25 @@ __global__ void k_mass_control(MassArgs A)
     }
 }
 
-// The four implicit solves of a substep in one launch (they are independent:
-// the mass-flux corrections of u and c are applied lazily, and the control
-// kernels that read the u and c row sums run after it).  blockIdx.y selects
-// the field: 0 u, 1 v, 2 c (u and c carry the shift of the previous control
-// step), 3 w.
+// The back substitutions of the four implicit solves in one launch; the
+// control kernels that read the u and c row sums run after it.  blockIdx.y
+// selects the field: 0 u, 1 v, 2 c, 3 w.
 template <int ORDER>
-__global__ void __launch_bounds__(SOLVE_THREADS, 9) k_solve4(Geo G, SolveBatch B)
+__global__ void __launch_bounds__(SOLVE_THREADS) k_back4(Geo G, SolveBatch B)
 {
     switch (blockIdx.y) {
-    case 0: solve_column<ORDER, false, true>(G, B.a[0]); break;
-    case 1: solve_column<ORDER, false, false>(G, B.a[1]); break;
-    case 2: solve_column<ORDER, false, true>(G, B.a[2]); break;
-    default: solve_column<ORDER, true, false>(G, B.a[3]); break;
+    case 0: back_column<ORDER, false>(G, B.a[0]); break;
+    case 1: back_column<ORDER, false>(G, B.a[1]); break;
+    case 2: back_column<ORDER, false>(G, B.a[2]); break;
+    default: back_column<ORDER, true>(G, B.a[3]); break;
     }
 }
 
-void launch_solve4(const Geo& G, const SolveBatch& B, cudaStream_t st)
+void launch_back4(const Geo& G, const SolveBatch& B, cudaStream_t st)
 {
     dim3 grd((unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS), 4);
-    if (G.order == 2) k_solve4<2><<<grd, SOLVE_THREADS, solve_smem_bytes(), st>>>(G, B);
-    else k_solve4<4><<<grd, SOLVE_THREADS, solve_smem_bytes(), st>>>(G, B);
+    if (G.order == 2) k_back4<2><<<grd, SOLVE_THREADS, 0, st>>>(G, B);
+    else k_back4<4><<<grd, SOLVE_THREADS, 0, st>>>(G, B);
 }
 
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st)
