@@ -641,40 +641,85 @@ __host__ __device__ constexpr int p2_pad(int n) { return n + n / 8; }
 // groups) or 4 lines at two consecutive positions (N = 512; stride = 2 mod 8).
 __host__ __device__ constexpr int p2_stride_x(int n) { return p2_pad(n) + (p2_lines(n) >= 8 ? 1 : 2); }
 
-template <int ORDER>
-__device__ __forceinline__ double div_point(const Geo& G, const DivArgs& A, int k, int i, int j, double uc, bool corr)
+// Divergence of the power-of-two path as its own streaming kernel
+// (divergence{2,4}, pressure.c:40-117).  A block owns an 8 (i) x 32 (j)
+// tile and climbs DV_KC planes.  Per plane, u with its x halo (rows i-2 ..
+// i+8) and v with its y halo (columns j-2 .. j+32) are staged in shared
+// memory by cp.async, double-buffered one plane ahead, so each value crosses
+// L2 once; w is carried up the column in a register window, and at the walls
+// that window supplies the extrapolated w of pressure.c:80-95.  The x
+// transform then reads the result as a real field.
+constexpr int DV_I = 8, DV_J = 32, DV_KC = 8;
+
+__device__ __forceinline__ void dv_cp8(double* dst, const double* src)
 {
-    // divergence{2,4} (pressure.c:40-117), u read as u + G_u mdpdx
-    const int nx = G.nx, ny = G.ny, n2 = G.n2;
-    const int kb = GZ - 1, kt = n2 - GZ - 1;
-    auto I = [&](int kk, int ii, int jj) { return ((long long) kk * nx + ii) * ny + jj; };
-    auto U = [&](int di) { double t = __ldg(A.u + I(k, wrapp(i + di, nx), j)); return corr ? t + uc : t; };
-    auto V = [&](int dj) { return __ldg(A.v + I(k, i, wrapp(j + dj, ny))); };
-    auto Wr = [&](int kk) { return __ldg(A.w + I(kk, i, j)); };
-    // divisions by the metrics are multiplications by their reciprocals
-    const double idzk = G.idz[k];
-    if (ORDER == 2)
-        return (U(0) - U(-1)) * G.idx + (V(0) - V(-1)) * G.idy + (Wr(k) - Wr(k - 1)) * idzk;
-    double wkm2 = (k - 2 == kb - 1) ? 2.0 * Wr(kb) - Wr(kb + 1) : Wr(k - 2);  // pressure.c:80-87
-    double wkp1 = (k + 1 == kt + 1) ? 2.0 * Wr(kt) - Wr(kt - 1) : Wr(k + 1);  // pressure.c:88-95
-    return (A1 * (U(0) - U(-1)) + A2 * (U(1) - U(-2))) * G.idx
-         + (A1 * (V(0) - V(-1)) + A2 * (V(1) - V(-2))) * G.idy
-         + (A1 * (Wr(k) - Wr(k - 1)) + A2 * (wkp1 - wkm2)) * idzk;
+    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// Divergence of the power-of-two path as its own streaming kernel (one
-// thread per point, rows of 32 consecutive j); the x transform then reads
-// it as a real field.
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_div(Geo G, DivArgs A)
+__global__ void __launch_bounds__(DV_I * DV_J) k_div(Geo G, DivArgs A)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = GZ + blockIdx.z;
-    if (j >= G.ny || i >= G.nx) return;
+    __shared__ double su[2][DV_I + 3][DV_J];   // u, rows i0-2 .. i0+8
+    __shared__ double sv[2][DV_I][DV_J + 3];   // v, columns j0-2 .. j0+32
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DV_J + tx;
+    const int j0 = blockIdx.x * DV_J, i0 = blockIdx.y * DV_I;
+    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const long long plane = G.plane;
+    const int k0 = GZ + blockIdx.z * DV_KC;
+    const int k1 = min(k0 + DV_KC, n2 - GZ);
+    const int i = i0 + ty, j = j0 + tx;
+    const bool valid = i < nx && j < ny;
+    auto load = [&](int kk, int buf) {
+        const double* uk = A.u + kk * plane;
+        const double* vk = A.v + kk * plane;
+        for (int e = tid; e < (DV_I + 3) * DV_J; e += DV_I * DV_J) {
+            const int r = e / DV_J, c = e - r * DV_J;
+            int ii = (i0 - 2 + r) % nx; if (ii < 0) ii += nx;
+            dv_cp8(&su[buf][r][c], uk + ii * ny + min(j0 + c, ny - 1));
+        }
+        for (int e = tid; e < DV_I * (DV_J + 3); e += DV_I * DV_J) {
+            const int r = e / (DV_J + 3), c = e - r * (DV_J + 3);
+            int jj = (j0 - 2 + c) % ny; if (jj < 0) jj += ny;
+            dv_cp8(&sv[buf][r][c], vk + min(i0 + r, nx - 1) * ny + jj);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
     const bool corr = A.mu != nullptr;
-    const double uc = corr ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
-    A.dv[((long long) k * G.nx + i) * G.ny + j] = div_point<ORDER>(G, A, k, i, j, uc, corr);
+    const double mu = corr ? *A.mu : 0.0;
+    const int kb = GZ - 1, kt = n2 - GZ - 1;
+    const long long c = valid ? (long long) i * ny + j : 0;
+    const double* __restrict__ wp = A.w + c;
+    load(k0, 0);
+    // w at rows k-2 .. k (order 4) / k-1, k (order 2) for the first row
+    double w0 = ORDER == 4 ? __ldg(wp + (k0 - 2) * plane) : 0.0;
+    double w1 = __ldg(wp + (k0 - 1) * plane);
+    double w2 = __ldg(wp + k0 * plane);
+    for (int k = k0; k < k1; k++) {
+        const int buf = (k - k0) & 1;
+        if (k + 1 < k1) load(k + 1, buf ^ 1);
+        else asm volatile("cp.async.commit_group;\n" ::: "memory");
+        const double w3 = __ldg(wp + (k + 1) * plane);   // row k+1 (a ghost row at the top: unused there)
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        const double uc = corr ? A.gu[k] * mu : 0.0;   // chanfast.c:516-519
+        auto U = [&](int d) { return corr ? su[buf][ty + 2 + d][tx] + uc : su[buf][ty + 2 + d][tx]; };
+        auto V = [&](int d) { return sv[buf][ty][tx + 2 + d]; };
+        const double idzk = G.idz[k];
+        double d;
+        if (ORDER == 2) {
+            d = (U(0) - U(-1)) * G.idx + (V(0) - V(-1)) * G.idy + (w2 - w1) * idzk;
+        } else {
+            const double wkm2 = (k - 2 == kb - 1) ? 2.0 * w1 - w2 : w0;   // pressure.c:80-87
+            const double wkp1 = (k + 1 == kt + 1) ? 2.0 * w2 - w1 : w3;   // pressure.c:88-95
+            d = (A1 * (U(0) - U(-1)) + A2 * (U(1) - U(-2))) * G.idx
+              + (A1 * (V(0) - V(-1)) + A2 * (V(1) - V(-2))) * G.idy
+              + (A1 * (w2 - w1) + A2 * (wkp1 - wkm2)) * idzk;
+        }
+        if (valid) A.dv[k * plane + c] = d;
+        w0 = w1; w1 = w2; w2 = w3;
+        __syncthreads();   // this buffer is refilled two planes on
+    }
 }
 
 // Real-to-complex x transform (fftx_d2c, pressure.c:122-160, scaled by 1/N)
@@ -800,7 +845,7 @@ static size_t p2_smem_y() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(dou
 template <int N>
 static void launch_div_fftx_p2(const Geo& G, const DivArgs& A, cudaStream_t st)
 {
-    dim3 blk(32, 4, 1), grd((G.ny + 31) / 32, (G.nx + 3) / 4, G.nz);
+    dim3 blk(DV_J, DV_I, 1), grd((G.ny + DV_J - 1) / DV_J, (G.nx + DV_I - 1) / DV_I, (G.nz + DV_KC - 1) / DV_KC);
     if (G.order == 2) k_div<2><<<grd, blk, 0, st>>>(G, A);
     else k_div<4><<<grd, blk, 0, st>>>(G, A);
     constexpr int L = p2_lines(N / 2);
