@@ -29,6 +29,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["host_band.cpp", "kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu", "instance.cu"]
 FMA_SOURCES = {"kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu"}
 LIB_CUDA = os.path.join(HERE, "libchanfast_cuda.so")
+# The reference's step functions (include/chanfast_steps.h): their own
+# library, bit-exact arithmetic (no FMA contraction).
+STEPS_SOURCE = "steps.cu"
+LIB_STEPS = os.path.join(HERE, "libchanfast_steps.so")
 LIB_DRIVER = os.path.join(HERE, "libchanfast.so")
 
 
@@ -69,6 +73,17 @@ def build(verbose=False, ptxas_info=False):
             sys.stdout.write(out)
     if _stale(LIB_CUDA, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIB_CUDA, *objs, "-lcudart"])
+    steps_src = os.path.join(CSRC, STEPS_SOURCE)
+    steps_hdr = os.path.join(INCLUDE, "chanfast_steps.h")
+    if os.path.exists(steps_src) and _stale(LIB_STEPS, [steps_src, steps_hdr]):
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--extended-lambda", "-Xcompiler",
+               "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", INCLUDE, "-shared", steps_src, "-o", LIB_STEPS,
+               "-Xlinker", "-Bsymbolic", "-lcudart"]
+        if ptxas_info:
+            cmd[1:1] = ["-Xptxas", "-v"]
+        out = _run(cmd)
+        if verbose or ptxas_info:
+            sys.stdout.write(out)
     drv = os.path.join(CSRC, "chanfast_driver.c")
     if os.path.exists(drv) and _stale(LIB_DRIVER, [drv, LIB_CUDA] + headers):
         _run([CC, "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-I", INCLUDE, drv, "-o", LIB_DRIVER,
