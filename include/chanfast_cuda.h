@@ -4,8 +4,8 @@
  * plain C ABI.  Two shared libraries implement it:
  *
  *   libchanfast_cuda.so  device engine + this instance API (cf_*)
- *   libchanfast.so       drop-in drivers chanfast2 / chanfast4 in C, on top of
- *                        the instance API
+ *   libchanfast.so       drop-in drivers chanfast2 / chanfast4 / channel2 /
+ *                        channel4 in C, on top of the instance API
  *
  * Conventions
  *  - Every cf_* function returns an int status: CF_OK (0) or a negative CF_E*
@@ -42,8 +42,11 @@ enum {
 enum { CF_U = 0, CF_V = 1, CF_W = 2, CF_C = 3, CF_P = 4 };
 enum { CF_LAYOUT_PADDED = 0, CF_LAYOUT_INTERIOR = 1 };
 
-/* Arguments of chanfast2 / chanfast4 (reference chanfast.h:1-21) that
- * determine one run; p_row = p_col = 1, it/nt/istat/cfl belong to the driver. */
+/* Arguments of chanfast2 / chanfast4 / channel2 / channel4 (reference
+ * chanfast.h:1-21, channel.h:1-21) that determine one run, plus the scheme
+ * that tells the two driver families apart; p_row = p_col = 1,
+ * it/nt/istat/cfl belong to the driver.  Zero-initialise the struct: a zero
+ * scheme is CF_SCHEME_CHANFAST. */
 typedef struct cf_config {
     int order;               /* 2 (chanfast2) or 4 (chanfast4) */
     int nx, ny, nz;          /* interior grid */
@@ -55,7 +58,16 @@ typedef struct cf_config {
     double want_uvolavg, want_cvolavg;
     double setuframe, setvframe;      /* Galilean frame (chanfast.c:61-64) */
     double betg_x, betg_y, betg_z;    /* buoyancy */
+    int scheme;              /* CF_SCHEME_CHANFAST (0) or CF_SCHEME_CHANNEL (1) */
 } cf_config;
+
+/* Time-integration schemes.  CHANFAST: diffusion implicit in z only, x-y
+ * diffusion explicit (chanfast2/chanfast4, chanfast.c:395-656).  CHANNEL:
+ * diffusion fully implicit, solved per (kx, ky) wavenumber after a 2-D FFT
+ * (channel2/channel4, channel.c:392-690 / 1342-1640); needs nx in
+ * {64, 128, 256, 512} and, at order 4, nz >= 8. */
+#define CF_SCHEME_CHANFAST 0
+#define CF_SCHEME_CHANNEL 1
 
 typedef struct cf_instance cf_instance;
 
@@ -162,7 +174,8 @@ const char *cf_strerror(int status);
  * outputdir/{u,v,w,c}_it<N>.dat every istat steps.  p_row * p_col must be
  * 1.  The reference returns nothing and aborts on error; these print the
  * failing status to stderr and return.  chanfast2_status / chanfast4_status
- * return it instead.
+ * return it instead.  channel2 / channel4 (channel.h:1-21) are the same with
+ * the fully implicit scheme (CF_SCHEME_CHANNEL and its size limits).
  * ------------------------------------------------------------------------ */
 void chanfast2(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
                int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
@@ -188,6 +201,30 @@ int chanfast4_status(int p_row, int p_col, int nx, int ny, int nz, int it, int n
                      double dpdx, double want_uvolavg, int uvolavgmode,
                      double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
                      double betg_x, double betg_y, double betg_z);
+void channel2(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+              int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+              double dt, double want_cfl, int cflmode, double nu, double prandtl,
+              double dpdx, double want_uvolavg, int uvolavgmode,
+              double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+              double betg_x, double betg_y, double betg_z);
+void channel4(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+              int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+              double dt, double want_cfl, int cflmode, double nu, double prandtl,
+              double dpdx, double want_uvolavg, int uvolavgmode,
+              double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+              double betg_x, double betg_y, double betg_z);
+int channel2_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                    int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                    double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                    double dpdx, double want_uvolavg, int uvolavgmode,
+                    double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                    double betg_x, double betg_y, double betg_z);
+int channel4_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                    int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                    double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                    double dpdx, double want_uvolavg, int uvolavgmode,
+                    double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                    double betg_x, double betg_y, double betg_z);
 
 #ifdef __cplusplus
 }

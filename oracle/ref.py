@@ -60,6 +60,7 @@ def lib():
             L.ref_set_field.argtypes = [vp, ctypes.c_int, dp]
             L.ref_get_field.argtypes = [vp, ctypes.c_int, dp]
             L.ref_substeps.argtypes = [vp, ctypes.c_long]
+            L.ref_channel_substeps.argtypes = [vp, ctypes.c_long]
             L.ref_project.argtypes = [vp, ctypes.c_double]
             L.ref_divergence.argtypes = [vp, dp]
             L.ref_log.restype = ctypes.c_long
@@ -68,6 +69,7 @@ def lib():
             L.ref_chanfast.argtypes = ([ctypes.c_char_p] + [ctypes.c_int] * 10 + [ctypes.c_double] * 5
                                        + [ctypes.c_int] + [ctypes.c_double] * 4 + [ctypes.c_int]
                                        + [ctypes.c_double, ctypes.c_int] + [ctypes.c_double] * 5)
+            L.ref_channel.argtypes = L.ref_chanfast.argtypes
             _lib = L
         return _lib
 
@@ -122,8 +124,11 @@ class RefInstance:
         self.L.ref_metrics(self.ctx, _dp(dz), _dp(zp), _dp(zw))
         return dz, zp, zw
 
-    def substeps(self, n):
-        if self.L.ref_substeps(self.ctx, n) != 0:
+    def substeps(self, n, scheme="chanfast"):
+        """n RK3 substeps of the chanfast (z-implicit) or channel (fully
+        implicit, channel.c) scheme."""
+        fn = {"chanfast": self.L.ref_substeps, "channel": self.L.ref_channel_substeps}[scheme]
+        if fn(self.ctx, n) != 0:
             raise RuntimeError("reference substep aborted (check() failed)")
 
     def project(self, dt=1.0):
@@ -143,15 +148,17 @@ class RefInstance:
         return out[:n]
 
 
-def run_chanfast(workdir, prm, it, nt, istat=None, cflmode=0, want_cfl=1.0):
-    """Run the unmodified chanfast2/chanfast4 driver in `workdir` (reads
-    outputdir/{u,v,w,c}_it<it>.dat, writes *_it<nt>.dat)."""
+def run_chanfast(workdir, prm, it, nt, istat=None, cflmode=0, want_cfl=1.0, scheme="chanfast"):
+    """Run the unmodified chanfast2/chanfast4 (or, with scheme="channel",
+    channel2/channel4) driver in `workdir` (reads outputdir/{u,v,w,c}_it<it>.dat,
+    writes *_it<nt>.dat)."""
     L = lib()
     istat = nt - it if istat is None else istat
-    rc = L.ref_chanfast(workdir.encode(), prm.order, prm.nx, prm.ny, prm.nz, it, nt, istat,
-                        prm.ngx, prm.ngy, prm.ngz, prm.lx, prm.ly, prm.lz, prm.dt, want_cfl,
-                        cflmode, prm.nu, prm.prandtl, prm.dpdx, prm.want_uvolavg, prm.uvolavgmode,
-                        prm.want_cvolavg, prm.cvolavgmode, prm.setuframe, prm.setvframe,
-                        prm.betg_x, prm.betg_y, prm.betg_z)
+    fn = {"chanfast": L.ref_chanfast, "channel": L.ref_channel}[scheme]
+    rc = fn(workdir.encode(), prm.order, prm.nx, prm.ny, prm.nz, it, nt, istat,
+            prm.ngx, prm.ngy, prm.ngz, prm.lx, prm.ly, prm.lz, prm.dt, want_cfl,
+            cflmode, prm.nu, prm.prandtl, prm.dpdx, prm.want_uvolavg, prm.uvolavgmode,
+            prm.want_cvolavg, prm.cvolavgmode, prm.setuframe, prm.setvframe,
+            prm.betg_x, prm.betg_y, prm.betg_z)
     if rc != 0:
-        raise RuntimeError(f"chanfast aborted rc={rc}")
+        raise RuntimeError(f"{scheme} driver aborted rc={rc}")

@@ -13,6 +13,12 @@
  * dt is fixed (cflmode = 0).  tests/ checks this replay against the real
  * chanfast2/chanfast4 entry points (bit-identical u, v, w, c).
  *
+ * ref_channel_substeps replays the fully implicit substep of channel2 /
+ * channel4 (channel.c:392-690 / :1342-1640) the same way: explicit terms
+ * without the x-y Laplacian, then per field the 3-D Helmholtz operator,
+ * FFT3D_FWD, solve_helmholtz_{u,w}, FFT3D_BWD; tests/ checks it against the
+ * real channel2/channel4 entry points (ref_channel).
+ *
  * Also exported: the case-1 style projection (cases.c:426-470) used to make
  * initial states divergence-free, and the reference divergence operator.
  */
@@ -38,6 +44,7 @@
 #include "advect.h"
 #include "scalar.h"
 #include "chanfast.h"
+#include "channel.h"
 #include "cases.h"
 
 extern jmp_buf *shim_abort_target;
@@ -416,12 +423,15 @@ typedef void (*mflux_t)(double *, double *, double *, double *, double *, double
                         int, int, int, int, int, int, double, double, double *);
 typedef void (*adv_t)(double *, double *, double *, double *, double *,
                       int, int, int, int, int, int, double, double, double *);
+typedef void (*op3fn_t)(double *, double *, int, int, int, int, int, int, double, double, double *, double);
+typedef void (*spfn_t)(fftw_complex *, int, int, int, int, int, int, int, int, double, double, double *,
+                       double, double, double, int, int);
 
-/* Run `nsub` RK3 substeps (chanfast.c:395-656 / 1319-1580), continuing the
- * substep counter and the f/g history kept in the context. */
-int ref_substeps(void *vc, long nsub)
+/* Run `nsub` RK3 substeps, continuing the substep counter and the f/g
+ * history kept in the context.  scheme 0: chanfast (chanfast.c:395-656 /
+ * 1319-1580); scheme 1: channel (channel.c:392-690 / 1342-1640). */
+static int substeps_impl(ref_ctx *c, long nsub, int scheme)
 {
-    ref_ctx *c = (ref_ctx *) vc;
     const ref_params *q = &c->prm;
     GUARD(-1);
     int o4 = q->order == 4;
@@ -437,6 +447,12 @@ int ref_substeps(void *vc, long nsub)
             mfz = o4 ? massfluxz4 : massfluxz2;
     adv_t adu = o4 ? advectu4 : advectu2, adv = o4 ? advectv4 : advectv2,
           adw = o4 ? advectw4 : advectw2;
+    op3fn_t hop3_u = o4 ? helmholtz_operator_u4 : helmholtz_operator_u2;
+    op3fn_t hop3_w = o4 ? helmholtz_operator_w4 : helmholtz_operator_w2;
+    spfn_t spec_u = o4 ? solve_helmholtz_u4 : solve_helmholtz_u2;
+    spfn_t spec_w = o4 ? solve_helmholtz_w4 : solve_helmholtz_w2;
+    const int implicit3d = scheme == 1;
+    decomp_plan *dc = c->decomp_c;
 
     module_init(q->order, q->nz, q->ngz);
     uframe_s = q->setuframe;
@@ -477,12 +493,15 @@ int ref_substeps(void *vc, long nsub)
         adv(v, m1, m2, m3, fv, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz);
         mfz(u, v, w, m1, m2, m3, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz);
         adw(w, m1, m2, m3, fw, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz);
-        lap_u(u, fu, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu);
-        lap_u(v, fv, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu);
-        lap_w(w, fw, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu);
+        if (!implicit3d) {   /* channel.c:419-438 has no explicit x-y diffusion */
+            lap_u(u, fu, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu);
+            lap_u(v, fv, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu);
+            lap_w(w, fw, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu);
+        }
         flux_quick(u, v, w, cc, m1, m2, m3, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz);
         advect_scalar(m1, m2, m3, fc, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz);
-        lap_u(cc, fc, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu / pr);
+        if (!implicit3d)
+            lap_u(cc, fc, lnx, lny, nz, ngx, ngy, ngz, dx, dy, nu / pr);
         if (o4)
             add_buoyancy4(cc, fu, fv, fw, q->betg_x, q->betg_y, q->betg_z, lnx, lny, nz, ngx, ngy, ngz);
         else
@@ -518,13 +537,30 @@ int ref_substeps(void *vc, long nsub)
             (void) kap;
 
             abc(x, lnx, lny, nz, ngx, ngy, ngz, xb, yb, dz, bb, bt, bt_, bt_);
-            hop(x, h, lnx, lny, nz, ngx, ngy, ngz, dz, na);
-            for (int i = 0; i < ls; i++) h[i] += gamdt * fx[i] + zetdt * gx[i];
-            for (int i = 0; i < ls; i++) bc[i] = 0.0;
-            abc(bc, lnx, lny, nz, ngx, ngy, ngz, xb, yb, dz, bb, bt, bt_, bt_);
-            hop(bc, hbc, lnx, lny, nz, ngx, ngy, ngz, dz, -nb);
-            for (int i = 0; i < ls; i++) h[i] -= hbc[i];
-            slv(x, h, lnx, lny, nz, ngx, ngy, ngz, dz, -nb, 0.0, 0.0, bt_, bt_);
+            if (implicit3d) {   /* channel.c:455-485 (u); same for v, c, w */
+                op3fn_t hop3 = isw ? hop3_w : hop3_u;
+                hop3(x, h, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz, na);
+                for (int i = 0; i < ls; i++) h[i] += gamdt * fx[i] + zetdt * gx[i];
+                for (int i = 0; i < ls; i++) bc[i] = 0.0;
+                abc(bc, lnx, lny, nz, ngx, ngy, ngz, xb, yb, dz, bb, bt, bt_, bt_);
+                hop3(bc, hbc, lnx, lny, nz, ngx, ngy, ngz, dx, dy, dz, -nb);
+                for (int i = 0; i < ls; i++) h[i] -= hbc[i];
+                fft3d_fwd(c, c->h_3d);
+                (isw ? spec_w : spec_u)(&(c->zwork_c1[dc->zst[0]][dc->zst[1]][dc->zst[2]]),
+                                        q->nx, dc->zsz[0], dc->zst[0] - 1, q->ny, dc->zsz[1], dc->zst[1] - 1,
+                                        nz, ngz, dx, dy, dz, -nb, 0.0, 0.0, bt_, bt_);
+                double ***x3 = fld == 0 ? c->u_3d : fld == 1 ? c->v_3d : fld == 2 ? c->c_3d : c->w_3d;
+                fft3d_bwd(c, x3);
+                ghostz_periodic(x, c->ghostz_p);
+            } else {
+                hop(x, h, lnx, lny, nz, ngx, ngy, ngz, dz, na);
+                for (int i = 0; i < ls; i++) h[i] += gamdt * fx[i] + zetdt * gx[i];
+                for (int i = 0; i < ls; i++) bc[i] = 0.0;
+                abc(bc, lnx, lny, nz, ngx, ngy, ngz, xb, yb, dz, bb, bt, bt_, bt_);
+                hop(bc, hbc, lnx, lny, nz, ngx, ngy, ngz, dz, -nb);
+                for (int i = 0; i < ls; i++) h[i] -= hbc[i];
+                slv(x, h, lnx, lny, nz, ngx, ngy, ngz, dz, -nb, 0.0, 0.0, bt_, bt_);
+            }
             abc(x, lnx, lny, nz, ngx, ngy, ngz, xb, yb, dz, bb, bt, bt_, bt_);
 
             if (fld == 0 || fld == 2) {
@@ -578,13 +614,29 @@ int ref_substeps(void *vc, long nsub)
     return 0;
 }
 
+int ref_substeps(void *vc, long nsub) { return substeps_impl((ref_ctx *) vc, nsub, 0); }
+int ref_channel_substeps(void *vc, long nsub) { return substeps_impl((ref_ctx *) vc, nsub, 1); }
+
 /* The real drivers, unmodified, run inside directory `workdir` (they read and
  * write outputdir/ relative to the current directory). */
-int ref_chanfast(const char *workdir, int order, int nx, int ny, int nz, int it, int nt, int istat,
-                 int ngx, int ngy, int ngz, double lx, double ly, double lz, double dt,
-                 double want_cfl, int cflmode, double nu, double prandtl, double dpdx,
-                 double want_uvolavg, int uvolavgmode, double want_cvolavg, int cvolavgmode,
-                 double setuframe, double setvframe, double betg_x, double betg_y, double betg_z)
+typedef void (*driver_t)(int, int, int, int, int, int, int, int, int, int, int, double, double, double,
+                         double, double, int, double, double, double, double, int, double, int, double,
+                         double, double, double, double);
+
+#define DRIVER_PARAMS const char *workdir, int order, int nx, int ny, int nz, int it, int nt, int istat, \
+                      int ngx, int ngy, int ngz, double lx, double ly, double lz, double dt, \
+                      double want_cfl, int cflmode, double nu, double prandtl, double dpdx, \
+                      double want_uvolavg, int uvolavgmode, double want_cvolavg, int cvolavgmode, \
+                      double setuframe, double setvframe, double betg_x, double betg_y, double betg_z
+#define DRIVER_ARGS nx, ny, nz, it, nt, istat, ngx, ngy, ngz, lx, ly, lz, dt, want_cfl, cflmode, \
+                    nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg, cvolavgmode, \
+                    setuframe, setvframe, betg_x, betg_y, betg_z
+
+static int run_driver(driver_t drv, const char *workdir, int nx, int ny, int nz, int it, int nt, int istat,
+                      int ngx, int ngy, int ngz, double lx, double ly, double lz, double dt,
+                      double want_cfl, int cflmode, double nu, double prandtl, double dpdx,
+                      double want_uvolavg, int uvolavgmode, double want_cvolavg, int cvolavgmode,
+                      double setuframe, double setvframe, double betg_x, double betg_y, double betg_z)
 {
     char cwd[4096];
     if (!getcwd(cwd, sizeof(cwd))) return -2;
@@ -596,17 +648,20 @@ int ref_chanfast(const char *workdir, int order, int nx, int ny, int nz, int it,
         if (chdir(cwd) != 0) return -4;
         return -1;
     }
-    if (order == 2)
-        chanfast2(1, 1, nx, ny, nz, it, nt, istat, ngx, ngy, ngz, lx, ly, lz, dt, want_cfl, cflmode,
-                  nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg, cvolavgmode,
-                  setuframe, setvframe, betg_x, betg_y, betg_z);
-    else
-        chanfast4(1, 1, nx, ny, nz, it, nt, istat, ngx, ngy, ngz, lx, ly, lz, dt, want_cfl, cflmode,
-                  nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg, cvolavgmode,
-                  setuframe, setvframe, betg_x, betg_y, betg_z);
+    drv(1, 1, DRIVER_ARGS);
     shim_abort_target = NULL;
     if (chdir(cwd) != 0) return -4;
     return 0;
+}
+
+int ref_chanfast(DRIVER_PARAMS)
+{
+    return run_driver(order == 2 ? chanfast2 : chanfast4, workdir, DRIVER_ARGS);
+}
+
+int ref_channel(DRIVER_PARAMS)
+{
+    return run_driver(order == 2 ? channel2 : channel4, workdir, DRIVER_ARGS);
 }
 
 /* Known-answer cases of cases.c (case0..case16) at one rank. */

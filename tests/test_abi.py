@@ -39,7 +39,7 @@ def libs(cf):
 
 def test_every_declared_symbol_is_exported(libs):
     decl = declared_functions()
-    assert {"cf_create", "cf_step", "chanfast2", "chanfast4"} <= decl
+    assert {"cf_create", "cf_step", "chanfast2", "chanfast4", "channel2", "channel4"} <= decl
     assert {"advectu4", "pressure_poisson4", "solve_helmholtz1d_w4", "heptdag"} <= decl
     have = exported(libs[0]) | exported(libs[1]) | exported(libs[2])
     missing = sorted(decl - have)
@@ -58,6 +58,14 @@ def test_strerror_and_argument_checks(cf):
     assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL
     bad = cf.Config.make(order=4, nx=14, ny=16, nz=16, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3)
     assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL  # 14 = 2*7: no radix-7 FFT
+    # the fully implicit scheme: power-of-two nx of 64..512, nz >= 8 at order 4, known scheme ids
+    bad = cf.Config.make(order=2, nx=48, ny=16, nz=16, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3, scheme="channel")
+    assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL
+    bad = cf.Config.make(order=4, nx=64, ny=16, nz=7, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3, scheme="channel")
+    assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL
+    bad = cf.Config.make(order=4, nx=64, ny=16, nz=16, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3)
+    bad.scheme = 2
+    assert L.cf_create(ctypes.byref(bad), None, ctypes.byref(h)) == cf.CF_EINVAL
     assert L.cf_step(None, 1) == cf.CF_EINVAL
 
 

@@ -40,6 +40,9 @@ class ChanfastError(RuntimeError):
         self.status = status
 
 
+SCHEMES = {"chanfast": 0, "channel": 1}   # CF_SCHEME_CHANFAST, CF_SCHEME_CHANNEL
+
+
 class Config(ctypes.Structure):
     """Mirror of cf_config."""
 
@@ -47,28 +50,33 @@ class Config(ctypes.Structure):
                 ("order", "nx", "ny", "nz", "ngx", "ngy", "ngz", "uvolavgmode", "cvolavgmode")] + \
                [(n, ctypes.c_double) for n in
                 ("lx", "ly", "lz", "dt", "nu", "prandtl", "dpdx", "want_uvolavg", "want_cvolavg",
-                 "setuframe", "setvframe", "betg_x", "betg_y", "betg_z")]
+                 "setuframe", "setvframe", "betg_x", "betg_y", "betg_z")] + \
+               [("scheme", ctypes.c_int)]
 
     @classmethod
     def make(cls, order, nx, ny, nz, lx, ly, lz, dt, nu, prandtl=1.0, dpdx=0.0,
              want_uvolavg=1.0, uvolavgmode=1, want_cvolavg=0.0, cvolavgmode=1,
              setuframe=0.0, setvframe=0.0, betg_x=0.0, betg_y=0.0, betg_z=0.0,
-             ngx=3, ngy=3, ngz=3):
+             ngx=3, ngy=3, ngz=3, scheme="chanfast"):
         c = cls()
         for k, v in dict(order=order, nx=nx, ny=ny, nz=nz, ngx=ngx, ngy=ngy, ngz=ngz,
                          uvolavgmode=uvolavgmode, cvolavgmode=cvolavgmode, lx=lx, ly=ly, lz=lz,
                          dt=dt, nu=nu, prandtl=prandtl, dpdx=dpdx, want_uvolavg=want_uvolavg,
                          want_cvolavg=want_cvolavg, setuframe=setuframe, setvframe=setvframe,
-                         betg_x=betg_x, betg_y=betg_y, betg_z=betg_z).items():
+                         betg_x=betg_x, betg_y=betg_y, betg_z=betg_z, scheme=SCHEMES[scheme]).items():
             setattr(c, k, v)
         return c
 
     @classmethod
-    def from_params(cls, p):
-        """From any object with the same attribute names (e.g. the oracle's Params)."""
+    def from_params(cls, p, scheme="chanfast"):
+        """From any object with the same attribute names (e.g. the oracle's
+        Params); `scheme` names the time integration ("chanfast": z-implicit
+        diffusion, "channel": fully implicit)."""
         c = cls()
         for name, _ in cls._fields_:
-            setattr(c, name, getattr(p, name))
+            if name != "scheme":
+                setattr(c, name, getattr(p, name))
+        c.scheme = SCHEMES[scheme]
         return c
 
     def padded_shape(self):
@@ -115,7 +123,7 @@ def lib():
 
 
 def driver_lib():
-    """libchanfast.so: the C drop-in drivers chanfast2 / chanfast4."""
+    """libchanfast.so: the C drop-in drivers chanfast2 / chanfast4 / channel2 / channel4."""
     global _drv
     if _drv is None:
         lib()
@@ -124,7 +132,7 @@ def driver_lib():
         D = ctypes.CDLL(LIB_DRIVER)
         args = ([ctypes.c_int] * 11 + [ctypes.c_double] * 5 + [ctypes.c_int] + [ctypes.c_double] * 4
                 + [ctypes.c_int] + [ctypes.c_double, ctypes.c_int] + [ctypes.c_double] * 5)
-        for name in ("chanfast2_status", "chanfast4_status"):
+        for name in ("chanfast2_status", "chanfast4_status", "channel2_status", "channel4_status"):
             getattr(D, name).argtypes = args
             getattr(D, name).restype = ctypes.c_int
         _drv = D
@@ -254,4 +262,12 @@ def chanfast(order, *args):
     reference, chanfast.h:1-21); returns the status instead of aborting."""
     D = driver_lib()
     fn = D.chanfast2_status if order == 2 else D.chanfast4_status
+    return fn(*args)
+
+
+def channel(order, *args):
+    """Call the C drop-in driver channel2/channel4 (same arguments as the
+    reference, channel.h:1-21); returns the status instead of aborting."""
+    D = driver_lib()
+    fn = D.channel2_status if order == 2 else D.channel4_status
     return fn(*args)

@@ -1,8 +1,11 @@
 /*
- * Drop-in drivers chanfast2 / chanfast4 in C over the chanfast_cuda C ABI.
+ * Drop-in drivers chanfast2 / chanfast4 / channel2 / channel4 in C over the
+ * chanfast_cuda C ABI.
  *
  * Same arguments and file protocol as the reference drivers (chanfast.h:1-21,
- * chanfast.c:71-992 / 995-1916) at p_row = p_col = 1:
+ * chanfast.c:71-992 / 995-1916; channel.h:1-21, channel.c:71-1018 /
+ * 1021-1968, the same loop with the fully implicit substep) at
+ * p_row = p_col = 1:
  *   - read outputdir/{u,v,w,c}_it<it>.dat (raw FP64, C order [nx][ny][nz],
  *     io.c:259-297)
  *   - for it in [it, nt): CFL of the current field (get.c:390-416), adapt dt
@@ -11,8 +14,8 @@
  *     the last substep to outputdir/pstat.dat and outputdir/cstat.dat
  *     (chanfast.c:525-528, 612-615)
  *   - every istat steps write outputdir/{u,v,w,c}_it<it+1>.dat (io.c:211-257)
- * The per-istat statistics profiles and spectra of chanfast.c:658-857 are
- * not produced.
+ * The per-istat statistics profiles and spectra of chanfast.c:658-857
+ * (channel.c:692-891) are not produced.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -65,7 +68,7 @@ static int append_ascii(const double *u, int n, const char *filename)
     return fclose(fp) == 0 ? CF_OK : CF_EIO;
 }
 
-static int run(int order, int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+static int run(int order, int scheme, int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
                int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
                double dt, double want_cfl, int cflmode, double nu, double prandtl,
                double dpdx, double want_uvolavg, int uvolavgmode,
@@ -84,6 +87,7 @@ static int run(int order, int p_row, int p_col, int nx, int ny, int nz, int it, 
     cfg.want_uvolavg = want_uvolavg; cfg.want_cvolavg = want_cvolavg;
     cfg.setuframe = setuframe; cfg.setvframe = setvframe;
     cfg.betg_x = betg_x; cfg.betg_y = betg_y; cfg.betg_z = betg_z;
+    cfg.scheme = scheme;
 
     cf_instance *inst = NULL;
     int rc = cf_create(&cfg, NULL, &inst);
@@ -132,7 +136,7 @@ int chanfast2_status(int p_row, int p_col, int nx, int ny, int nz, int it, int n
                      double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
                      double betg_x, double betg_y, double betg_z)
 {
-    return run(2, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z, lx, ly, lz,
+    return run(2, CF_SCHEME_CHANFAST, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z, lx, ly, lz,
                dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg,
                cvolavgmode, setuframe, setvframe, betg_x, betg_y, betg_z);
 }
@@ -144,7 +148,7 @@ int chanfast4_status(int p_row, int p_col, int nx, int ny, int nz, int it, int n
                      double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
                      double betg_x, double betg_y, double betg_z)
 {
-    return run(4, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z, lx, ly, lz,
+    return run(4, CF_SCHEME_CHANFAST, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z, lx, ly, lz,
                dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg, uvolavgmode, want_cvolavg,
                cvolavgmode, setuframe, setvframe, betg_x, betg_y, betg_z);
 }
@@ -175,4 +179,56 @@ void chanfast4(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int
                               uvolavgmode, want_cvolavg, cvolavgmode, setuframe, setvframe,
                               betg_x, betg_y, betg_z);
     if (rc) fprintf(stderr, "chanfast4: %s\n", cf_strerror(rc));
+}
+
+int channel2_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                    int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                    double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                    double dpdx, double want_uvolavg, int uvolavgmode,
+                    double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                    double betg_x, double betg_y, double betg_z)
+{
+    return run(2, CF_SCHEME_CHANNEL, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z,
+               lx, ly, lz, dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg, uvolavgmode,
+               want_cvolavg, cvolavgmode, setuframe, setvframe, betg_x, betg_y, betg_z);
+}
+
+int channel4_status(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+                    int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+                    double dt, double want_cfl, int cflmode, double nu, double prandtl,
+                    double dpdx, double want_uvolavg, int uvolavgmode,
+                    double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+                    double betg_x, double betg_y, double betg_z)
+{
+    return run(4, CF_SCHEME_CHANNEL, p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z,
+               lx, ly, lz, dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg, uvolavgmode,
+               want_cvolavg, cvolavgmode, setuframe, setvframe, betg_x, betg_y, betg_z);
+}
+
+void channel2(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+              int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+              double dt, double want_cfl, int cflmode, double nu, double prandtl,
+              double dpdx, double want_uvolavg, int uvolavgmode,
+              double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+              double betg_x, double betg_y, double betg_z)
+{
+    int rc = channel2_status(p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z,
+                             lx, ly, lz, dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg,
+                             uvolavgmode, want_cvolavg, cvolavgmode, setuframe, setvframe,
+                             betg_x, betg_y, betg_z);
+    if (rc) fprintf(stderr, "channel2: %s\n", cf_strerror(rc));
+}
+
+void channel4(int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
+              int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
+              double dt, double want_cfl, int cflmode, double nu, double prandtl,
+              double dpdx, double want_uvolavg, int uvolavgmode,
+              double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
+              double betg_x, double betg_y, double betg_z)
+{
+    int rc = channel4_status(p_row, p_col, nx, ny, nz, it, nt, istat, nghost_x, nghost_y, nghost_z,
+                             lx, ly, lz, dt, want_cfl, cflmode, nu, prandtl, dpdx, want_uvolavg,
+                             uvolavgmode, want_cvolavg, cvolavgmode, setuframe, setvframe,
+                             betg_x, betg_y, betg_z);
+    if (rc) fprintf(stderr, "channel4: %s\n", cf_strerror(rc));
 }

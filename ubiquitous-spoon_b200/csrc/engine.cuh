@@ -124,21 +124,40 @@ struct DivArgs {
     double* dv;            // real divergence field [n2][nx][ny] (power-of-two nx path)
 };
 
+// Real-to-complex x transform of rows kfirst .. of nfields real fields
+// (blockIdx.z = field, fields src_fstride doubles apart) into spectra
+// spec_fstride complex values apart.
+struct R2cArgs {
+    const double* src;
+    double2* spec;
+    FftPlan px;
+    double c8;
+    int kfirst;
+    long long src_fstride, spec_fstride;
+};
+
 struct FftyArgs {
     double2* spec;
     FftPlan py;
     int sign;
     int kfirst;
     double c8;
+    long long fstride;    // complex values between the spectra of batched fields
 };
 
+// Inverse x transform of spectrum rows kfirst .. of field blockIdx.z into
+// the same rows of p[blockIdx.z].
 struct C2rArgs {
     const double2* spec;
-    double* p;
+    double* p[4];
     FftPlan px;
     double c8;
+    int kfirst;
+    long long fstride;
 };
 
+// One per-wavenumber band solve over spectrum rows GZ .. GZ+nrows-1: the
+// pressure Poisson equation or the spectral Helmholtz solve of one field.
 struct PoissonArgs {
     double2* spec;
     double* scratch;          // width 3: 1 x [n2][ncol]; width 7: 3 x [n2][ncol]
@@ -148,6 +167,10 @@ struct PoissonArgs {
     double dsub[2][6][3];
     WallRowsD bot[2], top;
     double dt, dxdx, dydy;
+    int nrows;                // nz; nz - 1 for the w Helmholtz solve
+    double* avg;              // Helmholtz solves of u and c: xy-average profile [n2] out, or null
+    WallRowsD abot, atop;     // apply_bc closure rows of that field (its average's ghost rows)
+    double abc_bot, abc_top;  // and its wall values
 };
 
 constexpr int POIS_THREADS = 128;  // k_poisson block: one thread per (kx, ky) column
@@ -165,18 +188,24 @@ struct ProjArgs {
 };
 
 // ---------------------------------------------------------------- launchers
-void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st);
-void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st);
+// extrap: w ghosts as massflux4 leaves them (before the advection);
+// otherwise as apply_bc_w leaves them (after the spectral solves)
+void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st, bool extrap = true);
+void launch_rhs(const Geo& G, const RhsArgs& A, bool implicit3d, cudaStream_t st);
 constexpr int SOLVE_THREADS = 128;   // k_back4 block: one thread per column
 struct SolveBatch {
     SolveArgs a[4];   // u, v, c, w
 };
 void launch_back4(const Geo& G, const SolveBatch& B, cudaStream_t st);
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st);
+void launch_mass_control(const MassArgs& M, cudaStream_t st);
 void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st);
-void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st);
-void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st);
+bool fftx_batched_supported(int nx);
+void launch_fftx_r2c(const Geo& G, const R2cArgs& A, int nrows, int nfields, cudaStream_t st);
+void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st, int nfields = 1);
+void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st, int nfields = 1);
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st);
+void launch_helmholtz_spectral(const Geo& G, const PoissonArgs& A, cudaStream_t st);
 void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st);
 cudaError_t fft_set_smem_limits(int max_n);
 cudaError_t rhs_set_smem_limits();

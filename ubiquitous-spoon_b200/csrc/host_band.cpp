@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <stdexcept>
 
 namespace cf {
@@ -263,16 +264,20 @@ static void w_stencil_top4(Band& B, const std::vector<double>& dz, int k, double
     B.e[kp2] = 0.0; B.f[kp2] = 0.0; B.g[kp2] = 0.0; B.r[kp2] = bc;
 }
 
-static void w_reduce_bot4(Band& B, int k)
+// `dsub` (optional) receives the two diagonal subtractions of row k+1.
+static void w_reduce_bot4(Band& B, int k, double dsub[3][3] = nullptr)
 {
     int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
     auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
     auto& e = B.e; auto& f = B.f; auto& r = B.r;
-    double fac;
+    double fac, t;
     fac = a[kp1] / b[k];
-    a[kp1] -= b[k] * fac; b[kp1] -= c[k] * fac; c[kp1] -= d[k] * fac; d[kp1] -= e[k] * fac; e[kp1] -= f[k] * fac;
+    a[kp1] -= b[k] * fac; b[kp1] -= c[k] * fac; c[kp1] -= d[k] * fac;
+    t = e[k] * fac; d[kp1] -= t; if (dsub) dsub[0][0] = t;
+    e[kp1] -= f[k] * fac;
     fac = b[kp1] / d[km1];
-    b[kp1] -= d[km1] * fac; c[kp1] -= e[km1] * fac; d[kp1] -= f[km1] * fac;
+    b[kp1] -= d[km1] * fac; c[kp1] -= e[km1] * fac;
+    t = f[km1] * fac; d[kp1] -= t; if (dsub) dsub[0][1] = t;
     fac = c[kp1] / f[km2];
     c[kp1] -= f[km2] * fac; r[kp1] -= r[km2] * fac;
     fac = a[kp2] / d[km1];
@@ -283,16 +288,20 @@ static void w_reduce_bot4(Band& B, int k)
     a[kp3] -= f[km2] * fac; r[kp3] -= r[km2] * fac;
 }
 
-static void w_reduce_top4(Band& B, int k)
+// `dsub` (optional) receives the two diagonal subtractions of row k-1.
+static void w_reduce_top4(Band& B, int k, double dsub[3][3] = nullptr)
 {
     int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
     auto& b = B.b; auto& c = B.c; auto& d = B.d;
     auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
-    double fac;
+    double fac, t;
     fac = g[km1] / f[k];
-    g[km1] -= f[k] * fac; f[km1] -= e[k] * fac; e[km1] -= d[k] * fac; d[km1] -= c[k] * fac; c[km1] -= b[k] * fac;
+    g[km1] -= f[k] * fac; f[km1] -= e[k] * fac; e[km1] -= d[k] * fac;
+    t = c[k] * fac; d[km1] -= t; if (dsub) dsub[0][0] = t;
+    c[km1] -= b[k] * fac;
     fac = f[km1] / d[kp1];
-    f[km1] -= d[kp1] * fac; e[km1] -= c[kp1] * fac; d[km1] -= b[kp1] * fac;
+    f[km1] -= d[kp1] * fac; e[km1] -= c[kp1] * fac;
+    t = b[kp1] * fac; d[km1] -= t; if (dsub) dsub[0][1] = t;
     fac = e[km1] / b[kp2];
     e[km1] -= b[kp2] * fac; r[km1] -= r[kp2] * fac;
     fac = g[km2] / d[kp1];
@@ -523,14 +532,16 @@ static void apply_factor(const LineFactor& L, const double* rhs, double* x)
     for (int i = 0; i < L.n; i++) x[i] = y[i];
 }
 
-// Interior band rows of solve_helmholtz1d_u{2,4} (diffuseu.c:190-201, 239-268).
-static void band_rows_u(const Metrics& m, Band& B, double nudt)
+// Interior band rows of solve_helmholtz1d_u{2,4} (diffuseu.c:190-201, 239-268);
+// with area = dx*dy, the z part of solve_helmholtz_u{2,4} (diffuseu.c:430-445,
+// 564-590), whose cell volume is dx*dy*dz.
+static void band_rows_u(const Metrics& m, Band& B, double nudt, double area = 1.0)
 {
     const auto& dz = m.dz;
     for (int k = m.gz; k < m.n2 - m.gz; k++) {
         double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
         double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-        double dvol = dz[k];
+        double dvol = area * dz[k];
         if (m.order == 2) {
             B.a[k] = +dvol * nudt / (dzm1h * dz[k]);
             B.c[k] = +dvol * nudt / (dzp1h * dz[k]);
@@ -553,14 +564,16 @@ static void band_rows_u(const Metrics& m, Band& B, double nudt)
     }
 }
 
-// Interior band rows of solve_helmholtz1d_w{2,4} (diffusew.c:192-205, 242-272).
-static void band_rows_w(const Metrics& m, Band& B, double nudt)
+// Interior band rows of solve_helmholtz1d_w{2,4} (diffusew.c:192-205, 242-272);
+// with area = dx*dy, the z part of solve_helmholtz_w{2,4} (diffusew.c:494-509,
+// 571-597).
+static void band_rows_w(const Metrics& m, Band& B, double nudt, double area = 1.0)
 {
     const auto& dz = m.dz;
     for (int k = m.gz; k < m.n2 - m.gz - 1; k++) {
         double dzp1 = dz[k + 1], dzm0 = dz[k];
         double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-        double dvol = dzp1h;
+        double dvol = area * dzp1h;
         if (m.order == 2) {
             B.a[k] = +dvol * nudt / (dzm0 * dzp1h);
             B.c[k] = +dvol * nudt / (dzp1 * dzp1h);
@@ -715,24 +728,32 @@ void solve_column(const ImplicitSet& s, const Metrics& m, bool is_w, std::vector
     out = B.x;
 }
 
+// Stencil coefficients of the 1-D Helmholtz operator on rows k0 .. k0+n-1:
+// the operator is linear, so its coefficients are its response to unit columns.
+static std::vector<double> operator_coefs(const Metrics& m, int k0, int n, bool is_w, double nudt)
+{
+    const int H = m.order == 2 ? 1 : 3;
+    std::vector<double> L((size_t) n * (2 * H + 1), 0.0);
+    std::vector<double> e(m.n2, 0.0);
+    for (int i = 0; i < n; i++) {
+        int k = k0 + i;
+        for (int off = -H; off <= H; off++) {
+            e[k + off] = 1.0;
+            L[(size_t) i * (2 * H + 1) + off + H] = is_w ? helmholtz_w_at(m, e.data(), k, nudt)
+                                                         : helmholtz_u_at(m, e.data(), k, nudt);
+            e[k + off] = 0.0;
+        }
+    }
+    return L;
+}
+
 std::vector<double> fused_rows(const Metrics& m, const ImplicitSet& s, bool is_w, double nuadt,
                                double gamdt, double zetdt)
 {
     const int H = m.order == 2 ? 1 : 3;
     const int W = fused_width(m.order);
     const int k0 = s.fac.k0, n = s.fac.n;
-    std::vector<double> L((size_t) n * (2 * H + 1), 0.0);
-    // The operator is linear: its coefficients are its response to unit columns.
-    std::vector<double> e(m.n2, 0.0);
-    for (int i = 0; i < n; i++) {
-        int k = k0 + i;
-        for (int off = -H; off <= H; off++) {
-            e[k + off] = 1.0;
-            L[(size_t) i * (2 * H + 1) + off + H] = is_w ? helmholtz_w_at(m, e.data(), k, nuadt)
-                                                         : helmholtz_u_at(m, e.data(), k, nuadt);
-            e[k + off] = 0.0;
-        }
-    }
+    const std::vector<double> L = operator_coefs(m, k0, n, is_w, nuadt);
     std::vector<double> rows((size_t) n * W, 0.0);
     for (int i = 0; i < n; i++) {
         int k = k0 + i;
@@ -748,6 +769,117 @@ std::vector<double> fused_rows(const Metrics& m, const ImplicitSet& s, bool is_w
         r[2 * H + 6] = s.fac.F3[i] * iden;
     }
     return rows;
+}
+
+std::vector<double> channel_rows(const Metrics& m, const ImplicitSet& s, bool is_w, double nuadt,
+                                 double gamdt, double zetdt)
+{
+    const int H = m.order == 2 ? 1 : 3;
+    const int W = fused_width(m.order);
+    const int k0 = s.fac.k0, n = s.fac.n;
+    const std::vector<double> L = operator_coefs(m, k0, n, is_w, nuadt);
+    std::vector<double> rows((size_t) n * W, 0.0);
+    for (int i = 0; i < n; i++) {
+        double* r = &rows[(size_t) i * W];
+        for (int t = 0; t < 2 * H + 1; t++) r[t] = L[(size_t) i * (2 * H + 1) + t];
+        r[2 * H + 1] = gamdt;
+        r[2 * H + 2] = zetdt;
+        r[2 * H + 3] = -s.hbc[k0 + i];
+    }
+    return rows;
+}
+
+// Modified wavenumbers of the x-y second difference, the same for the
+// pressure Poisson and the spectral Helmholtz solves (pressure.c:312-315,
+// 376-389; diffuseu.c:426-429, 547-560).
+static void modified_wavenumbers(const Metrics& m, PoissonSet& P)
+{
+    auto lam = [&](int n, int i) {
+        double c1 = std::cos(2.0 * M_PI * 1.0 * (double) i / (double) n);
+        if (m.order == 2) return 2.0 - 2.0 * c1;
+        double c2 = std::cos(2.0 * M_PI * 2.0 * (double) i / (double) n);
+        double c3 = std::cos(2.0 * M_PI * 3.0 * (double) i / (double) n);
+        return (2.0 * A2 * A2 + 2.0 * A1 * A1) + (4.0 * A1 * A2 - 2.0 * A1 * A1) * c1
+               + (-4.0 * A1 * A2) * c2 + (-2.0 * A2 * A2) * c3;
+    };
+    P.lamx.resize(m.nx / 2 + 1);
+    for (int i = 0; i <= m.nx / 2; i++) P.lamx[i] = lam(m.nx, i);
+    P.lamy.resize(m.ny);
+    for (int j = 0; j < m.ny; j++) P.lamy[j] = lam(m.ny, j);
+}
+
+PoissonSet make_helmholtz_spectral(const Metrics& m, double nudt, bool is_w)
+{
+    PoissonSet P;
+    P.width = m.order == 2 ? 3 : 7;
+    const auto& dz = m.dz;
+    const int n2 = m.n2, g = m.gz;
+    const int n = is_w ? m.nz - 1 : m.nz;
+    const int kb = g - 1, kt = g + n;   // wall ghost row / face below and above the rows
+    const double area = m.dx * m.dy;
+    Band B(n2);
+    if (is_w) band_rows_w(m, B, nudt, area);
+    else band_rows_u(m, B, nudt, area);
+    P.dpart.assign(n2, 0.0);
+    P.dvol.assign(n2, 0.0);
+    for (int k = g; k < g + n; k++) {
+        // column-independent part of the diagonal; the wavenumber terms are
+        // cx = dvol nudt / dx^2, cy = dvol nudt / dy^2 (added on the device)
+        P.dvol[k] = area * (is_w ? 0.5 * (dz[k + 1] + dz[k]) : dz[k]);
+        double& dg = m.order == 2 ? B.b[k] : B.d[k];
+        P.dpart[k] = dg;
+        dg = 0.0;
+    }
+    double ds_b[3][3] = {{0}}, ds_t[3][3] = {{0}};
+    if (m.order == 2) {
+        if (is_w) { w_stencil2(B, kb, 0.0); w_stencil2(B, kt, 0.0); }
+        else { u_stencil_bot2(B, dz, kb, 0.0, BC_DIRICHLET); u_stencil_top2(B, dz, kt, 0.0, BC_DIRICHLET); }
+        P.bot[0] = rows_of(B, kb, -1);
+        P.top = rows_of(B, kt, +1);
+        // ghost_reduce_{bot,top}2: the diagonal of the first / last row loses c[kb]*fac / a[kt]*fac
+        double fac = B.a[kb + 1] / B.b[kb];
+        B.a[kb + 1] -= B.b[kb] * fac;
+        ds_b[0][0] = B.c[kb] * fac;
+        double fact = B.c[kt - 1] / B.b[kt];
+        B.c[kt - 1] -= B.b[kt] * fact;
+        ds_t[0][0] = B.a[kt] * fact;
+    } else if (is_w) {
+        w_stencil_bot4(B, dz, kb, 0.0);
+        w_stencil_top4(B, dz, kt, 0.0);
+        P.bot[0] = rows_of(B, kb, -1);
+        P.top = rows_of(B, kt, +1);
+        w_reduce_bot4(B, kb, ds_b);
+        w_reduce_top4(B, kt, ds_t);
+    } else {
+        u_stencil_bot4(B, dz, kb, 0.0, BC_DIRICHLET);
+        u_stencil_top4(B, dz, kt, 0.0, BC_DIRICHLET);
+        P.bot[0] = rows_of(B, kb, -1);
+        P.top = rows_of(B, kt, +1);
+        u_reduce_bot4(B, kb, ds_b);
+        u_reduce_top4(B, kt, ds_t);
+    }
+    P.bot[1] = P.bot[0];
+    const int rows[6] = {g, g + 1, g + 2, g + n - 3, g + n - 2, g + n - 1};
+    for (int q = 0; q < 6; q++) {
+        int k = rows[q];
+        const double vals[7] = {B.a[k], B.b[k], B.c[k], B.d[k], B.e[k], B.f[k], B.g[k]};
+        for (int t = 0; t < 7; t++) P.red[0][q][t] = vals[t];
+        for (int t = 0; t < 3; t++) P.dsub[0][q][t] = 0.0;
+    }
+    for (int t = 0; t < 3; t++) P.dsub[0][0][t] = ds_b[0][t];
+    P.dsub[0][1][0] = ds_b[1][0];
+    for (int t = 0; t < 3; t++) P.dsub[0][5][t] = ds_t[0][t];
+    P.dsub[0][4][0] = ds_t[1][0];
+    std::memcpy(P.red[1], P.red[0], sizeof(P.red[0]));
+    std::memcpy(P.dsub[1], P.dsub[0], sizeof(P.dsub[0]));
+    P.a.assign(n2, 0.0); P.b.assign(n2, 0.0); P.c.assign(n2, 0.0);
+    P.e.assign(n2, 0.0); P.f.assign(n2, 0.0); P.g.assign(n2, 0.0);
+    for (int k = g; k < g + n; k++) {
+        P.a[k] = B.a[k]; P.b[k] = B.b[k]; P.c[k] = B.c[k];
+        P.e[k] = B.e[k]; P.f[k] = B.f[k]; P.g[k] = B.g[k];
+    }
+    modified_wavenumbers(m, P);
+    return P;
 }
 
 PoissonSet make_poisson(const Metrics& m, double dt)
@@ -832,18 +964,7 @@ PoissonSet make_poisson(const Metrics& m, double dt)
         }
     }
     (void) nz;
-    auto lam = [&](int n, int i) {
-        double c1 = std::cos(2.0 * M_PI * 1.0 * (double) i / (double) n);
-        if (m.order == 2) return 2.0 - 2.0 * c1;
-        double c2 = std::cos(2.0 * M_PI * 2.0 * (double) i / (double) n);
-        double c3 = std::cos(2.0 * M_PI * 3.0 * (double) i / (double) n);
-        return (2.0 * A2 * A2 + 2.0 * A1 * A1) + (4.0 * A1 * A2 - 2.0 * A1 * A1) * c1
-               + (-4.0 * A1 * A2) * c2 + (-2.0 * A2 * A2) * c3;
-    };
-    P.lamx.resize(m.nx / 2 + 1);
-    for (int i = 0; i <= m.nx / 2; i++) P.lamx[i] = lam(m.nx, i);
-    P.lamy.resize(m.ny);
-    for (int j = 0; j < m.ny; j++) P.lamy[j] = lam(m.ny, j);
+    modified_wavenumbers(m, P);
     return P;
 }
 

@@ -102,6 +102,14 @@ std::vector<double> fused_rows(const Metrics& m, const ImplicitSet& s, bool is_w
                                double gamdt, double zetdt);
 inline int fused_width(int order) { return (order == 2 ? 3 : 7) + 6; }
 
+// Per-row coefficients of the channel scheme's Helmholtz right-hand side
+// (channel.c:455-467 and its v, c, w counterparts), z part:
+//   h_k = sum_m cu_m x_{k+m} + cf f_k + cg g_k + c0
+// = x + nuadt d2x/dz2 + gamdt f + zetdt g - hbc; the device adds
+// nuadt (d2/dx2 + d2/dy2) x.  Same row layout as fused_rows, f1..f3 = 0.
+std::vector<double> channel_rows(const Metrics& m, const ImplicitSet& s, bool is_w, double nuadt,
+                                 double gamdt, double zetdt);
+
 // Solve one column with an ImplicitSet factorisation (host reference of the
 // device kernel; used for the Green's function and for tests).
 void solve_column(const ImplicitSet& s, const Metrics& m, bool is_w, std::vector<double>& rhs_h,
@@ -124,6 +132,13 @@ struct PoissonSet {
     std::vector<double> lamx, lamy;  // modified wavenumbers (pressure.c:312-315 / 376-389)
 };
 PoissonSet make_poisson(const Metrics& m, double dt);
+
+// Per-wavenumber band of solve_helmholtz_{u,w}{2,4} (diffuseu.c:398-614,
+// diffusew.c:466-614) with Dirichlet walls and zero wall values, in the same
+// form: rows GZ .. GZ+n-1 (n = nz for cell-centred fields, nz - 1 for w),
+// diagonal dpart - lamx cx - lamy cy with cx = dvol nudt / dx^2 applied on
+// the device, both closure variants equal (no special mean mode).
+PoissonSet make_helmholtz_spectral(const Metrics& m, double nudt, bool is_w);
 
 // Bulk statistics of an xy-averaged profile (chanfast.c:485-509):
 // out = {z-average, kappa*d/dz at bottom, at top, centreline}.

@@ -306,6 +306,7 @@ struct cf_instance {
     double* partial = nullptr;     // per-warp row sums of the u solve
     double* partial_c = nullptr;   // and of the c solve
     double* avg = nullptr;
+    double* avg_c = nullptr;        // channel scheme: xy-average of c (avg holds u's)
     double* dscal = nullptr;        // [0] mdpdx, [1] dcdt
     long long* dcount = nullptr;    // device substep counter (log row)
     double* dlog = nullptr;
@@ -321,6 +322,7 @@ struct cf_instance {
     double c8 = 0.0;
     // per substep s (0..2): sets for u, v, c, w and the Poisson solve
     SetOffsets set[3][4];
+    PoissonOffsets hspec[3][3];     // channel scheme: spectral Helmholtz sets of u and v, c, w
     PoissonOffsets pois[3];
     PoissonOffsets pois_init;
     WallRowsD bc_ub, bc_ut, bc_wb, bc_wt;
@@ -343,6 +345,12 @@ int check_config(const cf_config* c)
     if (fft_radices(c->nx).empty() || fft_radices(c->ny).empty()) return CF_EINVAL;
     if (!(c->dt > 0.0) || !(c->nu >= 0.0) || !(c->prandtl > 0.0)) return CF_EINVAL;
     if (!(c->lx > 0.0) || !(c->ly > 0.0) || !(c->lz > 0.0)) return CF_EINVAL;
+    if (c->scheme != CF_SCHEME_CHANFAST && c->scheme != CF_SCHEME_CHANNEL) return CF_EINVAL;
+    // the fully implicit scheme batches its x transforms with the
+    // power-of-two kernels; its fourth-order w solve has nz - 1 rows, of
+    // which the three next to each wall carry the closure (nz >= 8)
+    if (c->scheme == CF_SCHEME_CHANNEL && (!fftx_batched_supported(c->nx) || (c->order == 4 && c->nz < 8)))
+        return CF_EINVAL;
     return CF_OK;
 }
 
@@ -352,9 +360,11 @@ int build_tables(cf_instance* I, double dt)
     const cf_config& C = I->cfg;
     const Metrics& m = I->m;
     Arena A;
+    const bool channel = C.scheme == CF_SCHEME_CHANNEL;
     auto addfac = [&](SetOffsets& so, const ImplicitSet& s, bool is_w, double nuadt, double gamdt,
                       double zetdt) {
-        so.rows = A.add(fused_rows(m, s, is_w, nuadt, gamdt, zetdt));
+        so.rows = A.add(channel ? channel_rows(m, s, is_w, nuadt, gamdt, zetdt)
+                                : fused_rows(m, s, is_w, nuadt, gamdt, zetdt));
         so.k0 = s.fac.k0;
         so.n = s.fac.n;
         so.F1 = A.add(s.fac.F1); so.F2 = A.add(s.fac.F2); so.F3 = A.add(s.fac.F3);
@@ -400,6 +410,27 @@ int build_tables(cf_instance* I, double dt)
     };
     for (int s = 0; s < 3; s++) addpois(I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt);
     addpois(I->pois_init, 1.0);
+    if (channel) {
+        // spectral Helmholtz sets with nudt = -nubdt (channel.c:471-478, 547-552, 576-581, 652-657)
+        auto addspec = [&](PoissonOffsets& po, double nudt, bool is_w) {
+            po.host = make_helmholtz_spectral(m, nudt, is_w);
+            po.a = A.add(po.host.a); po.b = A.add(po.host.b); po.c = A.add(po.host.c);
+            po.e = A.add(po.host.e); po.f = A.add(po.host.f); po.g = A.add(po.host.g);
+            po.dpart = A.add(po.host.dpart); po.dvol = A.add(po.host.dvol);
+            std::vector<double> cx(po.host.dvol.size()), cy(po.host.dvol.size());
+            for (size_t k = 0; k < cx.size(); k++) {
+                cx[k] = po.host.dvol[k] * nudt / (m.dx * m.dx);
+                cy[k] = po.host.dvol[k] * nudt / (m.dy * m.dy);
+            }
+            po.cx = A.add(cx); po.cy = A.add(cy);
+        };
+        for (int s = 0; s < 3; s++) {
+            double nubdt = C.nu * RK3_BET[s] * dt;
+            addspec(I->hspec[s][0], -nubdt, false);
+            addspec(I->hspec[s][1], -nubdt / C.prandtl, false);
+            addspec(I->hspec[s][2], -nubdt, true);
+        }
+    }
     size_t o_lamx = A.add(I->pois_init.host.lamx);
     size_t o_lamy = A.add(I->pois_init.host.lamy);
     // metrics
@@ -476,6 +507,10 @@ PoissonArgs poisson_args(cf_instance* I, const PoissonOffsets& po, double pdt)
     A.dt = pdt;
     A.dxdx = I->m.dx * I->m.dx;
     A.dydy = I->m.dy * I->m.dy;
+    A.nrows = I->cfg.nz;
+    A.avg = nullptr;
+    A.abot = A.atop = WallRowsD{};
+    A.abc_bot = A.abc_top = 0.0;
     return A;
 }
 
@@ -511,8 +546,8 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     FftyArgs Yb{I->spec, I->py, +1, 0, I->c8};
     launch_ffty(G, Yb, G.n2, st);
     if (tl) tl->mark(st);
-    C2rArgs X{I->spec, I->p, I->px, I->c8};
-    launch_fftx_c2r(G, X, st);
+    C2rArgs X{I->spec, {I->p, nullptr, nullptr, nullptr}, I->px, I->c8, 0, 0};
+    launch_fftx_c2r(G, X, G.n2, st);
     if (tl) tl->mark(st);
     ProjArgs P;
     P.u = I->u; P.v = I->v; P.w = I->w; P.c = I->c; P.p = I->p;
@@ -527,6 +562,82 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     if (tl) tl->mark(st);
 }
 
+// Mass-flux (u, q = 0) or scalar-mean (c, q = 2) control of substep set s
+// from the xy-average profile in `avg` (chanfast.c:485-529, 572-616).
+MassArgs mass_args(cf_instance* I, int s, int q, const double* avg)
+{
+    const cf_config& C = I->cfg;
+    const SetOffsets& so = I->set[s][q];
+    MassArgs M;
+    M.avg = avg;
+    M.dz = I->geo.dz;
+    M.order = C.order;
+    M.nz = C.nz;
+    M.n2 = I->geo.n2;
+    M.kappa = q == 0 ? C.nu : C.nu / C.prandtl;
+    std::memcpy(M.green, so.gstats, sizeof(M.green));
+    M.mode = q == 0 ? C.uvolavgmode : C.cvolavgmode;
+    M.target = q == 0 ? C.want_uvolavg - C.setuframe : C.want_cvolavg;
+    M.fixed = q == 0 ? -C.dpdx : 0.0;
+    M.m_out = I->dscal + (q == 0 ? 0 : 1);
+    M.counter = I->dcount;
+    M.log_base = I->dlog;
+    M.log_cap = I->log_cap;
+    M.col = q == 0 ? 0 : 5;
+    M.advance = q == 2 ? 1 : 0;
+    return M;
+}
+
+// The implicit half of a channel-scheme substep (channel.c:455-657 and
+// :1405-1607): k_rhs has left h in the g buffers (slots u, v, w, c, one
+// contiguous block); transform the four fields, solve per wavenumber, and
+// transform back into u, v, w, c; then apply_bc and the two controls.
+void enqueue_implicit3d(cf_instance* I, int s, Timeline* tl)
+{
+    const cf_config& C = I->cfg;
+    const Geo& G = I->geo;
+    cudaStream_t st = I->stream;
+    const long long fstride = G.plane * G.n2;      // between the g buffers
+    const long long sstride = G.splane * G.n2;     // between the four spectra
+    R2cArgs X{I->gbuf[0], I->spec, I->px, I->c8, GZ, fstride, sstride};
+    launch_fftx_r2c(G, X, G.nz, 4, st);
+    FftyArgs Y{I->spec, I->py, -1, GZ, I->c8, sstride};
+    launch_ffty(G, Y, G.nz, st, 4);
+    // slot order u, v, w, c; sets u/v 0, c 1, w 2
+    const int set_of_slot[4] = {0, 0, 2, 1};
+    for (int f = 0; f < 4; f++) {
+        PoissonArgs H = poisson_args(I, I->hspec[s][set_of_slot[f]], 0.0);
+        H.spec = I->spec + f * sstride;
+        H.nrows = f == 2 ? C.nz - 1 : C.nz;
+        if (f == 0 || f == 3) {   // u, c: the xy-average profile for the controls
+            H.avg = f == 0 ? I->avg : I->avg_c;
+            H.abot = I->bc_ub;
+            H.atop = I->bc_ut;
+            H.abc_bot = f == 0 ? 0.0 - C.setuframe : -0.5;
+            H.abc_top = f == 0 ? 0.0 - C.setuframe : +0.5;
+        }
+        launch_helmholtz_spectral(G, H, st);
+    }
+    FftyArgs Yb{I->spec, I->py, +1, GZ, I->c8, sstride};
+    launch_ffty(G, Yb, G.nz, st, 4);
+    C2rArgs Xb{I->spec, {I->u, I->v, I->w, I->c}, I->px, I->c8, GZ, sstride};
+    launch_fftx_c2r(G, Xb, G.nz, st, 4);
+    GhostArgs GA;
+    GA.F = Fields{I->u, I->v, I->w, I->c};
+    GA.ub = I->bc_ub; GA.ut = I->bc_ut; GA.wb = I->bc_wb; GA.wt = I->bc_wt;
+    GA.bc_u = 0.0 - C.setuframe;
+    GA.bc_v = 0.0 - C.setvframe;
+    GA.bc_c_bot = -0.5;
+    GA.bc_c_top = +0.5;
+    GA.bc_w = 0.0;
+    launch_ghosts(G, GA, st, false);
+    if (tl) tl->mark(st);
+    launch_mass_control(mass_args(I, s, 0, I->avg), st);
+    if (tl) tl->mark(st);
+    launch_mass_control(mass_args(I, s, 2, I->avg_c), st);
+    if (tl) tl->mark(st);
+}
+
 void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
 {
     const cf_config& C = I->cfg;
@@ -534,6 +645,7 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     cudaStream_t st = I->stream;
     const int s = (int) (I->substep % 3);
     const double dt = C.dt;
+    const bool channel = C.scheme == CF_SCHEME_CHANNEL;
     for (int q = 0; q < 4; q++) std::swap(I->fbuf[q], I->gbuf[q]);   // chanfast.c:397-402
 
     GhostArgs GA;
@@ -550,8 +662,12 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
 
     // RHS + forward sweeps; set index of each f slot (u, v, w, c) among the
     // implicit-solve sets (u, v, c, w)
+    // chanfast: x-y diffusion explicit in f with nu; channel: implicit, in
+    // h with nu alpha dt (channel.c:450-458)
+    const double nuadt = C.nu * RK3_ALP[s] * dt;
     RhsArgs R{I->u, I->v, I->w, I->c, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
-              C.nu, C.nu / C.prandtl, C.betg_x, C.betg_y, C.betg_z};
+              channel ? nuadt : C.nu, channel ? nuadt / C.prandtl : C.nu / C.prandtl,
+              C.betg_x, C.betg_y, C.betg_z};
     const int set_of_slot[4] = {0, 1, 3, 2};
     for (int f = 0; f < 4; f++) {
         R.sw[f].g = I->gbuf[f];
@@ -563,8 +679,14 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     R.wtop = I->bc_wt;
     R.wbc_bot = 0.0;
     R.wbc_top = 0.0;
-    launch_rhs(G, R, st);
+    launch_rhs(G, R, channel, st);
     if (tl) tl->mark(st);
+    if (channel) {
+        enqueue_implicit3d(I, s, tl);
+        pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, tl);
+        I->substep++;
+        return;
+    }
 
     double* fields[4] = {I->u, I->v, I->c, I->w};
     const int fidx[4] = {0, 1, 3, 2};   // u, v, c, w -> f/g slots (u, v, w, c)
@@ -588,28 +710,8 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     launch_back4(G, SB, st);
     if (tl) tl->mark(st);
     for (int q = 0; q < 4; q += 2) {   // mass-flux control (u), scalar-mean control (c)
-        const SetOffsets& so = I->set[s][q];
-        {
-            MassArgs M;
-            M.avg = I->avg;
-            M.dz = G.dz;
-            M.order = C.order;
-            M.nz = C.nz;
-            M.n2 = G.n2;
-            M.kappa = q == 0 ? C.nu : C.nu / C.prandtl;
-            std::memcpy(M.green, so.gstats, sizeof(M.green));
-            M.mode = q == 0 ? C.uvolavgmode : C.cvolavgmode;
-            M.target = q == 0 ? C.want_uvolavg - C.setuframe : C.want_cvolavg;
-            M.fixed = q == 0 ? -C.dpdx : 0.0;
-            M.m_out = I->dscal + (q == 0 ? 0 : 1);
-            M.counter = I->dcount;
-            M.log_base = I->dlog;
-            M.log_cap = I->log_cap;
-            M.col = q == 0 ? 0 : 5;
-            M.advance = q == 2 ? 1 : 0;
-            launch_mass(G, partial[q], I->avg, M, st);
-            if (tl) tl->mark(st);
-        }
+        launch_mass(G, partial[q], I->avg, mass_args(I, s, q, I->avg), st);
+        if (tl) tl->mark(st);
     }
     pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, tl);
     I->substep++;
@@ -644,9 +746,10 @@ int cf_destroy(cf_instance* I)
     if (I->stream) cudaStreamSynchronize(I->stream);
     if (I->gexec) cudaGraphExecDestroy(I->gexec);
     if (I->graph) cudaGraphDestroy(I->graph);
-    void* bufs[] = {I->u, I->v, I->w, I->c, I->p, I->fbuf[0], I->fbuf[1], I->fbuf[2], I->fbuf[3],
-                    I->gbuf[0], I->gbuf[1], I->gbuf[2], I->gbuf[3], I->spec, I->scratch, I->partial, I->partial_c,
-                    I->avg, I->dscal, I->dcount, I->dlog, I->staging, I->coef, I->twx, I->twy};
+    // fbuf[0] and gbuf[0] are the bases of the two four-field blocks
+    void* bufs[] = {I->u, I->v, I->w, I->c, I->p, I->fbuf[0], I->gbuf[0], I->spec, I->scratch, I->partial,
+                    I->partial_c, I->avg, I->avg_c, I->dscal, I->dcount, I->dlog, I->staging, I->coef, I->twx,
+                    I->twy};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (I->own_stream && I->stream) cudaStreamDestroy(I->stream);
@@ -682,20 +785,29 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
         I->own_stream = true;
     }
     const size_t fb = (size_t) G.plane * G.n2 * sizeof(double);
-    double** fl[] = {&I->u, &I->v, &I->w, &I->c, &I->p, &I->fbuf[0], &I->fbuf[1], &I->fbuf[2], &I->fbuf[3],
-                     &I->gbuf[0], &I->gbuf[1], &I->gbuf[2], &I->gbuf[3]};
+    double** fl[] = {&I->u, &I->v, &I->w, &I->c, &I->p};
     for (double** pp : fl) {
         CF_CUDA(cudaMalloc(pp, fb));
         CF_CUDA(cudaMemsetAsync(*pp, 0, fb, I->stream));
     }
-    CF_CUDA(cudaMalloc(&I->spec, (size_t) G.splane * G.n2 * sizeof(double2)));
-    CF_CUDA(cudaMemsetAsync(I->spec, 0, (size_t) G.splane * G.n2 * sizeof(double2), I->stream));
+    // the previous- and current-stage right-hand sides of u, v, w, c: two
+    // blocks of four consecutive fields (the channel scheme transforms a
+    // block in one batched launch)
+    for (double** blk : {I->fbuf, I->gbuf}) {
+        CF_CUDA(cudaMalloc(&blk[0], 4 * fb));
+        CF_CUDA(cudaMemsetAsync(blk[0], 0, 4 * fb, I->stream));
+        for (int q = 1; q < 4; q++) blk[q] = blk[0] + q * G.plane * G.n2;
+    }
+    const size_t nspec = (C.scheme == CF_SCHEME_CHANNEL ? 4 : 1) * (size_t) G.splane * G.n2;
+    CF_CUDA(cudaMalloc(&I->spec, nspec * sizeof(double2)));
+    CF_CUDA(cudaMemsetAsync(I->spec, 0, nspec * sizeof(double2), I->stream));
     const int nscr = C.order == 4 ? 3 : 1;
     CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
     const long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);   // per-warp partial sums of k_back4
     CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->partial_c, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->avg, (size_t) G.n2 * sizeof(double)));
+    CF_CUDA(cudaMalloc(&I->avg_c, (size_t) G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->dscal, 8 * sizeof(double)));
     CF_CUDA(cudaMemsetAsync(I->dscal, 0, 8 * sizeof(double), I->stream));
     CF_CUDA(cudaMalloc(&I->dcount, sizeof(long long)));
@@ -1028,12 +1140,14 @@ int cf_profile(cf_instance* I, int nsub, double* ms)
 
 int cf_launches_per_substep(const cf_instance* I)
 {
-    // ghosts, rhs + forward sweeps, the four back substitutions, 2 x (row average + mass control),
-    // div+fftx (two launches for power-of-two nx), ffty, poisson, ffty,
-    // fftx_c2r, project
+    // pressure: div+fftx (two launches for power-of-two nx), ffty, poisson,
+    // ffty, fftx_c2r, project.  chanfast: ghosts, rhs + forward sweeps, the
+    // four back substitutions, 2 x (row average + mass control).  channel
+    // (power-of-two nx only): ghosts, rhs + Helmholtz right-hand sides, fftx,
+    // ffty, four spectral solves, ffty, fftx_c2r, apply_bc, 2 x mass control.
     if (!I) return CF_EINVAL;
-    const int nx = I->cfg.nx;
-    return nx == 64 || nx == 128 || nx == 256 || nx == 512 ? 14 : 13;
+    const int pressure = fftx_batched_supported(I->cfg.nx) ? 7 : 6;
+    return (I->cfg.scheme == CF_SCHEME_CHANNEL ? 13 : 7) + pressure;
 }
 
 }  // extern "C"

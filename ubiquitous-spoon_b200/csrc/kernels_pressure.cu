@@ -18,6 +18,7 @@
 // transform over L lines of one thread block, twiddles from a host table.
 #include "engine.cuh"
 #include "host_band.h"
+#include "wall.cuh"
 
 namespace cf {
 
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
     const int kx0 = blockIdx.x * FFT_L;
     const int ny = G.ny, nkx = G.nkx;
     const int nl = min(FFT_L, nkx - kx0);
-    double2* base = A.spec + ((long long) k * nkx + kx0) * ny;
+    double2* base = A.spec + blockIdx.z * A.fstride + ((long long) k * nkx + kx0) * ny;
     for (int idx = threadIdx.x; idx < FFT_L * ny; idx += blockDim.x) {
         int line = idx / ny;
         sbuf[idx] = line < nl ? base[idx] : make_double2(0.0, 0.0);
@@ -245,18 +246,19 @@ __global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
 __global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
 {
     extern __shared__ double2 sbuf[];
-    const int k = blockIdx.y;
+    const int k = A.kfirst + blockIdx.y;
     const int j0 = blockIdx.x * FFT_L;
     const int nx = G.nx, ny = G.ny, nkx = G.nkx;
+    const double2* spec = A.spec + blockIdx.z * A.fstride;
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int pos = idx / FFT_L, jj = idx - pos * FFT_L, j = j0 + jj;
         double2 t = make_double2(0.0, 0.0);
         if (j < ny) {
             if (pos < nkx) {
-                t = A.spec[((long long) k * nkx + pos) * ny + j];
+                t = spec[((long long) k * nkx + pos) * ny + j];
                 if (pos == 0 || 2 * pos == nx) t.y = 0.0;
             } else {
-                t = A.spec[((long long) k * nkx + (nx - pos)) * ny + j];
+                t = spec[((long long) k * nkx + (nx - pos)) * ny + j];
                 t.y = -t.y;
             }
         }
@@ -267,7 +269,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
     fft_run<FFT_MAXC>(F, A.px);
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
-        if (j < ny) A.p[((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
+        if (j < ny) A.p[blockIdx.z][((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
     }
 }
 
@@ -317,19 +319,48 @@ __device__ __forceinline__ void fill_top(const WallRowsD& R, double x0, double x
     }
 }
 
+// xy-average profile of a Helmholtz solution from its (kx, ky) = (0, 0)
+// column: rows GZ .. GZ+n-1 already hold the solved values; the wall ghost
+// rows follow from the field's apply_bc closure, which is affine with
+// column-independent coefficients and so commutes with the average.  This is
+// get_xy_avg (get.c:281-302) of the field after apply_bc (channel.c:480-486),
+// rows the closure does not write being zero as they are there.
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs A)
+__device__ void average_walls(const PoissonArgs& A, int n2)
+{
+    double* avg = A.avg;
+    const int kb = GZ - 1, kt = GZ + A.nrows;
+    double g1, g2, g3;
+    bc_u_bot<ORDER>(A.abot, A.abc_bot, avg[kb + 1], avg[kb + 2], avg[kb + 3], g1, g2, g3);
+    for (int k = 0; k < GZ; k++) avg[k] = 0.0;
+    avg[kb] = g1;
+    if (ORDER == 4) { avg[kb - 1] = g2; avg[kb - 2] = g3; }
+    bc_u_top<ORDER>(A.atop, A.abc_top, avg[kt - 1], avg[kt - 2], avg[kt - 3], g1, g2, g3);
+    for (int k = kt; k < n2; k++) avg[k] = 0.0;
+    avg[kt] = g1;
+    if (ORDER == 4) { avg[kt + 1] = g2; avg[kt + 2] = g3; }
+}
+
+// Banded solve of one (kx, ky) column over spectrum rows GZ .. GZ+n-1:
+// pressure_poisson{2,4} (pressure.c:293-443) with FILL (the wall ghost rows
+// of the solution are filled from the closure, as p needs them), or
+// solve_helmholtz_{u,w}{2,4} (diffuseu.c:398-614, diffusew.c:466-614) without
+// (the field's apply_bc follows the inverse transform).  One thread per
+// column, Re and Im sharing one factorisation.
+template <int ORDER, bool FILL>
+__device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A)
 {
     const long long ncol = G.splane;
     const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
-    const int ny = G.ny, n2 = G.n2, nz = G.nz;
+    const int ny = G.ny, n2 = G.n2, n = A.nrows;
     const int kx = (int) (col / ny), ky = (int) (col - (long long) kx * ny);
     const int var = (kx == 0 && ky == 0) ? 1 : 0;   // pressure.c:331-338
     const double lamx = A.lamx[kx], lamy = A.lamy[ky];
+    const bool stats = !FILL && A.avg != nullptr && col == 0;
     double2* sp = A.spec;
     auto S = [&](int k) -> double2& { return sp[(long long) k * ncol + col]; };
-    auto bq = [&](int i) { return i < 3 ? i : (i >= nz - 3 ? 6 - (nz - i) : -1); };
+    auto bq = [&](int i) { return i < 3 ? i : (i >= n - 3 ? 6 - (n - i) : -1); };
 
     // Coefficients of interior row i (k = GZ + i) for this column.
     auto coef = [&](int i, double* cf) {
@@ -347,7 +378,7 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
     };
 
     if (ORDER == 2) {
-        // tridag.c:4-26; the diagonal is cf[1] for the 3-band rows
+        // tridag.c:4-26; the diagonal is cf[3], the off-diagonals cf[0], cf[2]
         double* gam = A.scratch;
         double cfv[7];
         coef(0, cfv);
@@ -357,7 +388,7 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
         double2 u = make_double2(r0.x * dv0 * ibet, r0.y * dv0 * ibet);
         S(GZ) = u;
         double cprev = cfv[2];
-        for (int i = 1; i < nz; i++) {
+        for (int i = 1; i < n; i++) {
             const int k = GZ + i;
             coef(i, cfv);
             double gm = cprev * ibet;
@@ -370,9 +401,10 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
             cprev = cfv[2];
         }
         double2 nxt = u;
-        double2 top1 = u, top2 = u, top3 = u;
-        double2 b0 = u, b1v = u, b2v = u;
-        for (int i = nz - 2; i >= 0; i--) {
+        double2 top1 = u;
+        double2 b0 = u;
+        if (stats) A.avg[GZ + n - 1] = u.x;
+        for (int i = n - 2; i >= 0; i--) {
             const int k = GZ + i;
             double gm = gam[(long long) (k + 1) * ncol + col];
             double2 t = S(k);
@@ -380,23 +412,25 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
             t.y -= gm * nxt.y;
             S(k) = t;
             nxt = t;
-            if (i == nz - 2) top2 = t;
-            if (i == 1) b1v = t;
+            if (stats) A.avg[k] = t.x;
             if (i == 0) b0 = t;
         }
-        (void) top3; (void) b2v;
-        if (nz == 1) b0 = top1;
-        double g1, g2, g3;
-        fill_bot<2>(A.bot[var], b0.x, 0.0, 0.0, g1, g2, g3);
-        double h1;
-        fill_bot<2>(A.bot[var], b0.y, 0.0, 0.0, h1, g2, g3);
-        S(GZ - 1) = make_double2(g1, h1);
-        fill_top<2>(A.top, top1.x, 0.0, 0.0, g1, g2, g3);
-        fill_top<2>(A.top, top1.y, 0.0, 0.0, h1, g2, g3);
-        S(n2 - GZ) = make_double2(g1, h1);
-        for (int k = 0; k < GZ - 1; k++) S(k) = make_double2(0.0, 0.0);
-        for (int k = n2 - GZ + 1; k < n2; k++) S(k) = make_double2(0.0, 0.0);
-        (void) b1v; (void) top2;
+        if (n == 1) b0 = top1;
+        if (FILL) {
+            double g1, g2, g3;
+            fill_bot<2>(A.bot[var], b0.x, 0.0, 0.0, g1, g2, g3);
+            double h1;
+            fill_bot<2>(A.bot[var], b0.y, 0.0, 0.0, h1, g2, g3);
+            S(GZ - 1) = make_double2(g1, h1);
+            fill_top<2>(A.top, top1.x, 0.0, 0.0, g1, g2, g3);
+            fill_top<2>(A.top, top1.y, 0.0, 0.0, h1, g2, g3);
+            S(n2 - GZ) = make_double2(g1, h1);
+            for (int k = 0; k < GZ - 1; k++) S(k) = make_double2(0.0, 0.0);
+            for (int k = n2 - GZ + 1; k < n2; k++) S(k) = make_double2(0.0, 0.0);
+        } else {
+            if (GZ + n < n2 - GZ) S(GZ + n) = make_double2(0.0, 0.0);   // w: the top wall face
+            if (stats) average_walls<2>(A, n2);
+        }
         return;
     }
 
@@ -414,14 +448,14 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
     const int t = threadIdx.x;
     auto fslot = [&](int i) { return pring + (i % POIS_PF) * POIS_THREADS + t; };
     auto ffetch = [&](int i) {
-        if (i < nz) cp_async16_ordered(fslot(i), &S(GZ + i));
+        if (i < n) cp_async16_ordered(fslot(i), &S(GZ + i));
         cp_async_commit_ordered();
     };
     for (int i = 0; i < POIS_PF; i++) ffetch(i);
     double p3 = 0, q3 = 0, r3 = 0, p2 = 0, q2 = 0, r2 = 0, p1 = 0, q1 = 0, r1 = 0;   // rows i-3, i-2, i-1
     double2 s3 = make_double2(0, 0), s2 = s3, s1 = s3;
     double cf[7];
-    for (int i = 0; i < nz; i++) {
+    for (int i = 0; i < n; i++) {
         const int k = GZ + i;
         cp_async_wait_ordered<POIS_PF - 1>();
         double2 h = *fslot(i);
@@ -459,9 +493,10 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
         }
     };
 #pragma unroll
-    for (int u = 0; u < POIS_PB; u++) bload(nz - 2 - u, u);
-    double2 x1 = S(GZ + nz - 1), x2 = make_double2(0, 0), x3 = x2;
-    for (int i0 = nz - 2; i0 >= 0; i0 -= POIS_PB) {
+    for (int u = 0; u < POIS_PB; u++) bload(n - 2 - u, u);
+    double2 x1 = S(GZ + n - 1), x2 = make_double2(0, 0), x3 = x2;
+    if (stats) A.avg[GZ + n - 1] = x1.x;
+    for (int i0 = n - 2; i0 >= 0; i0 -= POIS_PB) {
 #pragma unroll
         for (int u = 0; u < POIS_PB; u++) {
             const int i = i0 - u;
@@ -472,17 +507,23 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
                 const double2 xv = make_double2(sv.x - p * x1.x - q * x2.x - r * x3.x,
                                                 sv.y - p * x1.y - q * x2.y - r * x3.y);
                 S(GZ + i) = xv;
+                if (stats) A.avg[GZ + i] = xv.x;
                 x3 = x2; x2 = x1; x1 = xv;
             }
         }
     }
+    if (!FILL) {
+        if (GZ + n < n2 - GZ) S(GZ + n) = make_double2(0.0, 0.0);   // w: the top wall face
+        if (stats) average_walls<4>(A, n2);
+        return;
+    }
     // wall rows of the solution: bottom rows 0..2 are the last three results,
-    // top rows nz-1..nz-3 are read back
+    // top rows n-1..n-3 are read back
     double2 bt[3] = {x1, x2, x3};
-    if (nz < 3)
-        for (int i = 0; i < 3; i++) bt[i] = i < nz ? S(GZ + i) : make_double2(0.0, 0.0);
+    if (n < 3)
+        for (int i = 0; i < 3; i++) bt[i] = i < n ? S(GZ + i) : make_double2(0.0, 0.0);
     double2 tp[3];
-    for (int i = 0; i < 3; i++) tp[i] = nz - 1 - i >= 0 ? S(GZ + nz - 1 - i) : make_double2(0.0, 0.0);
+    for (int i = 0; i < 3; i++) tp[i] = n - 1 - i >= 0 ? S(GZ + n - 1 - i) : make_double2(0.0, 0.0);
     double g1, g2, g3, h1, h2, h3;
     fill_bot<4>(A.bot[var], bt[0].x, bt[1].x, bt[2].x, g1, g2, g3);
     fill_bot<4>(A.bot[var], bt[0].y, bt[1].y, bt[2].y, h1, h2, h3);
@@ -494,6 +535,18 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs 
     S(n2 - GZ) = make_double2(g1, h1);
     S(n2 - GZ + 1) = make_double2(g2, h2);
     S(n2 - GZ + 2) = make_double2(g3, h3);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs A)
+{
+    band_column<ORDER, true>(G, A);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(POIS_THREADS, 7) k_helmholtz_spectral(Geo G, PoissonArgs A)
+{
+    band_column<ORDER, false>(G, A);
 }
 
 // ------------------------------------------------------------ projection
@@ -729,16 +782,16 @@ __global__ void __launch_bounds__(DV_I * DV_J) k_div(Geo G, DivArgs A)
 // A line is M = N/2 points, 8 per thread; 256 / (M/8) lines of consecutive j
 // per block.
 template <int N>
-__global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, DivArgs A)
+__global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, R2cArgs A)
 {
     extern __shared__ double2 sbuf[];
     constexpr int M = N / 2, T = M / 8, L = p2_lines(M);
     const int l = threadIdx.x % L, t = threadIdx.x / L;
-    const int k = GZ + blockIdx.y;
+    const int k = A.kfirst + blockIdx.y;
     const int j = blockIdx.x * L + l;
     const bool valid = j < G.ny;
     const int ny = G.ny;
-    const double* row = A.dv + (long long) k * G.nx * ny + (valid ? j : 0);
+    const double* row = A.src + blockIdx.z * A.src_fstride + (long long) k * G.nx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -754,7 +807,7 @@ __global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, DivArgs A)
     __syncthreads();
     if (!valid) return;
     const double scale = 1.0 / (double) N;
-    double2* out = A.spec + (long long) k * G.nkx * ny + j;
+    double2* out = A.spec + blockIdx.z * A.spec_fstride + (long long) k * G.nkx * ny + j;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int kx = t + q * T;
@@ -782,7 +835,7 @@ __global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
     const int kx = blockIdx.x * L + l;
     const int nkx = G.nkx;
     const bool valid = kx < nkx;
-    double2* base = A.spec + ((long long) k * nkx + (valid ? kx : 0)) * N;
+    double2* base = A.spec + blockIdx.z * A.fstride + ((long long) k * nkx + (valid ? kx : 0)) * N;
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) v[q] = valid ? base[t + q * T] : make_double2(0.0, 0.0);
@@ -808,11 +861,11 @@ __global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
     extern __shared__ double2 sbuf[];
     constexpr int M = N / 2, T = M / 8, L = p2_lines(M);
     const int l = threadIdx.x % L, t = threadIdx.x / L;
-    const int k = blockIdx.y;
+    const int k = A.kfirst + blockIdx.y;
     const int j = blockIdx.x * L + l;
     const bool valid = j < G.ny;
     const int ny = G.ny;
-    const double2* base = A.spec + (long long) k * G.nkx * ny + (valid ? j : 0);
+    const double2* base = A.spec + blockIdx.z * A.fstride + (long long) k * G.nkx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -828,7 +881,7 @@ __global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
     }
     fft_p2_line<M>(v, t, sbuf + l * p2_stride_x(M), A.px.tw, +1, A.c8, 2);
     if (!valid) return;
-    double* out = A.p + (long long) k * G.nx * ny + j;
+    double* out = A.p[blockIdx.z] + (long long) k * G.nx * ny + j;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int m = t + q * T;
@@ -843,28 +896,35 @@ template <int N>
 static size_t p2_smem_y() { return (size_t) p2_lines(N) * p2_pad(N) * sizeof(double2); }
 
 template <int N>
+static void launch_r2c_p2(const Geo& G, const R2cArgs& A, int nrows, int nfields, cudaStream_t st)
+{
+    constexpr int L = p2_lines(N / 2);
+    k_fftx_r2c_p2<N><<<dim3((G.ny + L - 1) / L, nrows, nfields), 256, p2_smem_x<N / 2>(), st>>>(G, A);
+}
+
+template <int N>
 static void launch_div_fftx_p2(const Geo& G, const DivArgs& A, cudaStream_t st)
 {
     dim3 blk(DV_J, DV_I, 1), grd((G.ny + DV_J - 1) / DV_J, (G.nx + DV_I - 1) / DV_I, (G.nz + DV_KC - 1) / DV_KC);
     if (G.order == 2) k_div<2><<<grd, blk, 0, st>>>(G, A);
     else k_div<4><<<grd, blk, 0, st>>>(G, A);
-    constexpr int L = p2_lines(N / 2);
-    k_fftx_r2c_p2<N><<<dim3((G.ny + L - 1) / L, G.nz), 256, p2_smem_x<N / 2>(), st>>>(G, A);
+    R2cArgs R{A.dv, A.spec, A.px, A.c8, GZ, 0, 0};
+    launch_r2c_p2<N>(G, R, G.nz, 1, st);
 }
 
 template <int N>
-static void launch_ffty_p2(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st)
+static void launch_ffty_p2(const Geo& G, const FftyArgs& A, int nrows, int nfields, cudaStream_t st)
 {
     constexpr int L = p2_lines(N);
-    dim3 grd((G.nkx + L - 1) / L, nrows);
+    dim3 grd((G.nkx + L - 1) / L, nrows, nfields);
     k_ffty_p2<N><<<grd, 256, p2_smem_y<N>(), st>>>(G, A);
 }
 
 template <int N>
-static void launch_c2r_p2(const Geo& G, const C2rArgs& A, cudaStream_t st)
+static void launch_c2r_p2(const Geo& G, const C2rArgs& A, int nrows, int nfields, cudaStream_t st)
 {
     constexpr int L = p2_lines(N / 2);
-    dim3 grd((G.ny + L - 1) / L, G.n2);
+    dim3 grd((G.ny + L - 1) / L, nrows, nfields);
     k_fftx_c2r_p2<N><<<grd, 256, p2_smem_x<N / 2>(), st>>>(G, A);
 }
 
@@ -896,29 +956,45 @@ void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st)
     else k_div_fftx<4><<<grd, FFT_THREADS, sm, st>>>(G, A);
 }
 
-void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st)
+bool fftx_batched_supported(int nx)
 {
-    switch (G.ny) {
-    case 64: return launch_ffty_p2<64>(G, A, nrows, st);
-    case 128: return launch_ffty_p2<128>(G, A, nrows, st);
-    case 256: return launch_ffty_p2<256>(G, A, nrows, st);
-    case 512: return launch_ffty_p2<512>(G, A, nrows, st);
+    return nx == 64 || nx == 128 || nx == 256 || nx == 512;
+}
+
+void launch_fftx_r2c(const Geo& G, const R2cArgs& A, int nrows, int nfields, cudaStream_t st)
+{
+    switch (G.nx) {   // power-of-two nx only (fftx_batched_supported)
+    case 64: return launch_r2c_p2<64>(G, A, nrows, nfields, st);
+    case 128: return launch_r2c_p2<128>(G, A, nrows, nfields, st);
+    case 256: return launch_r2c_p2<256>(G, A, nrows, nfields, st);
+    case 512: return launch_r2c_p2<512>(G, A, nrows, nfields, st);
     default: break;
     }
-    dim3 grd((G.nkx + FFT_L - 1) / FFT_L, nrows);
+}
+
+void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st, int nfields)
+{
+    switch (G.ny) {
+    case 64: return launch_ffty_p2<64>(G, A, nrows, nfields, st);
+    case 128: return launch_ffty_p2<128>(G, A, nrows, nfields, st);
+    case 256: return launch_ffty_p2<256>(G, A, nrows, nfields, st);
+    case 512: return launch_ffty_p2<512>(G, A, nrows, nfields, st);
+    default: break;
+    }
+    dim3 grd((G.nkx + FFT_L - 1) / FFT_L, nrows, nfields);
     k_ffty<<<grd, FFT_THREADS, fft_smem_bytes(G.ny), st>>>(G, A);
 }
 
-void launch_fftx_c2r(const Geo& G, const C2rArgs& A, cudaStream_t st)
+void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st, int nfields)
 {
     switch (G.nx) {
-    case 64: return launch_c2r_p2<64>(G, A, st);
-    case 128: return launch_c2r_p2<128>(G, A, st);
-    case 256: return launch_c2r_p2<256>(G, A, st);
-    case 512: return launch_c2r_p2<512>(G, A, st);
+    case 64: return launch_c2r_p2<64>(G, A, nrows, nfields, st);
+    case 128: return launch_c2r_p2<128>(G, A, nrows, nfields, st);
+    case 256: return launch_c2r_p2<256>(G, A, nrows, nfields, st);
+    case 512: return launch_c2r_p2<512>(G, A, nrows, nfields, st);
     default: break;
     }
-    dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.n2);
+    dim3 grd((G.ny + FFT_L - 1) / FFT_L, nrows, nfields);
     k_fftx_c2r<<<grd, FFT_THREADS, fft_smem_bytes(G.nx), st>>>(G, A);
 }
 
@@ -927,6 +1003,13 @@ void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
     unsigned nb = (unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS);
     if (G.order == 2) k_poisson<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
     else k_poisson<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
+}
+
+void launch_helmholtz_spectral(const Geo& G, const PoissonArgs& A, cudaStream_t st)
+{
+    unsigned nb = (unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS);
+    if (G.order == 2) k_helmholtz_spectral<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
+    else k_helmholtz_spectral<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
 }
 
 void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st)

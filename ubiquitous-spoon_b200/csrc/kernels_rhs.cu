@@ -12,6 +12,7 @@
 //            agree with the reference to rounding.
 #include "engine.cuh"
 #include "host_band.h"
+#include "wall.cuh"
 
 #include <type_traits>
 
@@ -22,72 +23,10 @@ __device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >
 
 // ------------------------------------------------------------------ ghosts
 
-template <int ORDER>
-__device__ __forceinline__ void bc_u_bot(const WallRowsD& R, double bc, double x0, double x1, double x2,
-                                         double& g1, double& g2, double& g3)
-{
-    // ghost_fill_bot{2,4} (diffuseu.c:687-693, 899-918): rows k = gz-1, k-1, k-2
-    if (ORDER == 2) {
-        g1 = (R.row[0][2] * x0 - bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (R.row[2][6] * x0) / -R.row[2][5];
-        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0 + R.row[1][6] * x1 - bc) / -R.row[1][3];
-        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1
-              + R.row[0][6] * x2) / -R.row[0][1];
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ void bc_u_top(const WallRowsD& R, double bc, double x0, double x1, double x2,
-                                         double& g1, double& g2, double& g3)
-{
-    // ghost_fill_top{2,4} (diffuseu.c:696-702, 921-940); x0 = x[kt-1], x1 = x[kt-2], x2 = x[kt-3]
-    if (ORDER == 2) {
-        g1 = (R.row[0][0] * x0 - bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (R.row[2][0] * x0) / -R.row[2][1];
-        g2 = (R.row[1][0] * x1 + R.row[1][1] * x0 + R.row[1][2] * g1 - bc) / -R.row[1][3];
-        g3 = (R.row[0][0] * x2 + R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1
-              + R.row[0][4] * g2) / -R.row[0][5];
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ void bc_w_bot(const WallRowsD& R, double bc, double x0, double x1,
-                                         double& g1, double& g2, double& g3)
-{
-    // diffusew.c:667-680 (order 2), 849-865 (order 4); x0 = w[gz], x1 = w[gz+1]
-    if (ORDER == 2) {
-        g1 = (-bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (-bc) / -R.row[2][5];
-        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0) / -R.row[1][3];
-        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1) / -R.row[0][1];
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ void bc_w_top(const WallRowsD& R, double bc, double x0, double x1,
-                                         double& g1, double& g2, double& g3)
-{
-    // x0 = w[kt-1], x1 = w[kt-2] with kt = n2-gz-1 the top wall face
-    if (ORDER == 2) {
-        g1 = (-bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (-bc) / -R.row[2][1];
-        g2 = (R.row[1][1] * x0 + R.row[1][2] * g1) / -R.row[1][3];
-        g3 = (R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1 + R.row[0][4] * g2) / -R.row[0][5];
-    }
-}
-
-
 // One thread per column: wall ghost rows of u, v, c (apply_bc_u) and w
-// (apply_bc_w, then the massflux4 extrapolation of advect.c:100-131).
-template <int ORDER>
+// (apply_bc_w, then with EXTRAP the massflux4 extrapolation of
+// advect.c:100-131).
+template <int ORDER, bool EXTRAP>
 __global__ void k_ghosts(Geo G, GhostArgs A)
 {
     long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
@@ -116,12 +55,17 @@ __global__ void k_ghosts(Geo G, GhostArgs A)
     bc_w_top<ORDER>(A.wt, A.bc_w, at(w, wt - 1), at(w, wt - 2), top1, top2, top3);
     at(w, kb) = g1;
     at(w, wt) = top1;
-    if (ORDER == 4) {
+    if (ORDER == 4 && EXTRAP) {
         // massflux4 wall extrapolation (advect.c:108-109, 124-125)
         at(w, kb - 1) = 2.0 * g1 - at(w, kb + 1);
         at(w, kb - 2) = 2.0 * g1 - at(w, kb + 2);
         at(w, wt + 1) = 2.0 * top1 - at(w, wt - 1);
         at(w, wt + 2) = 2.0 * top1 - at(w, wt - 2);
+    } else if (ORDER == 4) {
+        at(w, kb - 1) = g2;
+        at(w, kb - 2) = g3;
+        at(w, wt + 1) = top2;
+        at(w, wt + 2) = top3;
     }
     (void) g2; (void) g3; (void) top2; (void) top3;
 }
@@ -141,6 +85,13 @@ __global__ void k_ghosts(Geo G, GhostArgs A)
 // forward half of tridag/heptdag): the old field window x_{k-H..k+H} is in
 // the ring, f was just computed, g is read and overwritten by s.  The back
 // substitution follows in k_back4 (kernels_solve.cu).
+//
+// IMPL3D (the fully implicit scheme of channel.c): f has no x-y diffusion
+// (channel.c:419-438), and in place of the sweep row each thread forms the
+// Helmholtz right-hand side h = x + nuadt (Lxy + Lz) x + gamdt f + zetdt g
+// - hbc (channel.c:455-467, 531-543, 560-572, 636-648) of its point, which
+// overwrites g; A.nu and A.kappa then carry nuadt and nuadt / prandtl.  The
+// spectral solves follow (kernels_pressure.cu).
 
 constexpr int RT_I = 8, RT_J = 32, RT_H = 3, RT_SLOTS = 8;
 constexpr int RT_PI = RT_I + 2 * RT_H, RT_PJ = RT_J + 2 * RT_H;   // 14 x 38
@@ -204,7 +155,7 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int ORDER>
+template <int ORDER, bool IMPL3D>
 __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
 {
     extern __shared__ double sm[];
@@ -341,11 +292,12 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     double gb0, gb1, gb2, gt0 = 0.0, gt1 = 0.0, gt2 = 0.0;
     bc_w_bot<ORDER>(A.wbot, A.wbc_bot, W(0, 0, 0), W(0, 0, 1), gb0, gb1, gb2);
     (void) gb0;
-    auto sweep = [&](int f, auto X, double fk, double gk, double& s1, double& s2, double& s3) {
+    auto sweep = [&](int f, auto X, double fk, double gk, double lk, double& s1, double& s2, double& s3) {
         const double* r = cst + ((k & 1) * 4 + f) * RT_FWMAX;   // staged coefficient row
         double sk = r[2 * H + 3] + r[2 * H + 1] * fk + r[2 * H + 2] * gk;
 #pragma unroll
         for (int q = 0; q < 2 * H + 1; q++) sk += r[q] * X(q - H);
+        if (IMPL3D) return sk + lk;   // h of this point (channel_rows: no elimination)
         sk -= r[2 * H + 4] * s1;
         if (ORDER == 4) sk -= r[2 * H + 5] * s2 + r[2 * H + 6] * s3;
         s3 = s2; s2 = s1; s1 = sk;
@@ -364,6 +316,7 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
         const double gu = gk[0] + shift_u, gv = gk[RT_THREADS];
         const double gw = gk[2 * RT_THREADS], gc = gk[3 * RT_THREADS] + shift_c;
         double fu, fv, fw = 0.0, fc;
+        double lu, lv, lw = 0.0, lc;   // x-y diffusion terms
 
         if (ORDER == 2) {
             auto adv_cell = [&](auto Q, auto MX, auto MY, auto MZ) {   // advectu2 / advectv2 (advect.c:286-417)
@@ -398,10 +351,10 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
                 return nu * (((F(1, 0, 0) - q0) * idx - (q0 - F(-1, 0, 0)) * idx) * idx
                              + ((F(0, 1, 0) - q0) * idy - (q0 - F(0, -1, 0)) * idy) * idy);
             };
-            fu += lap2(U, A.nu);
-            fv += lap2(V, A.nu);
-            if (do_w) fw += lap2(W, A.nu);
-            fc = lap2(C, A.kappa);
+            lu = lap2(U, A.nu);
+            lv = lap2(V, A.nu);
+            if (do_w) lw = lap2(W, A.nu);
+            lc = lap2(C, A.kappa);
         } else {
             // advectu4 / advectv4 / advectw4 (advect.c:466-734).  Within one
             // cell every x-direction mass flux carries the same metric
@@ -491,11 +444,17 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
                                 + L1 * ((F(0, 1, 0) - q0) + (F(0, -1, 0) - q0));
                 return nu * (lx * idx2 + ly * idy2);
             };
-            fu += lap4(U, A.nu);
-            fv += lap4(V, A.nu);
-            if (do_w) fw += lap4(W, A.nu);
-            fc = lap4(C, A.kappa);
+            lu = lap4(U, A.nu);
+            lv = lap4(V, A.nu);
+            if (do_w) lw = lap4(W, A.nu);
+            lc = lap4(C, A.kappa);
         }
+        if (!IMPL3D) {
+            fu += lu;
+            fv += lv;
+            fw += lw;
+        }
+        fc = IMPL3D ? 0.0 : lc;
 
         {   // flux_quick + advect_scalar (scalar.c:79-162), order independent
             double c0 = C(0, 0, 0);
@@ -534,10 +493,10 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
             return W(0, 0, dk);
         };
         (void) gt0;
-        const double s_u = sweep(0, [&](int dk) { return U(0, 0, dk); }, fu, gu, su1, su2, su3);
-        const double s_v = sweep(1, [&](int dk) { return V(0, 0, dk); }, fv, gv, sv1, sv2, sv3);
-        const double s_w = do_w ? sweep(2, XW, fw, gw, sw1, sw2, sw3) : 0.0;
-        const double s_c = sweep(3, [&](int dk) { return C(0, 0, dk); }, fc, gc, sc1, sc2, sc3);
+        const double s_u = sweep(0, [&](int dk) { return U(0, 0, dk); }, fu, gu, lu, su1, su2, su3);
+        const double s_v = sweep(1, [&](int dk) { return V(0, 0, dk); }, fv, gv, lv, sv1, sv2, sv3);
+        const double s_w = do_w ? sweep(2, XW, fw, gw, lw, sw1, sw2, sw3) : 0.0;
+        const double s_c = sweep(3, [&](int dk) { return C(0, 0, dk); }, fc, gc, lc, sc1, sc2, sc3);
         if (out) {
             A.fu[ijk] = fu;
             A.fv[ijk] = fv;
@@ -565,28 +524,40 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
 
 // ------------------------------------------------------------- launchers
 
-void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st)
+void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st, bool extrap)
 {
     int th = 256;
     long long nb = (G.plane + th - 1) / th;
-    if (G.order == 2) k_ghosts<2><<<(unsigned) nb, th, 0, st>>>(G, A);
-    else k_ghosts<4><<<(unsigned) nb, th, 0, st>>>(G, A);
+    if (extrap) {
+        if (G.order == 2) k_ghosts<2, true><<<(unsigned) nb, th, 0, st>>>(G, A);
+        else k_ghosts<4, true><<<(unsigned) nb, th, 0, st>>>(G, A);
+    } else {
+        if (G.order == 2) k_ghosts<2, false><<<(unsigned) nb, th, 0, st>>>(G, A);
+        else k_ghosts<4, false><<<(unsigned) nb, th, 0, st>>>(G, A);
+    }
 }
 
-void launch_rhs(const Geo& G, const RhsArgs& A, cudaStream_t st)
+void launch_rhs(const Geo& G, const RhsArgs& A, bool implicit3d, cudaStream_t st)
 {
     dim3 blk(RT_J, RT_I, 1);
     dim3 grd((G.ny + RT_J - 1) / RT_J, (G.nx + RT_I - 1) / RT_I, 1);
     size_t sm = rhs_smem_bytes();
-    if (G.order == 2) k_rhs<2><<<grd, blk, sm, st>>>(G, A);
-    else k_rhs<4><<<grd, blk, sm, st>>>(G, A);
+    if (implicit3d) {
+        if (G.order == 2) k_rhs<2, true><<<grd, blk, sm, st>>>(G, A);
+        else k_rhs<4, true><<<grd, blk, sm, st>>>(G, A);
+    } else {
+        if (G.order == 2) k_rhs<2, false><<<grd, blk, sm, st>>>(G, A);
+        else k_rhs<4, false><<<grd, blk, sm, st>>>(G, A);
+    }
 }
 
 cudaError_t rhs_set_smem_limits()
 {
     int v = (int) rhs_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_rhs<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaError_t e = cudaFuncSetAttribute(k_rhs<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     return e;
 }
 

@@ -16,66 +16,9 @@
 // of get_xy_avg, get.c:281-302).
 #include "engine.cuh"
 #include "host_band.h"
+#include "wall.cuh"
 
 namespace cf {
-
-template <int ORDER>
-__device__ __forceinline__ void bcu_bot(const WallRowsD& R, double bc, double x0, double x1, double x2,
-                                        double& g1, double& g2, double& g3)
-{
-    if (ORDER == 2) {
-        g1 = (R.row[0][2] * x0 - bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (R.row[2][6] * x0) / -R.row[2][5];
-        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0 + R.row[1][6] * x1 - bc) / -R.row[1][3];
-        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1
-              + R.row[0][6] * x2) / -R.row[0][1];
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ void bcu_top(const WallRowsD& R, double bc, double x0, double x1, double x2,
-                                        double& g1, double& g2, double& g3)
-{
-    if (ORDER == 2) {
-        g1 = (R.row[0][0] * x0 - bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (R.row[2][0] * x0) / -R.row[2][1];
-        g2 = (R.row[1][0] * x1 + R.row[1][1] * x0 + R.row[1][2] * g1 - bc) / -R.row[1][3];
-        g3 = (R.row[0][0] * x2 + R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1
-              + R.row[0][4] * g2) / -R.row[0][5];
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ void bcw_bot(const WallRowsD& R, double bc, double x0, double x1,
-                                        double& g1, double& g2, double& g3)
-{
-    if (ORDER == 2) {
-        g1 = (-bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (-bc) / -R.row[2][5];
-        g2 = (R.row[1][4] * g1 + R.row[1][5] * x0) / -R.row[1][3];
-        g3 = (R.row[0][2] * g2 + R.row[0][3] * g1 + R.row[0][4] * x0 + R.row[0][5] * x1) / -R.row[0][1];
-    }
-}
-
-template <int ORDER>
-__device__ __forceinline__ void bcw_top(const WallRowsD& R, double bc, double x0, double x1,
-                                        double& g1, double& g2, double& g3)
-{
-    if (ORDER == 2) {
-        g1 = (-bc) / -R.row[0][1];
-        g2 = g3 = 0.0;
-    } else {
-        g1 = (-bc) / -R.row[2][1];
-        g2 = (R.row[1][1] * x0 + R.row[1][2] * g1) / -R.row[1][3];
-        g3 = (R.row[0][1] * x1 + R.row[0][2] * x0 + R.row[0][3] * g1 + R.row[0][4] * g2) / -R.row[0][5];
-    }
-}
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -141,11 +84,11 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A)
     // apply_bc after the solve (chanfast.c:481-482)
     double b1, b2, b3, t1, t2, t3;
     if (IS_W) {
-        bcw_bot<ORDER>(A.bcb, A.bc_bot, bot0, bot1, b1, b2, b3);
-        bcw_top<ORDER>(A.bct, A.bc_top, top0, top1, t1, t2, t3);
+        bc_w_bot<ORDER>(A.bcb, A.bc_bot, bot0, bot1, b1, b2, b3);
+        bc_w_top<ORDER>(A.bct, A.bc_top, top0, top1, t1, t2, t3);
     } else {
-        bcu_bot<ORDER>(A.bcb, A.bc_bot, bot0, bot1, bot2, b1, b2, b3);
-        bcu_top<ORDER>(A.bct, A.bc_top, top0, top1, top2, t1, t2, t3);
+        bc_u_bot<ORDER>(A.bcb, A.bc_bot, bot0, bot1, bot2, b1, b2, b3);
+        bc_u_top<ORDER>(A.bct, A.bc_top, top0, top1, top2, t1, t2, t3);
     }
     if (active) {
         x[(long long) kb * P + col] = b1;
@@ -258,6 +201,11 @@ void launch_mass(const Geo& G, const double* partial, double* avg, const MassArg
     long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);
     double scale = 1.0 / ((double) G.nx * (double) G.ny);
     k_row_average<<<G.n2, 256, 0, st>>>(partial, nwarps, G.n2, scale, avg);
+    k_mass_control<<<1, 32, 0, st>>>(M);
+}
+
+void launch_mass_control(const MassArgs& M, cudaStream_t st)
+{
     k_mass_control<<<1, 32, 0, st>>>(M);
 }
 
