@@ -52,9 +52,17 @@ WORKLOADS = {
     "config0": dict(name="chanfast2 64x64x64 Re_b=2800", order=2, nx=64, ny=64, nz=64,
                     lx=4 * math.pi, ly=4 * math.pi / 3, lz=2.0, dt=1e-3, nu=1.0 / 2800.0, prandtl=1.0,
                     seed=0, amp=0.1, c_amp=0.0, run_steps=100),
+    # the fully implicit scheme (channel4) on the headline grid
+    "channel4": dict(name="channel4 512x512x384 Re_b=20000", order=4, nx=512, ny=512, nz=384,
+                     lx=2 * math.pi, ly=math.pi, lz=2.0, dt=2.5e-4, nu=1.0 / 20000.0, prandtl=0.71,
+                     seed=2, amp=0.05, c_amp=0.01, run_steps=20, scheme="channel", b_alg=496.0),
 }
 WORKLOAD = WORKLOADS["config2"]
 B_ALG = 240.0            # algorithmic HBM bytes per point-substep (whole substep)
+# The fully implicit scheme adds, per field, the x and y transforms there and
+# back and the spectral solve over the half spectrum (8 B/pt each way per
+# pass: 5 passes x 16 B x 4 fields) and drops the back substitution (64 B):
+# 240 + 320 - 64 = 496 B/pt (the workload's "b_alg").
 METRIC = "FP64 Mpt-substeps/s"
 # Minimal bytes per interior point of each kernel group (own inputs + outputs):
 # rhs = RHS + forward sweeps (read u,v,w,c,g x4; write f x4, s x4), solve = back
@@ -144,10 +152,11 @@ def _ref_worker(args):
     for nm, a in zip("uvwc", (u, v, wf, c)):
         R.set(nm, a)
     R.project(1.0)
+    scheme = w.get("scheme", "chanfast")
     if warm:
-        R.substeps(warm)
+        R.substeps(warm, scheme)
     t0 = time.perf_counter()
-    R.substeps(nsub)
+    R.substeps(nsub, scheme)
     dt = time.perf_counter() - t0
     R.close()
     return dt
@@ -170,7 +179,8 @@ def cpu_reference(nsub, warm, nproc=None):
         times = pool.map(_ref_worker, [(wname, nx, ny, nsub, warm, 100 + r) for r in range(nproc)])
     pts = nx * ny * WORKLOAD["nz"]
     value = sum(pts * nsub / t for t in times) / 1e6
-    sample = (f"unmodified reference chanfast{WORKLOAD['order']} substep (oracle/_ref, single-rank MPI/FFTW shims, "
+    sample = (f"unmodified reference {WORKLOAD.get('scheme', 'chanfast')}{WORKLOAD['order']} substep "
+              f"(oracle/_ref, single-rank MPI/FFTW shims, "
               f"gcc -O3 -funroll-loops) on {nproc} independent {nx}x{ny}x{WORKLOAD['nz']} instances, "
               f"{nsub} timed substeps each after {warm} warm-up")
     return value, nproc, sample, max(times)
@@ -209,7 +219,9 @@ def run_ours(args):
     cf = importlib.import_module("ubiquitous-spoon_b200")
     w = WORKLOAD
     cfg = cf.Config.make(order=w["order"], nx=w["nx"], ny=w["ny"], nz=w["nz"], lx=w["lx"], ly=w["ly"],
-                         lz=w["lz"], dt=w["dt"], nu=w["nu"], prandtl=w["prandtl"])
+                         lz=w["lz"], dt=w["dt"], nu=w["nu"], prandtl=w["prandtl"],
+                         scheme=w.get("scheme", "chanfast"))
+    b_alg = w.get("b_alg", B_ALG)
     stream = torch.cuda.Stream()
     inst = cf.Instance(cfg, stream=ctypes_stream(stream))
     inst.init_fields(w["seed"] + rank, w["amp"], w["c_amp"])
@@ -246,22 +258,22 @@ def run_ours(args):
     kernels = {}
     for name, t in prof.items():
         t1 = t / 3.0
-        nb = KERNEL_BYTES.get(name)
+        nb = KERNEL_BYTES.get(name) if "scheme" not in w else None
         gbs = nb * pts / (t1 * 1e-3) / 1e9 if nb and t1 > 0 else None
         kernels[name] = {"ms": round(t1, 4), "alg_bytes_per_pt": nb,
                          "gbs": round(gbs, 1) if gbs else None,
                          "frac": round(gbs / peak, 3) if gbs else None}
     substep_ms = ms_per_step / 3.0
-    achieved = B_ALG * pts / (substep_ms * 1e-3) / 1e9
+    achieved = b_alg * pts / (substep_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_per_substep.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and "scheme" not in w:   # measured for the headline workload
         with open(tpath) as f:
             traffic = json.load(f).get("dram_bytes_per_substep_full_size")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "kernel": f"whole RK3 substep (CUDA graph of {inst.launches_per_substep()} launches)",
-                "alg_bytes_per_unit": B_ALG, "unit_desc": "interior point-substep",
+                "alg_bytes_per_unit": b_alg, "unit_desc": "interior point-substep",
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "kernels": kernels, "profiled_substep_ms": round(sub_ms, 4)}
 
