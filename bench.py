@@ -336,6 +336,92 @@ def run_ours(args):
         print(json.dumps(result), flush=True)
 
 
+# ------------------------------------------------------------- ensemble
+
+ENSEMBLE_GRIDS = [(64, 64, 64), (96, 96, 64), (128, 128, 96), (192, 192, 128)]   # (nx, ny, nz)
+
+
+def ensemble_members(n=64):
+    """The 64-instance ensemble: per seed s a grid from ENSEMBLE_GRIDS and
+    Re_b ~ U[2800, 10000], order 2, box 4pi x 4pi/3 x 2, dt 1e-3."""
+    import numpy as np
+    out = []
+    for s in range(n):
+        rng = np.random.default_rng(s)
+        nx, ny, nz = ENSEMBLE_GRIDS[int(rng.integers(len(ENSEMBLE_GRIDS)))]
+        out.append(dict(seed=s, nx=nx, ny=ny, nz=nz, re=float(rng.uniform(2800.0, 10000.0))))
+    return out
+
+
+def run_ensemble(args):
+    """Solves/hour of the ensemble batched (cf_batch: one launch per stage
+    for all 64 instances, replayed as a CUDA graph) against the same
+    instances one after another through the plain path (cf_step_graph), both
+    on device time; a solve is 500 RK3 steps, timed over args.steps."""
+    import torch
+    cf = importlib.import_module("ubiquitous-spoon_b200")
+    torch.cuda.set_device(0)
+    members = ensemble_members()
+
+    def create():
+        insts = []
+        for m in members:
+            cfg = cf.Config.make(order=2, nx=m["nx"], ny=m["ny"], nz=m["nz"], lx=4 * math.pi,
+                                 ly=4 * math.pi / 3, lz=2.0, dt=1e-3, nu=1.0 / m["re"], prandtl=1.0)
+            inst = cf.Instance(cfg)
+            inst.init_fields(m["seed"], 0.1, 0.0)
+            insts.append(inst)
+        for inst in insts:
+            inst.sync()
+        return insts
+
+    pts = sum(m["nx"] * m["ny"] * m["nz"] for m in members)
+    # batched
+    insts = create()
+    B = cf.Batch(insts)
+    B.run(args.warmup)
+    B.sync()
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        B.run(args.steps)
+        B.sync()
+        t_batch = time.perf_counter() - t0
+    launches = B.launches_per_substep()
+    div = max(inst.max_divergence() for inst in insts)
+    B.close()
+    for inst in insts:
+        inst.close()
+    # one after another, plain path
+    insts = create()
+    t_seq = 0.0
+    for inst in insts:
+        inst.step_graph(args.warmup)
+        inst.sync()
+        t0 = time.perf_counter()
+        inst.step_graph(args.steps)
+        inst.sync()
+        t_seq += time.perf_counter() - t0
+        inst.close()
+    solve_steps = 500
+    per_h = lambda t: len(members) / (t * solve_steps / args.steps) * 3600.0
+    result = {
+        "metric": "ensemble solves/h", "value": round(per_h(t_batch), 1), "unit": "solves/h",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "sequential_plain_path": round(per_h(t_seq), 1), "speedup_vs_sequential": round(t_seq / t_batch, 2),
+        "mpt_substeps_per_s": round(pts * 3 * args.steps / t_batch / 1e6, 1),
+        "ms_per_step_all_members": round(t_batch / args.steps * 1e3, 3),
+        "batched_launches_per_substep": launches, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "64-instance ensemble, order 2, grids per seed from "
+                               + ", ".join("x".join(map(str, g)) for g in ENSEMBLE_GRIDS)
+                               + ", Re_b ~ U[2800, 10000], dt 1e-3",
+                   "solve": f"{solve_steps} RK3 steps (timed over {args.steps}, scaled)",
+                   "points": pts, "timing": "wall clock around stream-synchronised runs"},
+        "max_divergence": div, "clocks": clk.summary(),
+    }
+    print(json.dumps(result), flush=True)
+
+
 def ctypes_stream(torch_stream):
     import ctypes
     return ctypes.c_void_p(torch_stream.cuda_stream)
@@ -372,6 +458,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="the 64-instance batched ensemble against running its members one after another")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 (default) is the benchmark; the others serve profiling and checks")
     args = ap.parse_args()
@@ -379,7 +467,9 @@ def main():
     WORKLOAD = WORKLOADS[args.workload]
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
-    if args.impl == "reference":
+    if args.ensemble:
+        run_ensemble(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

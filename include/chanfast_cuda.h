@@ -167,6 +167,34 @@ int cf_launches_per_substep(const cf_instance *inst);
 const char *cf_strerror(int status);
 
 /* ------------------------------------------------------------------------
+ * Batches: many independent instances stepped together, one kernel launch
+ * per stage of the substep covering all of them (per-instance work records
+ * in device memory: geometry, arguments, own grid).  Members may differ in
+ * grid size, order and physical parameters; they must use
+ * CF_SCHEME_CHANFAST and live on one device.  Each member's results are the
+ * same, bit for bit, as stepping it alone with cf_step.
+ *
+ * cf_batch_step: advance every member by nsub substeps on `stream` (NULL:
+ * the first member's stream), recording the launches on the spot.  Ordered
+ * after, and before, work on the members' own streams.
+ *
+ * cf_batch_create / cf_batch_run: record a two-step cycle once (uploaded
+ * per-instance records) and replay it as a CUDA graph for nsteps RK3 steps
+ * (an odd step runs eagerly).  While in a batch, a member must not be stepped
+ * otherwise or have its dt changed; cf_batch_run then returns CF_EINVAL and
+ * the batch must be created again.  Fields, logs and the other cf_* calls of
+ * a member remain available (after cf_batch_sync).
+ * ------------------------------------------------------------------------ */
+typedef struct cf_batch cf_batch;
+int cf_batch_step(cf_instance **members, int n, int nsub, void *stream);
+int cf_batch_create(cf_instance **members, int n, void *stream, cf_batch **out);
+int cf_batch_run(cf_batch *batch, int nsteps);
+int cf_batch_sync(cf_batch *batch);
+/* Batched launches per substep of the whole batch (all members together). */
+int cf_batch_launches_per_substep(const cf_batch *batch);
+int cf_batch_destroy(cf_batch *batch);
+
+/* ------------------------------------------------------------------------
  * Drop-in drivers (libchanfast.so).  Same names and arguments as the
  * reference (chanfast.h:1-21, called at main.c:56-60); they read
  * outputdir/{u,v,w,c}_it<it>.dat, run nt - it time steps on the current

@@ -109,6 +109,13 @@ def _bind(L):
     L.cf_profile.argtypes = [vp, ip, dp]
     L.cf_strerror.restype = ctypes.c_char_p
     L.cf_strerror.argtypes = [ip]
+    pvp = ctypes.POINTER(vp)
+    L.cf_batch_step.argtypes = [pvp, ip, ip, vp]
+    L.cf_batch_create.argtypes = [pvp, ip, vp, pvp]
+    L.cf_batch_run.argtypes = [vp, ip]
+    L.cf_batch_sync.argtypes = [vp]
+    L.cf_batch_launches_per_substep.argtypes = [vp]
+    L.cf_batch_destroy.argtypes = [vp]
     return L
 
 
@@ -255,6 +262,61 @@ class Instance:
 
     def launches_per_substep(self):
         return int(self.L.cf_launches_per_substep(self.h))
+
+
+def _handles(instances):
+    arr = (ctypes.c_void_p * len(instances))()
+    for q, inst in enumerate(instances):
+        arr[q] = inst.h.value
+    return arr
+
+
+def batch_step(instances, nsub, stream=None):
+    """Advance every instance by nsub substeps, one launch per stage of the
+    substep for all of them (cf_batch_step)."""
+    L = lib()
+    _check(L.cf_batch_step(_handles(instances), len(instances), nsub, stream), "cf_batch_step")
+
+
+class Batch:
+    """Instances stepped together by a recorded two-step cycle replayed as
+    one CUDA graph (cf_batch_create / cf_batch_run).  The instances stay
+    usable for fields and logs; they must not be stepped otherwise while in
+    the batch."""
+
+    def __init__(self, instances, stream=None):
+        self.L = lib()
+        self.instances = list(instances)
+        h = ctypes.c_void_p()
+        _check(self.L.cf_batch_create(_handles(self.instances), len(self.instances), stream, ctypes.byref(h)),
+               "cf_batch_create")
+        self.h = h
+
+    def run(self, nsteps):
+        _check(self.L.cf_batch_run(self.h, nsteps), "cf_batch_run")
+
+    def sync(self):
+        _check(self.L.cf_batch_sync(self.h), "cf_batch_sync")
+
+    def launches_per_substep(self):
+        return int(self.L.cf_batch_launches_per_substep(self.h))
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.cf_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def chanfast(order, *args):

@@ -114,6 +114,14 @@ struct MassArgs {
     int advance;          // 1: increment the counter afterwards (last statistics of a substep)
 };
 
+struct RowAvgArgs {
+    const double* partial;   // per-warp row sums [nwarps][n2]
+    long long nwarps;
+    int n2;
+    double scale;            // 1 / (nx ny)
+    double* avg;             // [n2] out
+};
+
 struct DivArgs {
     const double *u, *v, *w;
     const double* gu;      // Green's function column of u (n2) or null
@@ -208,6 +216,33 @@ void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st);
 void launch_helmholtz_spectral(const Geo& G, const PoissonArgs& A, cudaStream_t st);
 void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st);
 cudaError_t fft_set_smem_limits(int max_n);
+
+// ------------------------------------------------- batched launches (batch.cuh)
+struct BatchLaunch;
+dim3 grid_ghosts(const Geo& G);
+dim3 grid_rhs(const Geo& G);
+dim3 grid_back4(const Geo& G);
+dim3 grid_div(const Geo& G);                       // power-of-two nx: divergence
+dim3 grid_r2c(const Geo& G, int nrows, int nfields);
+dim3 grid_div_fftx(const Geo& G);                  // other nx: divergence + x transform
+dim3 grid_ffty(const Geo& G, int nrows, int nfields);
+dim3 grid_poisson(const Geo& G);
+dim3 grid_c2r(const Geo& G, int nrows, int nfields);
+dim3 grid_project(const Geo& G);
+bool batch_pow2(int n);                            // n has a power-of-two transform kernel
+RowAvgArgs row_average_args(const Geo& G, const double* partial, double* avg);
+void launch_ghosts_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_rhs_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_back4_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_row_average_batch(const BatchLaunch& L, cudaStream_t st);
+void launch_mass_control_batch(const BatchLaunch& L, cudaStream_t st);
+void launch_div_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_r2c_batch(const BatchLaunch& L, int nx, cudaStream_t st);
+void launch_div_fftx_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st);   // ny: power of two, else generic
+void launch_poisson_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st);    // nx: power of two, else generic
+void launch_project_batch(const BatchLaunch& L, int order, cudaStream_t st);
 cudaError_t rhs_set_smem_limits();
 size_t fft_smem_bytes(int n);
 constexpr int FFT_MAX_N = 512;

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -18,6 +19,7 @@
 
 #include "chanfast_cuda.h"
 #include "engine.cuh"
+#include "batch.cuh"
 #include "host_band.h"
 
 using namespace cf;
@@ -514,9 +516,6 @@ PoissonArgs poisson_args(cf_instance* I, const PoissonOffsets& po, double pdt)
     return A;
 }
 
-// Divergence -> FFT -> Poisson -> inverse FFT -> projection with step `pdt`.
-// With `corr`, the lazily applied mass-flux corrections of substep set `s`
-// are folded in (divergence and projection read u + G_u * mdpdx, c + G_c * dcdt).
 // Optional per-kernel timing: events recorded after each launch group.
 struct Timeline {
     cudaEvent_t ev[CF_NKERNEL_GROUPS + 1];
@@ -524,31 +523,53 @@ struct Timeline {
     void mark(cudaStream_t st) { cudaEventRecord(ev[n++], st); }
 };
 
-void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr,
-                       Timeline* tl = nullptr);
-void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr,
-                       Timeline* tl)
+// Where the launches of a z-implicit substep go.  The base class launches
+// each stage at once on the instance stream (and marks the timeline between
+// launch groups); the batch (cf_batch below) overrides every stage to record
+// it instead, and later runs each stage of many instances as one launch.
+struct Sink {
+    cudaStream_t st = nullptr;
+    Timeline* tl = nullptr;
+    virtual ~Sink() = default;
+    virtual void mark() { if (tl) tl->mark(st); }
+    virtual void ghosts(const Geo& G, const GhostArgs& A) { launch_ghosts(G, A, st); }
+    virtual void rhs(const Geo& G, const RhsArgs& A) { launch_rhs(G, A, false, st); }
+    virtual void back4(const Geo& G, const SolveBatch& B) { launch_back4(G, B, st); }
+    virtual void mass(const Geo& G, const double* partial, double* avg, const MassArgs& M)
+    {
+        launch_mass(G, partial, avg, M, st);
+    }
+    virtual void div_fftx(const Geo& G, const DivArgs& A) { launch_div_fftx(G, A, st); }
+    virtual void ffty(const Geo& G, const FftyArgs& A, int nrows) { launch_ffty(G, A, nrows, st); }
+    virtual void poisson(const Geo& G, const PoissonArgs& A) { launch_poisson(G, A, st); }
+    virtual void c2r(const Geo& G, const C2rArgs& A, int nrows) { launch_fftx_c2r(G, A, nrows, st); }
+    virtual void project(const Geo& G, const ProjArgs& A) { launch_project(G, A, st); }
+};
+
+// Divergence -> FFT -> Poisson -> inverse FFT -> projection with step `pdt`.
+// With `corr`, the lazily applied mass-flux corrections of substep set `s`
+// are folded in (divergence and projection read u + G_u * mdpdx, c + G_c * dcdt).
+void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr, Sink& K)
 {
     const Geo& G = I->geo;
-    cudaStream_t st = I->stream;
     double* b = I->coef;
     // the divergence field of the power-of-two path lives in p, which the
     // inverse transform below rewrites completely
     DivArgs D{I->u, I->v, I->w, corr ? b + I->set[s][0].green : nullptr, corr ? I->dscal : nullptr,
               I->spec, I->px, I->c8, I->p};
-    launch_div_fftx(G, D, st);
-    if (tl) tl->mark(st);
+    K.div_fftx(G, D);
+    K.mark();
     FftyArgs Y{I->spec, I->py, -1, GZ, I->c8};
-    launch_ffty(G, Y, G.nz, st);
-    if (tl) tl->mark(st);
-    launch_poisson(G, poisson_args(I, po, pdt), st);
-    if (tl) tl->mark(st);
+    K.ffty(G, Y, G.nz);
+    K.mark();
+    K.poisson(G, poisson_args(I, po, pdt));
+    K.mark();
     FftyArgs Yb{I->spec, I->py, +1, 0, I->c8};
-    launch_ffty(G, Yb, G.n2, st);
-    if (tl) tl->mark(st);
+    K.ffty(G, Yb, G.n2);
+    K.mark();
     C2rArgs X{I->spec, {I->p, nullptr, nullptr, nullptr}, I->px, I->c8, 0, 0};
-    launch_fftx_c2r(G, X, G.n2, st);
-    if (tl) tl->mark(st);
+    K.c2r(G, X, G.n2);
+    K.mark();
     ProjArgs P;
     P.u = I->u; P.v = I->v; P.w = I->w; P.c = I->c; P.p = I->p;
     P.gu = corr ? b + I->set[s][0].green : nullptr;
@@ -558,8 +579,17 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     P.dt = pdt;
     P.dtdx = pdt / I->m.dx;
     P.dtdy = pdt / I->m.dy;
-    launch_project(G, P, st);
-    if (tl) tl->mark(st);
+    K.project(G, P);
+    K.mark();
+}
+
+void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int s, bool corr,
+                       Timeline* tl = nullptr)
+{
+    Sink K;
+    K.st = I->stream;
+    K.tl = tl;
+    pressure_sequence(I, po, pdt, s, corr, K);
 }
 
 // Mass-flux (u, q = 0) or scalar-mean (c, q = 2) control of substep set s
@@ -638,11 +668,12 @@ void enqueue_implicit3d(cf_instance* I, int s, Timeline* tl)
     if (tl) tl->mark(st);
 }
 
-void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
+// One RK3 substep of instance I through sink K.  The fully implicit scheme
+// is not batched: its launches go to K's stream directly.
+void enqueue_substep(cf_instance* I, Sink& K)
 {
     const cf_config& C = I->cfg;
     const Geo& G = I->geo;
-    cudaStream_t st = I->stream;
     const int s = (int) (I->substep % 3);
     const double dt = C.dt;
     const bool channel = C.scheme == CF_SCHEME_CHANNEL;
@@ -656,9 +687,9 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     GA.bc_c_bot = -0.5;
     GA.bc_c_top = +0.5;
     GA.bc_w = 0.0;
-    if (tl) tl->mark(st);
-    launch_ghosts(G, GA, st);
-    if (tl) tl->mark(st);
+    K.mark();
+    K.ghosts(G, GA);
+    K.mark();
 
     // RHS + forward sweeps; set index of each f slot (u, v, w, c) among the
     // implicit-solve sets (u, v, c, w)
@@ -679,14 +710,16 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
     R.wtop = I->bc_wt;
     R.wbc_bot = 0.0;
     R.wbc_top = 0.0;
-    launch_rhs(G, R, channel, st);
-    if (tl) tl->mark(st);
     if (channel) {
-        enqueue_implicit3d(I, s, tl);
-        pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, tl);
+        launch_rhs(G, R, true, K.st);
+        K.mark();
+        enqueue_implicit3d(I, s, K.tl);
+        pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, K);
         I->substep++;
         return;
     }
+    K.rhs(G, R);
+    K.mark();
 
     double* fields[4] = {I->u, I->v, I->c, I->w};
     const int fidx[4] = {0, 1, 3, 2};   // u, v, c, w -> f/g slots (u, v, w, c)
@@ -707,17 +740,304 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
         S.bct = is_w ? I->bc_wt : I->bc_ut;
         S.partial = partial[q];
     }
-    launch_back4(G, SB, st);
-    if (tl) tl->mark(st);
+    K.back4(G, SB);
+    K.mark();
     for (int q = 0; q < 4; q += 2) {   // mass-flux control (u), scalar-mean control (c)
-        launch_mass(G, partial[q], I->avg, mass_args(I, s, q, I->avg), st);
-        if (tl) tl->mark(st);
+        // each control has its own average buffer, so batched stages of
+        // different instances and fields never share one
+        double* avg = q == 0 ? I->avg : I->avg_c;
+        K.mass(G, partial[q], avg, mass_args(I, s, q, avg));
+        K.mark();
     }
-    pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, tl);
+    pressure_sequence(I, I->pois[s], (RK3_ALP[s] + RK3_BET[s]) * dt, s, true, K);
     I->substep++;
 }
 
+void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
+{
+    Sink K;
+    K.st = I->stream;
+    K.tl = tl;
+    enqueue_substep(I, K);
+}
+
+// ------------------------------------------------------------------ batches
+//
+// A batch runs the same stage of many z-implicit instances as one launch:
+// BatchSink records each instance's stage arguments (with its geometry and
+// its own grid) instead of launching; compile() groups the records of a
+// stage by kernel variant (order; transform size for the power-of-two
+// transforms), lays them out in one device block with each record's first
+// flat block, and turns every group into one batched launch (batch.cuh).
+
+enum StageKind { ST_GHOSTS, ST_RHS, ST_BACK4, ST_MASS, ST_DIV, ST_FFTY, ST_POISSON, ST_C2R, ST_PROJECT };
+
+struct BatchStage {
+    int kind = -1;
+    std::vector<BatchRec<GhostArgs>> ghosts;
+    std::vector<BatchRec<RhsArgs>> rhs;
+    std::vector<BatchRec<SolveBatch>> back4;
+    std::vector<BatchRec<RowAvgArgs>> rowavg;
+    std::vector<BatchRec<MassArgs>> control;
+    std::vector<BatchRec<DivArgs>> div;        // power-of-two nx: the divergence ...
+    std::vector<BatchRec<R2cArgs>> r2c;        // ... then its x transform
+    std::vector<BatchRec<DivArgs>> div_fftx;   // other nx: both in one kernel
+    std::vector<BatchRec<FftyArgs>> ffty;
+    std::vector<BatchRec<PoissonArgs>> poisson;
+    std::vector<BatchRec<C2rArgs>> c2r;
+    std::vector<BatchRec<ProjArgs>> project;
+};
+
+template <class Args>
+BatchRec<Args> batch_rec(const Geo& G, const Args& A, dim3 g)
+{
+    BatchRec<Args> r;
+    r.G = G;
+    r.A = A;
+    r.gx = g.x;
+    r.gy = g.y;
+    r.gz = g.z;
+    r.begin = 0;
+    return r;
+}
+
+struct BatchSink : Sink {
+    std::vector<BatchStage> stages;
+    size_t cursor = 0;
+    bool mismatch = false;
+    BatchStage& next(int kind)
+    {
+        if (cursor == stages.size()) {
+            stages.emplace_back();
+            stages.back().kind = kind;
+        }
+        BatchStage& S = stages[cursor++];
+        if (S.kind != kind) mismatch = true;
+        return S;
+    }
+    void mark() override {}
+    void ghosts(const Geo& G, const GhostArgs& A) override
+    {
+        next(ST_GHOSTS).ghosts.push_back(batch_rec(G, A, grid_ghosts(G)));
+    }
+    void rhs(const Geo& G, const RhsArgs& A) override { next(ST_RHS).rhs.push_back(batch_rec(G, A, grid_rhs(G))); }
+    void back4(const Geo& G, const SolveBatch& B) override
+    {
+        next(ST_BACK4).back4.push_back(batch_rec(G, B, grid_back4(G)));
+    }
+    void mass(const Geo& G, const double* partial, double* avg, const MassArgs& M) override
+    {
+        BatchStage& S = next(ST_MASS);
+        S.rowavg.push_back(batch_rec(G, row_average_args(G, partial, avg), dim3(G.n2)));
+        S.control.push_back(batch_rec(G, M, dim3(1)));
+    }
+    void div_fftx(const Geo& G, const DivArgs& A) override
+    {
+        BatchStage& S = next(ST_DIV);
+        if (batch_pow2(G.nx)) {
+            S.div.push_back(batch_rec(G, A, grid_div(G)));
+            R2cArgs R{A.dv, A.spec, A.px, A.c8, GZ, 0, 0};
+            S.r2c.push_back(batch_rec(G, R, grid_r2c(G, G.nz, 1)));
+        } else {
+            S.div_fftx.push_back(batch_rec(G, A, grid_div_fftx(G)));
+        }
+    }
+    void ffty(const Geo& G, const FftyArgs& A, int nrows) override
+    {
+        next(ST_FFTY).ffty.push_back(batch_rec(G, A, grid_ffty(G, nrows, 1)));
+    }
+    void poisson(const Geo& G, const PoissonArgs& A) override
+    {
+        next(ST_POISSON).poisson.push_back(batch_rec(G, A, grid_poisson(G)));
+    }
+    void c2r(const Geo& G, const C2rArgs& A, int nrows) override
+    {
+        next(ST_C2R).c2r.push_back(batch_rec(G, A, grid_c2r(G, nrows, 1)));
+    }
+    void project(const Geo& G, const ProjArgs& A) override
+    {
+        next(ST_PROJECT).project.push_back(batch_rec(G, A, grid_project(G)));
+    }
+};
+
+enum BatchKernel { BK_GHOSTS, BK_RHS, BK_BACK4, BK_ROWAVG, BK_CONTROL, BK_DIV, BK_R2C, BK_DIV_FFTX, BK_FFTY,
+                   BK_POISSON, BK_C2R, BK_PROJECT };
+
+struct BatchOp {
+    int kernel;
+    int key;              // order, or the transform size (0: generic transforms)
+    BatchLaunch L;        // L.recs holds a byte offset into the program's record block until upload
+};
+
+struct BatchProgram {
+    std::vector<char> blob;    // host copy of every record
+    void* dblob = nullptr;     // device copy (the launches read it)
+    std::vector<BatchOp> ops;
+    int substeps = 0;
+};
+
+// Append one group per key of `recs` to P: records laid out contiguously
+// with their first flat blocks, one batched launch each.
+template <class Args, class KeyFn, class SmemFn>
+void add_groups(BatchProgram& P, int kernel, const std::vector<BatchRec<Args>>& recs, KeyFn key, SmemFn smem)
+{
+    std::map<int, std::vector<BatchRec<Args>>> groups;
+    for (const auto& r : recs) groups[key(r)].push_back(r);
+    for (auto& kv : groups) {
+        auto& g = kv.second;
+        unsigned begin = 0;
+        size_t sm = 0;
+        for (auto& r : g) {
+            r.begin = begin;
+            begin += r.gx * r.gy * r.gz;
+            sm = std::max(sm, (size_t) smem(r));
+        }
+        size_t off = (P.blob.size() + 255) / 256 * 256;
+        P.blob.resize(off + g.size() * sizeof(BatchRec<Args>));
+        std::memcpy(P.blob.data() + off, g.data(), g.size() * sizeof(BatchRec<Args>));
+        BatchOp op;
+        op.kernel = kernel;
+        op.key = kv.first;
+        op.L.recs = reinterpret_cast<const void*>(off);
+        op.L.n = (int) g.size();
+        op.L.blocks = begin;
+        op.L.smem = sm;
+        P.ops.push_back(op);
+    }
+}
+
+void compile(const BatchSink& K, BatchProgram& P)
+{
+    auto order = [](const auto& r) { return r.G.order; };
+    auto none = [](const auto&) { return 0; };
+    auto p2nx = [](const auto& r) { return batch_pow2(r.G.nx) ? r.G.nx : 0; };
+    auto p2ny = [](const auto& r) { return batch_pow2(r.G.ny) ? r.G.ny : 0; };
+    auto smem_nx = [](const auto& r) { return batch_pow2(r.G.nx) ? (size_t) 0 : fft_smem_bytes(r.G.nx); };
+    auto smem_ny = [](const auto& r) { return batch_pow2(r.G.ny) ? (size_t) 0 : fft_smem_bytes(r.G.ny); };
+    for (const BatchStage& S : K.stages) {
+        switch (S.kind) {
+        case ST_GHOSTS: add_groups(P, BK_GHOSTS, S.ghosts, order, none); break;
+        case ST_RHS: add_groups(P, BK_RHS, S.rhs, order, none); break;
+        case ST_BACK4: add_groups(P, BK_BACK4, S.back4, order, none); break;
+        case ST_MASS:
+            add_groups(P, BK_ROWAVG, S.rowavg, none, none);
+            add_groups(P, BK_CONTROL, S.control, none, none);
+            break;
+        case ST_DIV:
+            add_groups(P, BK_DIV, S.div, order, none);
+            add_groups(P, BK_R2C, S.r2c, p2nx, none);
+            add_groups(P, BK_DIV_FFTX, S.div_fftx, order, smem_nx);
+            break;
+        case ST_FFTY: add_groups(P, BK_FFTY, S.ffty, p2ny, smem_ny); break;
+        case ST_POISSON: add_groups(P, BK_POISSON, S.poisson, order, none); break;
+        case ST_C2R: add_groups(P, BK_C2R, S.c2r, p2nx, smem_nx); break;
+        default: add_groups(P, BK_PROJECT, S.project, order, none); break;
+        }
+    }
+}
+
+int upload(BatchProgram& P, cudaStream_t st)
+{
+    CF_CUDA(cudaMallocAsync(&P.dblob, std::max<size_t>(P.blob.size(), 256), st));
+    CF_CUDA(cudaMemcpyAsync(P.dblob, P.blob.data(), P.blob.size(), cudaMemcpyHostToDevice, st));
+    for (BatchOp& op : P.ops)
+        op.L.recs = static_cast<const char*>(P.dblob) + reinterpret_cast<size_t>(op.L.recs);
+    return CF_OK;
+}
+
+void run_program(const BatchProgram& P, cudaStream_t st)
+{
+    for (const BatchOp& op : P.ops) {
+        const BatchLaunch& L = op.L;
+        switch (op.kernel) {
+        case BK_GHOSTS: launch_ghosts_batch(L, op.key, st); break;
+        case BK_RHS: launch_rhs_batch(L, op.key, st); break;
+        case BK_BACK4: launch_back4_batch(L, op.key, st); break;
+        case BK_ROWAVG: launch_row_average_batch(L, st); break;
+        case BK_CONTROL: launch_mass_control_batch(L, st); break;
+        case BK_DIV: launch_div_batch(L, op.key, st); break;
+        case BK_R2C: launch_r2c_batch(L, op.key, st); break;
+        case BK_DIV_FFTX: launch_div_fftx_batch(L, op.key, st); break;
+        case BK_FFTY: launch_ffty_batch(L, op.key, st); break;
+        case BK_POISSON: launch_poisson_batch(L, op.key, st); break;
+        case BK_C2R: launch_c2r_batch(L, op.key, st); break;
+        default: launch_project_batch(L, op.key, st); break;
+        }
+    }
+}
+
+// Record `nsub` substeps of every member into P (this advances each member's
+// host-side substep counter and f/g roles, as stepping would).
+int record(const std::vector<cf_instance*>& v, int nsub, BatchProgram& P)
+{
+    BatchSink K;
+    for (int q = 0; q < nsub; q++) {
+        const size_t base = K.stages.size();
+        size_t per = 0;
+        for (size_t m = 0; m < v.size(); m++) {
+            K.cursor = base;
+            enqueue_substep(v[m], K);
+            const size_t n = K.cursor - base;
+            if (m == 0) per = n;
+            if (n != per || K.mismatch) {
+                g_last_error = "batch members emit different stage sequences";
+                return CF_EINVAL;
+            }
+        }
+    }
+    compile(K, P);
+    P.substeps = nsub;
+    return CF_OK;
+}
+
+// Order the batch stream after each member's stream (before) or each member
+// stream after the batch stream (after).
+int join_streams(const std::vector<cf_instance*>& v, cudaStream_t st, cudaEvent_t ev, bool before)
+{
+    if (before) {
+        for (cf_instance* I : v) {
+            if (I->stream == st) continue;
+            CF_CUDA(cudaEventRecord(ev, I->stream));
+            CF_CUDA(cudaStreamWaitEvent(st, ev, 0));
+        }
+    } else {
+        CF_CUDA(cudaEventRecord(ev, st));
+        for (cf_instance* I : v)
+            if (I->stream != st) CF_CUDA(cudaStreamWaitEvent(I->stream, ev, 0));
+    }
+    return CF_OK;
+}
+
+int check_members(cf_instance* const* v, int n)
+{
+    if (!v || n <= 0) return CF_EINVAL;
+    for (int m = 0; m < n; m++) {
+        if (!v[m]) return CF_EINVAL;
+        if (v[m]->cfg.scheme != CF_SCHEME_CHANFAST || v[m]->device != v[0]->device) return CF_EINVAL;
+        for (int q = 0; q < m; q++)
+            if (v[q] == v[m]) return CF_EINVAL;
+    }
+    return CF_OK;
+}
+
 }  // namespace
+
+// Members are stepped by two programs, the substeps 0-2 and 3-5 of a
+// two-step cycle (six substeps restore every member's f/g roles); the whole
+// cycle replays as one CUDA graph.
+struct cf_batch {
+    std::vector<cf_instance*> v;
+    std::vector<long> expect;       // each member's substep count the programs expect
+    std::vector<double*> coef;      // each member's table block the records point into
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    BatchProgram half[2];
+    int cursor = 0;                 // the half that runs next
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t ev = nullptr;
+};
 
 // ======================================================================= C ABI
 
@@ -1136,6 +1456,190 @@ int cf_profile(cf_instance* I, int nsub, double* ms)
     }
     for (int g = 0; g <= CF_NKERNEL_GROUPS; g++) cudaEventDestroy(tl.ev[g]);
     return rc;
+}
+
+int cf_batch_step(cf_instance** members, int n, int nsub, void* stream)
+{
+    int rc = check_members(members, n);
+    if (rc) return rc;
+    if (nsub < 0) return CF_EINVAL;
+    if (nsub == 0) return CF_OK;
+    std::vector<cf_instance*> v(members, members + n);
+    cudaStream_t st = stream ? (cudaStream_t) stream : v[0]->stream;
+    BatchProgram P;
+    rc = record(v, nsub, P);
+    if (rc) return rc;
+    cudaEvent_t ev;
+    CF_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    rc = join_streams(v, st, ev, true);
+    if (rc == CF_OK) rc = upload(P, st);
+    if (rc == CF_OK) {
+        run_program(P, st);
+        cudaError_t e = cudaGetLastError();
+        cudaFreeAsync(P.dblob, st);
+        if (e != cudaSuccess) {
+            g_last_error = cudaGetErrorString(e);
+            rc = CF_ECUDA;
+        }
+    }
+    if (rc == CF_OK) rc = join_streams(v, st, ev, false);
+    cudaEventDestroy(ev);
+    return rc;
+}
+
+int cf_batch_destroy(cf_batch* B)
+{
+    if (!B) return CF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(B->device);
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    for (BatchProgram& P : B->half)
+        if (P.dblob) cudaFree(P.dblob);
+    if (B->ev) cudaEventDestroy(B->ev);
+    if (B->own_stream && B->stream) cudaStreamDestroy(B->stream);
+    cudaSetDevice(prev);
+    delete B;
+    return CF_OK;
+}
+
+static int batch_create_impl(cf_batch* B, cf_instance** members, int n, void* stream)
+{
+    B->v.assign(members, members + n);
+    B->device = members[0]->device;
+    if (stream) {
+        B->stream = (cudaStream_t) stream;
+    } else {
+        CF_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+        B->own_stream = true;
+    }
+    CF_CUDA(cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming));
+    std::vector<long> start;
+    for (cf_instance* I : B->v) start.push_back(I->substep);
+    for (int h = 0; h < 2; h++) {
+        int rc = record(B->v, 3, B->half[h]);
+        if (rc) {
+            for (size_t m = 0; m < B->v.size(); m++) B->v[m]->substep = start[m];
+            return rc;
+        }
+    }
+    // recording stepped the host state through the whole cycle: the f/g
+    // roles are back, the counters are put back
+    for (size_t m = 0; m < B->v.size(); m++) {
+        B->v[m]->substep = start[m];
+        B->coef.push_back(B->v[m]->coef);
+    }
+    B->expect = start;
+    for (BatchProgram& P : B->half) {
+        int rc = upload(P, B->stream);
+        if (rc) return rc;
+    }
+    CF_CUDA(cudaStreamSynchronize(B->stream));
+    return CF_OK;
+}
+
+int cf_batch_create(cf_instance** members, int n, void* stream, cf_batch** out)
+{
+    if (!out) return CF_EINVAL;
+    *out = nullptr;
+    int rc = check_members(members, n);
+    if (rc) return rc;
+    cf_batch* B = new (std::nothrow) cf_batch();
+    if (!B) return CF_ENOMEM;
+    int prev = 0;
+    CF_CUDA(cudaGetDevice(&prev));
+    CF_CUDA(cudaSetDevice(members[0]->device));
+    rc = batch_create_impl(B, members, n, stream);
+    cudaSetDevice(prev);
+    if (rc) {
+        cf_batch_destroy(B);
+        return rc;
+    }
+    *out = B;
+    return CF_OK;
+}
+
+// Run half h of the cycle eagerly and move the members' host state with it.
+static int batch_half(cf_batch* B, int h)
+{
+    run_program(B->half[h], B->stream);
+    CF_CUDA(cudaGetLastError());
+    for (size_t m = 0; m < B->v.size(); m++) {
+        cf_instance* I = B->v[m];
+        for (int q = 0; q < 3; q++)
+            for (int f = 0; f < 4; f++) std::swap(I->fbuf[f], I->gbuf[f]);
+        I->substep += 3;
+        B->expect[m] += 3;
+    }
+    B->cursor ^= 1;
+    return CF_OK;
+}
+
+int cf_batch_run(cf_batch* B, int nsteps)
+{
+    if (!B || nsteps < 0) return CF_EINVAL;
+    for (size_t m = 0; m < B->v.size(); m++) {
+        // stepped outside the batch, or its tables rebuilt (cf_set_dt): the
+        // recorded programs no longer describe it
+        if (B->v[m]->substep != B->expect[m] || B->v[m]->coef != B->coef[m]) {
+            g_last_error = "batch member changed outside the batch; create the batch again";
+            return CF_EINVAL;
+        }
+    }
+    int prev = 0;
+    CF_CUDA(cudaGetDevice(&prev));
+    CF_CUDA(cudaSetDevice(B->device));
+    int rc = join_streams(B->v, B->stream, B->ev, true);
+    if (rc == CF_OK && nsteps > 0 && B->cursor == 1) {
+        rc = batch_half(B, 1);
+        nsteps--;
+    }
+    while (rc == CF_OK && nsteps >= 2) {
+        if (!B->gexec) {
+            cudaError_t e = cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                run_program(B->half[0], B->stream);
+                run_program(B->half[1], B->stream);
+                e = cudaStreamEndCapture(B->stream, &B->graph);
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&B->gexec, B->graph, 0);
+            if (e != cudaSuccess) {
+                g_last_error = std::string("batch graph: ") + cudaGetErrorString(e);
+                rc = CF_ECUDA;
+                break;
+            }
+        }
+        cudaError_t e = cudaGraphLaunch(B->gexec, B->stream);
+        if (e != cudaSuccess) {
+            g_last_error = cudaGetErrorString(e);
+            rc = CF_ECUDA;
+            break;
+        }
+        for (size_t m = 0; m < B->v.size(); m++) {
+            B->v[m]->substep += 6;
+            B->expect[m] += 6;
+        }
+        nsteps -= 2;
+    }
+    if (rc == CF_OK && nsteps == 1) rc = batch_half(B, 0);
+    if (rc == CF_OK) rc = join_streams(B->v, B->stream, B->ev, false);
+    cudaSetDevice(prev);
+    return rc;
+}
+
+int cf_batch_sync(cf_batch* B)
+{
+    if (!B) return CF_EINVAL;
+    CF_CUDA(cudaStreamSynchronize(B->stream));
+    return CF_OK;
+}
+
+int cf_batch_launches_per_substep(const cf_batch* B)
+{
+    if (!B) return CF_EINVAL;
+    return (int) ((B->half[0].ops.size() + B->half[1].ops.size()) / 6);
 }
 
 int cf_launches_per_substep(const cf_instance* I)

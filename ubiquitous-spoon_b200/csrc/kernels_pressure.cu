@@ -19,6 +19,7 @@
 #include "engine.cuh"
 #include "host_band.h"
 #include "wall.cuh"
+#include "batch.cuh"
 
 namespace cf {
 
@@ -169,11 +170,11 @@ constexpr int FFT_MAXC = 16;    // N * L / threads for N <= 512
 
 
 template <int ORDER>
-__global__ void __launch_bounds__(FFT_THREADS) k_div_fftx(Geo G, DivArgs A)
+__device__ __forceinline__ void k_div_fftx_body(const Geo& G, const DivArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
-    const int k = GZ + blockIdx.y;
-    const int j0 = blockIdx.x * FFT_L;
+    const int k = GZ + bid.y;
+    const int j0 = bid.x * FFT_L;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
     const double dx = G.dx, dy = G.dy, dzk = G.dz[k];
     const double uc = A.mu ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
@@ -214,17 +215,31 @@ __global__ void __launch_bounds__(FFT_THREADS) k_div_fftx(Geo G, DivArgs A)
     }
 }
 
+template <int ORDER>
+__global__ void __launch_bounds__(FFT_THREADS) k_div_fftx(Geo G, DivArgs A)
+{
+    k_div_fftx_body<ORDER>(G, A, blockIdx);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(FFT_THREADS) k_div_fftx_batch(const BatchRec<DivArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<DivArgs>& R = batch_locate(r, n, b);
+    k_div_fftx_body<ORDER>(R.G, R.A, b);
+}
+
 // ------------------------------------------------------------------ y FFT
 
 
-__global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
+__device__ __forceinline__ void k_ffty_body(const Geo& G, const FftyArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
-    const int k = A.kfirst + blockIdx.y;
-    const int kx0 = blockIdx.x * FFT_L;
+    const int k = A.kfirst + bid.y;
+    const int kx0 = bid.x * FFT_L;
     const int ny = G.ny, nkx = G.nkx;
     const int nl = min(FFT_L, nkx - kx0);
-    double2* base = A.spec + blockIdx.z * A.fstride + ((long long) k * nkx + kx0) * ny;
+    double2* base = A.spec + bid.z * A.fstride + ((long long) k * nkx + kx0) * ny;
     for (int idx = threadIdx.x; idx < FFT_L * ny; idx += blockDim.x) {
         int line = idx / ny;
         sbuf[idx] = line < nl ? base[idx] : make_double2(0.0, 0.0);
@@ -240,16 +255,28 @@ __global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
     }
 }
 
+__global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
+{
+    k_ffty_body(G, A, blockIdx);
+}
+
+__global__ void __launch_bounds__(FFT_THREADS) k_ffty_batch(const BatchRec<FftyArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<FftyArgs>& R = batch_locate(r, n, b);
+    k_ffty_body(R.G, R.A, b);
+}
+
 // ---------------------------------------------------------- inverse x FFT
 
 
-__global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
+__device__ __forceinline__ void k_fftx_c2r_body(const Geo& G, const C2rArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
-    const int k = A.kfirst + blockIdx.y;
-    const int j0 = blockIdx.x * FFT_L;
+    const int k = A.kfirst + bid.y;
+    const int j0 = bid.x * FFT_L;
     const int nx = G.nx, ny = G.ny, nkx = G.nkx;
-    const double2* spec = A.spec + blockIdx.z * A.fstride;
+    const double2* spec = A.spec + bid.z * A.fstride;
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int pos = idx / FFT_L, jj = idx - pos * FFT_L, j = j0 + jj;
         double2 t = make_double2(0.0, 0.0);
@@ -269,8 +296,20 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
     fft_run<FFT_MAXC>(F, A.px);
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
-        if (j < ny) A.p[blockIdx.z][((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
+        if (j < ny) A.p[bid.z][((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
     }
+}
+
+__global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
+{
+    k_fftx_c2r_body(G, A, blockIdx);
+}
+
+__global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r_batch(const BatchRec<C2rArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<C2rArgs>& R = batch_locate(r, n, b);
+    k_fftx_c2r_body(R.G, R.A, b);
 }
 
 // ------------------------------------------------------------ Poisson in z
@@ -348,10 +387,10 @@ __device__ void average_walls(const PoissonArgs& A, int n2)
 // (the field's apply_bc follows the inverse transform).  One thread per
 // column, Re and Im sharing one factorisation.
 template <int ORDER, bool FILL>
-__device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A)
+__device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, uint3 bid)
 {
     const long long ncol = G.splane;
-    const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    const long long col = (long long) bid.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
     const int ny = G.ny, n2 = G.n2, n = A.nrows;
     const int kx = (int) (col / ny), ky = (int) (col - (long long) kx * ny);
@@ -540,24 +579,32 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A)
 template <int ORDER>
 __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs A)
 {
-    band_column<ORDER, true>(G, A);
+    band_column<ORDER, true>(G, A, blockIdx);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson_batch(const BatchRec<PoissonArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<PoissonArgs>& R = batch_locate(r, n, b);
+    band_column<ORDER, true>(R.G, R.A, b);
 }
 
 template <int ORDER>
 __global__ void __launch_bounds__(POIS_THREADS, 7) k_helmholtz_spectral(Geo G, PoissonArgs A)
 {
-    band_column<ORDER, false>(G, A);
+    band_column<ORDER, false>(G, A, blockIdx);
 }
 
 // ------------------------------------------------------------ projection
 
 
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
+__device__ __forceinline__ void k_project_body(const Geo& G, const ProjArgs& A, uint3 bid)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+    const int j = bid.x * blockDim.x + threadIdx.x;
+    const int i = bid.y * blockDim.y + threadIdx.y;
+    const int k = bid.z;
     if (j >= G.ny || i >= G.nx) return;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
     auto I = [&](int kk, int ii, int jj) {
@@ -587,6 +634,20 @@ __global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
         A.w[ijk] = A.w[ijk] - wp1h * (dt * G.idzp1h[k]);
     }
     if (A.mc) A.c[ijk] = A.c[ijk] + A.gc[k] * (*A.mc);   // chanfast.c:603-606
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
+{
+    k_project_body<ORDER>(G, A, blockIdx);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_project_batch(const BatchRec<ProjArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<ProjArgs>& R = batch_locate(r, n, b);
+    k_project_body<ORDER>(R.G, R.A, b);
 }
 
 // ------------------------------------------------- power-of-two fast path
@@ -711,15 +772,15 @@ __device__ __forceinline__ void dv_cp8(double* dst, const double* src)
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(DV_I * DV_J) k_div(Geo G, DivArgs A)
+__device__ __forceinline__ void k_div_body(const Geo& G, const DivArgs& A, uint3 bid)
 {
     __shared__ double su[2][DV_I + 3][DV_J];   // u, rows i0-2 .. i0+8
     __shared__ double sv[2][DV_I][DV_J + 3];   // v, columns j0-2 .. j0+32
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DV_J + tx;
-    const int j0 = blockIdx.x * DV_J, i0 = blockIdx.y * DV_I;
+    const int j0 = bid.x * DV_J, i0 = bid.y * DV_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
     const long long plane = G.plane;
-    const int k0 = GZ + blockIdx.z * DV_KC;
+    const int k0 = GZ + bid.z * DV_KC;
     const int k1 = min(k0 + DV_KC, n2 - GZ);
     const int i = i0 + ty, j = j0 + tx;
     const bool valid = i < nx && j < ny;
@@ -775,6 +836,20 @@ __global__ void __launch_bounds__(DV_I * DV_J) k_div(Geo G, DivArgs A)
     }
 }
 
+template <int ORDER>
+__global__ void __launch_bounds__(DV_I * DV_J) k_div(Geo G, DivArgs A)
+{
+    k_div_body<ORDER>(G, A, blockIdx);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(DV_I * DV_J) k_div_batch(const BatchRec<DivArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<DivArgs>& R = batch_locate(r, n, b);
+    k_div_body<ORDER>(R.G, R.A, b);
+}
+
 // Real-to-complex x transform (fftx_d2c, pressure.c:122-160, scaled by 1/N)
 // as a complex transform of half length: z[m] = x[2m] + i x[2m+1], Z = FFT(z),
 // X[k] = E[k] + exp(-2 pi i k/N) O[k] with E, O the transforms of the even and
@@ -782,16 +857,16 @@ __global__ void __launch_bounds__(DV_I * DV_J) k_div(Geo G, DivArgs A)
 // A line is M = N/2 points, 8 per thread; 256 / (M/8) lines of consecutive j
 // per block.
 template <int N>
-__global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, R2cArgs A)
+__device__ __forceinline__ void k_fftx_r2c_p2_body(const Geo& G, const R2cArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
     constexpr int M = N / 2, T = M / 8, L = p2_lines(M);
     const int l = threadIdx.x % L, t = threadIdx.x / L;
-    const int k = A.kfirst + blockIdx.y;
-    const int j = blockIdx.x * L + l;
+    const int k = A.kfirst + bid.y;
+    const int j = bid.x * L + l;
     const bool valid = j < G.ny;
     const int ny = G.ny;
-    const double* row = A.src + blockIdx.z * A.src_fstride + (long long) k * G.nx * ny + (valid ? j : 0);
+    const double* row = A.src + bid.z * A.src_fstride + (long long) k * G.nx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -807,7 +882,7 @@ __global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, R2cArgs A)
     __syncthreads();
     if (!valid) return;
     const double scale = 1.0 / (double) N;
-    double2* out = A.spec + blockIdx.z * A.spec_fstride + (long long) k * G.nkx * ny + j;
+    double2* out = A.spec + bid.z * A.spec_fstride + (long long) k * G.nkx * ny + j;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int kx = t + q * T;
@@ -826,16 +901,30 @@ __global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, R2cArgs A)
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
+__global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, R2cArgs A)
+{
+    k_fftx_r2c_p2_body<N>(G, A, blockIdx);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_fftx_r2c_p2_batch(const BatchRec<R2cArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<R2cArgs>& R = batch_locate(r, n, b);
+    k_fftx_r2c_p2_body<N>(R.G, R.A, b);
+}
+
+template <int N>
+__device__ __forceinline__ void k_ffty_p2_body(const Geo& G, const FftyArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
     constexpr int T = N / 8, L = p2_lines(N);
     const int t = threadIdx.x % T, l = threadIdx.x / T;
-    const int k = A.kfirst + blockIdx.y;
-    const int kx = blockIdx.x * L + l;
+    const int k = A.kfirst + bid.y;
+    const int kx = bid.x * L + l;
     const int nkx = G.nkx;
     const bool valid = kx < nkx;
-    double2* base = A.spec + blockIdx.z * A.fstride + ((long long) k * nkx + (valid ? kx : 0)) * N;
+    double2* base = A.spec + bid.z * A.fstride + ((long long) k * nkx + (valid ? kx : 0)) * N;
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) v[q] = valid ? base[t + q * T] : make_double2(0.0, 0.0);
@@ -850,22 +939,36 @@ __global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
     }
 }
 
+template <int N>
+__global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
+{
+    k_ffty_p2_body<N>(G, A, blockIdx);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_ffty_p2_batch(const BatchRec<FftyArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<FftyArgs>& R = batch_locate(r, n, b);
+    k_ffty_p2_body<N>(R.G, R.A, b);
+}
+
 // Complex-to-real x transform (fftx_c2d, pressure.c:163-200) as an inverse
 // complex transform of half length: with X[0] and X[N/2] taken real (as
 // FFTW's c2r does), Z[k] = (X[k] + conj X[M-k]) + i exp(2 pi i k/N)
 // (X[k] - conj X[M-k]) for k < M, z = IFFT(Z) unnormalised, and
 // x[2m] = Re z[m], x[2m+1] = Im z[m].
 template <int N>
-__global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
+__device__ __forceinline__ void k_fftx_c2r_p2_body(const Geo& G, const C2rArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
     constexpr int M = N / 2, T = M / 8, L = p2_lines(M);
     const int l = threadIdx.x % L, t = threadIdx.x / L;
-    const int k = A.kfirst + blockIdx.y;
-    const int j = blockIdx.x * L + l;
+    const int k = A.kfirst + bid.y;
+    const int j = bid.x * L + l;
     const bool valid = j < G.ny;
     const int ny = G.ny;
-    const double2* base = A.spec + blockIdx.z * A.fstride + (long long) k * G.nkx * ny + (valid ? j : 0);
+    const double2* base = A.spec + bid.z * A.fstride + (long long) k * G.nkx * ny + (valid ? j : 0);
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -881,13 +984,27 @@ __global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
     }
     fft_p2_line<M>(v, t, sbuf + l * p2_stride_x(M), A.px.tw, +1, A.c8, 2);
     if (!valid) return;
-    double* out = A.p[blockIdx.z] + (long long) k * G.nx * ny + j;
+    double* out = A.p[bid.z] + (long long) k * G.nx * ny + j;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int m = t + q * T;
         out[(long long) (2 * m) * ny] = v[q].x;
         out[(long long) (2 * m + 1) * ny] = v[q].y;
     }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
+{
+    k_fftx_c2r_p2_body<N>(G, A, blockIdx);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_fftx_c2r_p2_batch(const BatchRec<C2rArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<C2rArgs>& R = batch_locate(r, n, b);
+    k_fftx_c2r_p2_body<N>(R.G, R.A, b);
 }
 
 template <int N>
@@ -931,11 +1048,17 @@ static void launch_c2r_p2(const Geo& G, const C2rArgs& A, int nrows, int nfields
 template <int N>
 static cudaError_t p2_set_smem()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_fftx_r2c_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N / 2>());
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_x<N / 2>());
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) p2_smem_y<N>());
+    const int sx = (int) p2_smem_x<N / 2>(), sy = (int) p2_smem_y<N>();
+    cudaError_t e = cudaFuncSetAttribute(k_fftx_r2c_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sy);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_r2c_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sy);
     return e;
 }
+
+static bool pow2_kernel_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
 
 // -------------------------------------------------------------- launchers
 
@@ -1020,6 +1143,106 @@ void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st)
     else k_project<4><<<grd, blk, 0, st>>>(G, A);
 }
 
+// ------------------------------------------------------ batched launches
+//
+// Grids of the single-instance launches above, per stage, and the batched
+// launches over records carrying those grids (batch.cuh).  Power-of-two
+// transforms are batched per size (their kernels are templates on it); the
+// generic transforms of different sizes share one launch with the largest
+// instance's shared memory.
+
+dim3 grid_div(const Geo& G)
+{
+    return dim3((G.ny + DV_J - 1) / DV_J, (G.nx + DV_I - 1) / DV_I, (G.nz + DV_KC - 1) / DV_KC);
+}
+
+dim3 grid_r2c(const Geo& G, int nrows, int nfields)
+{
+    const int L = p2_lines(G.nx / 2);
+    return dim3((G.ny + L - 1) / L, nrows, nfields);
+}
+
+dim3 grid_div_fftx(const Geo& G) { return dim3((G.ny + FFT_L - 1) / FFT_L, G.nz); }
+
+dim3 grid_ffty(const Geo& G, int nrows, int nfields)
+{
+    const int L = pow2_kernel_size(G.ny) ? p2_lines(G.ny) : FFT_L;
+    return dim3((G.nkx + L - 1) / L, nrows, nfields);
+}
+
+dim3 grid_c2r(const Geo& G, int nrows, int nfields)
+{
+    const int L = pow2_kernel_size(G.nx) ? p2_lines(G.nx / 2) : FFT_L;
+    return dim3((G.ny + L - 1) / L, nrows, nfields);
+}
+
+dim3 grid_poisson(const Geo& G) { return dim3((unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS)); }
+
+dim3 grid_project(const Geo& G) { return dim3((G.ny + 31) / 32, (G.nx + 3) / 4, G.n2); }
+
+template <class Args>
+static const BatchRec<Args>* recs_of(const BatchLaunch& L) { return static_cast<const BatchRec<Args>*>(L.recs); }
+
+void launch_div_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    dim3 blk(DV_J, DV_I, 1);
+    if (order == 2) k_div_batch<2><<<L.blocks, blk, 0, st>>>(recs_of<DivArgs>(L), L.n);
+    else k_div_batch<4><<<L.blocks, blk, 0, st>>>(recs_of<DivArgs>(L), L.n);
+}
+
+void launch_r2c_batch(const BatchLaunch& L, int nx, cudaStream_t st)
+{
+    switch (nx) {
+    case 64: k_fftx_r2c_p2_batch<64><<<L.blocks, 256, p2_smem_x<32>(), st>>>(recs_of<R2cArgs>(L), L.n); break;
+    case 128: k_fftx_r2c_p2_batch<128><<<L.blocks, 256, p2_smem_x<64>(), st>>>(recs_of<R2cArgs>(L), L.n); break;
+    case 256: k_fftx_r2c_p2_batch<256><<<L.blocks, 256, p2_smem_x<128>(), st>>>(recs_of<R2cArgs>(L), L.n); break;
+    default: k_fftx_r2c_p2_batch<512><<<L.blocks, 256, p2_smem_x<256>(), st>>>(recs_of<R2cArgs>(L), L.n); break;
+    }
+}
+
+void launch_div_fftx_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    if (order == 2) k_div_fftx_batch<2><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<DivArgs>(L), L.n);
+    else k_div_fftx_batch<4><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<DivArgs>(L), L.n);
+}
+
+void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st)
+{
+    switch (ny) {
+    case 64: k_ffty_p2_batch<64><<<L.blocks, 256, p2_smem_y<64>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
+    case 128: k_ffty_p2_batch<128><<<L.blocks, 256, p2_smem_y<128>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
+    case 256: k_ffty_p2_batch<256><<<L.blocks, 256, p2_smem_y<256>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
+    case 512: k_ffty_p2_batch<512><<<L.blocks, 256, p2_smem_y<512>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
+    default: k_ffty_batch<<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<FftyArgs>(L), L.n); break;
+    }
+}
+
+void launch_poisson_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    if (order == 2) k_poisson_batch<2><<<L.blocks, POIS_THREADS, 0, st>>>(recs_of<PoissonArgs>(L), L.n);
+    else k_poisson_batch<4><<<L.blocks, POIS_THREADS, pois_smem_bytes(), st>>>(recs_of<PoissonArgs>(L), L.n);
+}
+
+void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st)
+{
+    switch (nx) {
+    case 64: k_fftx_c2r_p2_batch<64><<<L.blocks, 256, p2_smem_x<32>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
+    case 128: k_fftx_c2r_p2_batch<128><<<L.blocks, 256, p2_smem_x<64>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
+    case 256: k_fftx_c2r_p2_batch<256><<<L.blocks, 256, p2_smem_x<128>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
+    case 512: k_fftx_c2r_p2_batch<512><<<L.blocks, 256, p2_smem_x<256>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
+    default: k_fftx_c2r_batch<<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<C2rArgs>(L), L.n); break;
+    }
+}
+
+void launch_project_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    dim3 blk(32, 4, 1);
+    if (order == 2) k_project_batch<2><<<L.blocks, blk, 0, st>>>(recs_of<ProjArgs>(L), L.n);
+    else k_project_batch<4><<<L.blocks, blk, 0, st>>>(recs_of<ProjArgs>(L), L.n);
+}
+
+bool batch_pow2(int n) { return pow2_kernel_size(n); }
+
 cudaError_t fft_set_smem_limits(int max_n)
 {
     size_t sm = fft_smem_bytes(max_n);
@@ -1033,6 +1256,13 @@ cudaError_t fft_set_smem_limits(int max_n)
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    }
+    if (e == cudaSuccess) {   // batched generic transforms: room for the largest size
+        int v = (int) fft_smem_bytes(FFT_MAX_N);
+        e = cudaFuncSetAttribute(k_div_fftx_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     }
     return e;
 }

@@ -13,6 +13,7 @@
 #include "engine.cuh"
 #include "host_band.h"
 #include "wall.cuh"
+#include "batch.cuh"
 
 #include <type_traits>
 
@@ -27,9 +28,9 @@ __device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >
 // (apply_bc_w, then with EXTRAP the massflux4 extrapolation of
 // advect.c:100-131).
 template <int ORDER, bool EXTRAP>
-__global__ void k_ghosts(Geo G, GhostArgs A)
+__device__ __forceinline__ void ghosts_body(const Geo& G, const GhostArgs& A, uint3 bid)
 {
-    long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    long long col = (long long) bid.x * blockDim.x + threadIdx.x;
     if (col >= G.plane) return;
     const long long P = G.plane;
     const int n2 = G.n2, kb = GZ - 1, kt = n2 - GZ;
@@ -68,6 +69,20 @@ __global__ void k_ghosts(Geo G, GhostArgs A)
         at(w, wt + 2) = top3;
     }
     (void) g2; (void) g3; (void) top2; (void) top3;
+}
+
+template <int ORDER, bool EXTRAP>
+__global__ void k_ghosts(Geo G, GhostArgs A)
+{
+    ghosts_body<ORDER, EXTRAP>(G, A, blockIdx);
+}
+
+template <int ORDER, bool EXTRAP>
+__global__ void k_ghosts_batch(const BatchRec<GhostArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<GhostArgs>& R = batch_locate(r, n, b);
+    ghosts_body<ORDER, EXTRAP>(R.G, R.A, b);
 }
 
 // --------------------------------------------------------------------- RHS
@@ -156,11 +171,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <int ORDER, bool IMPL3D>
-__global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
+__device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 bid)
 {
     extern __shared__ double sm[];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RT_J + tx;
-    const int j0 = blockIdx.x * RT_J, i0 = blockIdx.y * RT_I;
+    const int j0 = bid.x * RT_J, i0 = bid.y * RT_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
     const long long plane = (long long) nx * ny;
     const int kb = GZ, ke = GZ + G.nz;   // all interior rows: the forward sweeps run in order
@@ -522,12 +537,30 @@ __global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
     }
 }
 
+template <int ORDER, bool IMPL3D>
+__global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
+{
+    rhs_body<ORDER, IMPL3D>(G, A, blockIdx);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(RT_THREADS, 1) k_rhs_batch(const BatchRec<RhsArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<RhsArgs>& R = batch_locate(r, n, b);
+    rhs_body<ORDER, false>(R.G, R.A, b);
+}
+
 // ------------------------------------------------------------- launchers
+
+constexpr int GHOST_THREADS = 256;
+
+dim3 grid_ghosts(const Geo& G) { return dim3((unsigned) ((G.plane + GHOST_THREADS - 1) / GHOST_THREADS)); }
 
 void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st, bool extrap)
 {
-    int th = 256;
-    long long nb = (G.plane + th - 1) / th;
+    const int th = GHOST_THREADS;
+    const unsigned nb = grid_ghosts(G).x;
     if (extrap) {
         if (G.order == 2) k_ghosts<2, true><<<(unsigned) nb, th, 0, st>>>(G, A);
         else k_ghosts<4, true><<<(unsigned) nb, th, 0, st>>>(G, A);
@@ -537,10 +570,27 @@ void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st, bool extra
     }
 }
 
+dim3 grid_rhs(const Geo& G) { return dim3((G.ny + RT_J - 1) / RT_J, (G.nx + RT_I - 1) / RT_I, 1); }
+
+void launch_ghosts_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    auto r = static_cast<const BatchRec<GhostArgs>*>(L.recs);
+    if (order == 2) k_ghosts_batch<2, true><<<L.blocks, GHOST_THREADS, 0, st>>>(r, L.n);
+    else k_ghosts_batch<4, true><<<L.blocks, GHOST_THREADS, 0, st>>>(r, L.n);
+}
+
+void launch_rhs_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    auto r = static_cast<const BatchRec<RhsArgs>*>(L.recs);
+    dim3 blk(RT_J, RT_I, 1);
+    if (order == 2) k_rhs_batch<2><<<L.blocks, blk, rhs_smem_bytes(), st>>>(r, L.n);
+    else k_rhs_batch<4><<<L.blocks, blk, rhs_smem_bytes(), st>>>(r, L.n);
+}
+
 void launch_rhs(const Geo& G, const RhsArgs& A, bool implicit3d, cudaStream_t st)
 {
     dim3 blk(RT_J, RT_I, 1);
-    dim3 grd((G.ny + RT_J - 1) / RT_J, (G.nx + RT_I - 1) / RT_I, 1);
+    dim3 grd = grid_rhs(G);
     size_t sm = rhs_smem_bytes();
     if (implicit3d) {
         if (G.order == 2) k_rhs<2, true><<<grd, blk, sm, st>>>(G, A);
@@ -558,6 +608,8 @@ cudaError_t rhs_set_smem_limits()
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
     return e;
 }
 

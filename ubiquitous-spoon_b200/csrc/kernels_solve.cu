@@ -17,6 +17,7 @@
 #include "engine.cuh"
 #include "host_band.h"
 #include "wall.cuh"
+#include "batch.cuh"
 
 namespace cf {
 
@@ -28,9 +29,9 @@ __device__ __forceinline__ double warp_sum(double v)
 
 // Back substitution and apply_bc of one column of one field.
 template <int ORDER, bool IS_W>
-__device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A)
+__device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A, uint3 bid)
 {
-    const long long col = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    const long long col = (long long) bid.x * blockDim.x + threadIdx.x;
     const bool active = col < G.plane;
     const long long P = G.plane;
     const int n2 = G.n2;
@@ -53,7 +54,7 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A)
     double y1 = 0.0, y2 = 0.0, y3 = 0.0;
     double top0 = 0.0, top1 = 0.0, top2 = 0.0, bot0 = 0.0, bot1 = 0.0, bot2 = 0.0;
     const bool stats = A.partial != nullptr;
-    const long long wrow = ((long long) blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const long long wrow = ((long long) bid.x * blockDim.x + threadIdx.x) / 32;
     for (int i0 = n - 1; i0 >= 0; i0 -= PD) {
 #pragma unroll
         for (int u = 0; u < PD; u++) {
@@ -120,27 +121,35 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A)
 
 // Row sums of the per-warp partials -> xy-average profile avg[k]
 // (get_xy_avg, get.c:281-302).  One block per row, fixed summation order.
-__global__ void k_row_average(const double* __restrict__ partial, long long nwarps, int n2,
-                              double scale, double* __restrict__ avg)
+__device__ __forceinline__ void row_average_body(const RowAvgArgs& A, uint3 bid)
 {
     __shared__ double red[256];
-    const int k = blockIdx.x;
+    const int k = bid.x, n2 = A.n2;
+    const double* __restrict__ partial = A.partial;
     double s = 0.0;
-    for (long long w = threadIdx.x; w < nwarps; w += blockDim.x) s += partial[w * n2 + k];
+    for (long long w = threadIdx.x; w < A.nwarps; w += blockDim.x) s += partial[w * n2 + k];
     red[threadIdx.x] = s;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if ((int) threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) avg[k] = red[0] * scale;
+    if (threadIdx.x == 0) A.avg[k] = red[0] * A.scale;
 }
 
+__global__ void k_row_average(RowAvgArgs A) { row_average_body(A, blockIdx); }
+
+__global__ void k_row_average_batch(const BatchRec<RowAvgArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<RowAvgArgs>& R = batch_locate(r, n, b);
+    row_average_body(R.A, b);
+}
 
 // Bulk-mean control of chanfast.c:485-529 (u) / 572-616 (c).
-__global__ void k_mass_control(MassArgs A)
+__device__ __forceinline__ void mass_control_body(const MassArgs& A)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x != 0) return;
     const double* avg = A.avg;
     const double* dz = A.dz;
     const int g = GZ, n2 = A.n2, nz = A.nz;
@@ -175,38 +184,92 @@ __global__ void k_mass_control(MassArgs A)
     }
 }
 
+__global__ void k_mass_control(MassArgs A)
+{
+    if (blockIdx.x == 0) mass_control_body(A);
+}
+
+__global__ void k_mass_control_batch(const BatchRec<MassArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<MassArgs>& R = batch_locate(r, n, b);
+    mass_control_body(R.A);
+}
+
 // The back substitutions of the four implicit solves in one launch; the
 // control kernels that read the u and c row sums run after it.  blockIdx.y
 // selects the field: 0 u, 1 v, 2 c, 3 w.
 template <int ORDER>
-__global__ void __launch_bounds__(SOLVE_THREADS) k_back4(Geo G, SolveBatch B)
+__device__ __forceinline__ void back4_body(const Geo& G, const SolveBatch& B, uint3 bid)
 {
-    switch (blockIdx.y) {
-    case 0: back_column<ORDER, false>(G, B.a[0]); break;
-    case 1: back_column<ORDER, false>(G, B.a[1]); break;
-    case 2: back_column<ORDER, false>(G, B.a[2]); break;
-    default: back_column<ORDER, true>(G, B.a[3]); break;
+    switch (bid.y) {
+    case 0: back_column<ORDER, false>(G, B.a[0], bid); break;
+    case 1: back_column<ORDER, false>(G, B.a[1], bid); break;
+    case 2: back_column<ORDER, false>(G, B.a[2], bid); break;
+    default: back_column<ORDER, true>(G, B.a[3], bid); break;
     }
 }
 
+template <int ORDER>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_back4(Geo G, SolveBatch B)
+{
+    back4_body<ORDER>(G, B, blockIdx);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_back4_batch(const BatchRec<SolveBatch>* r, int n)
+{
+    uint3 b;
+    const BatchRec<SolveBatch>& R = batch_locate(r, n, b);
+    back4_body<ORDER>(R.G, R.A, b);
+}
+
+dim3 grid_back4(const Geo& G) { return dim3((unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS), 4); }
+
 void launch_back4(const Geo& G, const SolveBatch& B, cudaStream_t st)
 {
-    dim3 grd((unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS), 4);
+    dim3 grd = grid_back4(G);
     if (G.order == 2) k_back4<2><<<grd, SOLVE_THREADS, 0, st>>>(G, B);
     else k_back4<4><<<grd, SOLVE_THREADS, 0, st>>>(G, B);
 }
 
+RowAvgArgs row_average_args(const Geo& G, const double* partial, double* avg)
+{
+    RowAvgArgs R;
+    R.partial = partial;
+    R.nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);
+    R.n2 = G.n2;
+    R.scale = 1.0 / ((double) G.nx * (double) G.ny);
+    R.avg = avg;
+    return R;
+}
+
 void launch_mass(const Geo& G, const double* partial, double* avg, const MassArgs& M, cudaStream_t st)
 {
-    long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);
-    double scale = 1.0 / ((double) G.nx * (double) G.ny);
-    k_row_average<<<G.n2, 256, 0, st>>>(partial, nwarps, G.n2, scale, avg);
+    k_row_average<<<G.n2, 256, 0, st>>>(row_average_args(G, partial, avg));
     k_mass_control<<<1, 32, 0, st>>>(M);
 }
 
 void launch_mass_control(const MassArgs& M, cudaStream_t st)
 {
     k_mass_control<<<1, 32, 0, st>>>(M);
+}
+
+void launch_back4_batch(const BatchLaunch& L, int order, cudaStream_t st)
+{
+    auto r = static_cast<const BatchRec<SolveBatch>*>(L.recs);
+    if (order == 2) k_back4_batch<2><<<L.blocks, SOLVE_THREADS, 0, st>>>(r, L.n);
+    else k_back4_batch<4><<<L.blocks, SOLVE_THREADS, 0, st>>>(r, L.n);
+}
+
+void launch_row_average_batch(const BatchLaunch& L, cudaStream_t st)
+{
+    k_row_average_batch<<<L.blocks, 256, 0, st>>>(static_cast<const BatchRec<RowAvgArgs>*>(L.recs), L.n);
+}
+
+void launch_mass_control_batch(const BatchLaunch& L, cudaStream_t st)
+{
+    k_mass_control_batch<<<L.blocks, 32, 0, st>>>(static_cast<const BatchRec<MassArgs>*>(L.recs), L.n);
 }
 
 }  // namespace cf
