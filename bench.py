@@ -422,6 +422,75 @@ def run_ensemble(args):
     print(json.dumps(result), flush=True)
 
 
+# -------------------------------------------------------------- serving
+
+SERVE_GRIDS = ENSEMBLE_GRIDS + [(256, 256, 192)]
+
+
+def serve_trace(n, rate, step_scale, seed=0):
+    """Poisson arrivals at `rate` per second; per request a grid from
+    SERVE_GRIDS, Re_b log-uniform in [2800, 20000], order 2 or 4, and
+    U[200, 2000] RK3 steps times step_scale."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for q in range(n):
+        t += rng.exponential(1.0 / rate)
+        nx, ny, nz = SERVE_GRIDS[int(rng.integers(len(SERVE_GRIDS)))]
+        re = float(math.exp(rng.uniform(math.log(2800.0), math.log(20000.0))))
+        order = int(rng.choice([2, 4]))
+        steps = max(1, int(round(int(rng.integers(200, 2001)) * step_scale)))
+        out.append(dict(arrival_s=t, nx=nx, ny=ny, nz=nz, re=re, order=order, nsteps=steps, seed=q))
+    return out
+
+
+def run_serve(args):
+    """p50 / p99 completion latency and solves/hour of the serving loop
+    (cf_serve: admission by a 150 GB budget, continuous batching, one
+    batched step per round) on a Poisson trace; with --serve-baseline also
+    the same trace served one solve at a time (max_active = 1)."""
+    import numpy as np
+    import torch
+    cf = importlib.import_module("ubiquitous-spoon_b200")
+    torch.cuda.set_device(0)
+    trace = serve_trace(args.serve_requests, 4.0, args.serve_step_scale)
+    reqs = []
+    for r in trace:
+        cfg = cf.Config.make(order=r["order"], nx=r["nx"], ny=r["ny"], nz=r["nz"], lx=2 * math.pi, ly=math.pi,
+                             lz=2.0, dt=2.5e-4 if r["nx"] >= 256 else 1e-3, nu=1.0 / r["re"], prandtl=0.71)
+        reqs.append(dict(cfg=cfg, seed=r["seed"], amp=0.05, c_amp=0.01, nsteps=r["nsteps"],
+                         arrival_s=r["arrival_s"]))
+
+    def measure(max_active):
+        t0 = time.perf_counter()
+        res = cf.serve(reqs, hbm_budget_bytes=150e9, max_active=max_active, quantum=1)
+        wall = time.perf_counter() - t0
+        lat = np.array([x["finish_s"] - r["arrival_s"] for x, r in zip(res, reqs)])
+        ok = sum(1 for x in res if x["status"] == 0)
+        work = sum(r["nx"] * r["ny"] * r["nz"] * 3 * r["nsteps"] for r in trace)
+        return {"p50_latency_s": round(float(np.percentile(lat, 50)), 3),
+                "p99_latency_s": round(float(np.percentile(lat, 99)), 3),
+                "solves_per_h": round(ok / wall * 3600.0, 1), "completed": ok, "wall_s": round(wall, 2),
+                "mpt_substeps_per_s": round(work / wall / 1e6, 1)}
+
+    with ClockSampler(0) as clk:
+        served = measure(64)
+    result = {"metric": "serving p50/p99 completion latency, solves/h", "value": served["solves_per_h"],
+              "unit": "solves/h", "n_gpus": 1, "higher_is_better": True, "served": served,
+              "dtype": "f64", "data": "synthetic",
+              "config": {"workload": f"{len(reqs)} requests, Poisson arrivals 4/s (seed 0), grids "
+                                     + ", ".join("x".join(map(str, g)) for g in SERVE_GRIDS)
+                                     + ", Re_b log-U[2800, 20000], order 2 or 4",
+                         "steps": f"U[200, 2000] x {args.serve_step_scale} RK3 steps per request",
+                         "admission": "150 GB budget by cf_instance_bytes, at most 64 resident",
+                         "rounds": "one RK3 step of every resident solve per batched call"},
+              "clocks": clk.summary()}
+    if args.serve_baseline:
+        result["one_at_a_time"] = measure(1)
+    print(json.dumps(result), flush=True)
+
+
 def ctypes_stream(torch_stream):
     import ctypes
     return ctypes.c_void_p(torch_stream.cuda_stream)
@@ -460,6 +529,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ensemble", action="store_true",
                     help="the 64-instance batched ensemble against running its members one after another")
+    ap.add_argument("--serve", action="store_true", help="the serving loop on a Poisson request trace")
+    ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--serve-step-scale", type=float, default=0.1,
+                    help="scale of the U[200, 2000] step counts (1.0 = the full trace)")
+    ap.add_argument("--serve-baseline", action="store_true", help="also serve the trace one solve at a time")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 (default) is the benchmark; the others serve profiling and checks")
     args = ap.parse_args()
@@ -469,6 +543,8 @@ def main():
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.ensemble:
         run_ensemble(args)
+    elif args.serve:
+        run_serve(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

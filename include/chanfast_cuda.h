@@ -195,6 +195,46 @@ int cf_batch_launches_per_substep(const cf_batch *batch);
 int cf_batch_destroy(cf_batch *batch);
 
 /* ------------------------------------------------------------------------
+ * Serving: a request loop over the instance and batch calls.
+ *
+ * cf_instance_bytes: device memory an instance of this configuration holds
+ * (fields, right-hand sides, spectrum, solver scratch, tables, the staging
+ * buffer of one padded field); 0 for an invalid configuration.
+ *
+ * cf_serve: serve n requests that arrive at arrival_s seconds after the call
+ * (non-decreasing).  In arrival order, a request is admitted (instance
+ * created, seeded initial state, cf_init_fields) once it has arrived, while
+ * the resident instances' cf_instance_bytes plus its own stay within
+ * hbm_budget_bytes and fewer than max_active are resident.  Each round
+ * advances every resident solve by min(quantum, steps left) RK3 steps with
+ * cf_batch_step (new arrivals join at the next round); a solve that has run
+ * its steps is retired at once: on_done(index, inst, user) may read its
+ * fields, then its memory is released (inst is NULL for a request that
+ * failed; its status says why).  Requests use CF_SCHEME_CHANFAST.  Each
+ * solve's result is the same, bit for bit, as stepping it alone with
+ * cf_batch_step.  Times in results are seconds after the call.
+ * ------------------------------------------------------------------------ */
+typedef struct cf_request {
+    cf_config cfg;
+    unsigned long long seed;     /* cf_init_fields arguments */
+    double amp, c_amp;
+    int nsteps;                  /* RK3 steps to run */
+    double arrival_s;
+} cf_request;
+
+typedef struct cf_result {
+    double admit_s, finish_s;
+    int status;
+    long long steps_done;
+} cf_result;
+
+typedef void (*cf_done_fn)(int index, cf_instance *inst, void *user);
+
+unsigned long long cf_instance_bytes(const cf_config *cfg);
+int cf_serve(const cf_request *reqs, int n, double hbm_budget_bytes, int max_active, int quantum,
+             void *stream, cf_done_fn on_done, void *user, cf_result *results);
+
+/* ------------------------------------------------------------------------
  * Drop-in drivers (libchanfast.so).  Same names and arguments as the
  * reference (chanfast.h:1-21, called at main.c:56-60); they read
  * outputdir/{u,v,w,c}_it<it>.dat, run nt - it time steps on the current

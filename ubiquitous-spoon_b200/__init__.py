@@ -86,6 +86,23 @@ class Config(ctypes.Structure):
         return (self.nx, self.ny, self.nz)
 
 
+class Request(ctypes.Structure):
+    """Mirror of cf_request."""
+
+    _fields_ = [("cfg", Config), ("seed", ctypes.c_ulonglong), ("amp", ctypes.c_double),
+                ("c_amp", ctypes.c_double), ("nsteps", ctypes.c_int), ("arrival_s", ctypes.c_double)]
+
+
+class Result(ctypes.Structure):
+    """Mirror of cf_result."""
+
+    _fields_ = [("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double), ("status", ctypes.c_int),
+                ("steps_done", ctypes.c_longlong)]
+
+
+DONE_FN = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
+
+
 def _bind(L):
     vp, ip, dp, ll = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long
     L.cf_create.argtypes = [ctypes.POINTER(Config), vp, ctypes.POINTER(vp)]
@@ -110,6 +127,10 @@ def _bind(L):
     L.cf_strerror.restype = ctypes.c_char_p
     L.cf_strerror.argtypes = [ip]
     pvp = ctypes.POINTER(vp)
+    L.cf_instance_bytes.restype = ctypes.c_ulonglong
+    L.cf_instance_bytes.argtypes = [ctypes.POINTER(Config)]
+    L.cf_serve.argtypes = [ctypes.POINTER(Request), ip, ctypes.c_double, ip, ip, vp, DONE_FN, vp,
+                           ctypes.POINTER(Result)]
     L.cf_batch_step.argtypes = [pvp, ip, ip, vp]
     L.cf_batch_create.argtypes = [pvp, ip, vp, pvp]
     L.cf_batch_run.argtypes = [vp, ip]
@@ -168,13 +189,26 @@ class Instance:
     def __init__(self, cfg: Config, stream=None):
         self.L = lib()
         self.cfg = cfg
+        self.owned = True
         h = ctypes.c_void_p()
         _check(self.L.cf_create(ctypes.byref(cfg), stream, ctypes.byref(h)), "cf_create")
         self.h = h
 
+    @classmethod
+    def borrow(cls, handle, cfg):
+        """A view of an instance owned elsewhere (the serving loop): usable
+        while the owner keeps it alive, never destroyed through the view."""
+        v = cls.__new__(cls)
+        v.L = lib()
+        v.cfg = cfg
+        v.owned = False
+        v.h = ctypes.c_void_p(handle)
+        return v
+
     def close(self):
         if getattr(self, "h", None) and self.h.value:
-            self.L.cf_destroy(self.h)
+            if getattr(self, "owned", True):
+                self.L.cf_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __enter__(self):
@@ -262,6 +296,46 @@ class Instance:
 
     def launches_per_substep(self):
         return int(self.L.cf_launches_per_substep(self.h))
+
+
+def instance_bytes(cfg):
+    """Device bytes an instance of this configuration holds (cf_instance_bytes)."""
+    return int(lib().cf_instance_bytes(ctypes.byref(cfg)))
+
+
+def serve(requests, hbm_budget_bytes, max_active=64, quantum=1, stream=None, on_done=None):
+    """Run the serving loop (cf_serve) over `requests`, a list of dicts with
+    keys cfg (Config), seed, amp, c_amp, nsteps, arrival_s (seconds after the
+    call, non-decreasing).  on_done(index, view) is called as each solve
+    retires, with a borrowed Instance view (get_field, log) or None if the
+    request failed.  Returns a list of dicts: admit_s, finish_s, status,
+    steps_done."""
+    L = lib()
+    n = len(requests)
+    reqs = (Request * n)()
+    for q, r in enumerate(requests):
+        reqs[q].cfg = r["cfg"]
+        reqs[q].seed = r.get("seed", 0)
+        reqs[q].amp = r.get("amp", 0.1)
+        reqs[q].c_amp = r.get("c_amp", 0.01)
+        reqs[q].nsteps = r["nsteps"]
+        reqs[q].arrival_s = r.get("arrival_s", 0.0)
+    res = (Result * n)()
+    errors = []
+
+    def done(index, handle, user):
+        if on_done is None:
+            return
+        try:
+            on_done(index, Instance.borrow(handle, requests[index]["cfg"]) if handle else None)
+        except Exception as e:   # keep the C loop running; report afterwards
+            errors.append(e)
+
+    cb = DONE_FN(done)
+    _check(L.cf_serve(reqs, n, float(hbm_budget_bytes), max_active, quantum, stream, cb, None, res), "cf_serve")
+    if errors:
+        raise errors[0]
+    return [dict(admit_s=r.admit_s, finish_s=r.finish_s, status=r.status, steps_done=r.steps_done) for r in res]
 
 
 def _handles(instances):

@@ -26,7 +26,8 @@ NVCC = os.environ.get("NVCC", "nvcc")
 CC = os.environ.get("CC", "gcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["host_band.cpp", "kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu", "instance.cu"]
+CUDA_SOURCES = ["host_band.cpp", "kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu", "instance.cu",
+                "serve.cpp"]
 FMA_SOURCES = {"kernels_rhs.cu", "kernels_solve.cu", "kernels_pressure.cu"}
 LIB_CUDA = os.path.join(HERE, "libchanfast_cuda.so")
 # The reference's step functions (include/chanfast_steps.h): their own

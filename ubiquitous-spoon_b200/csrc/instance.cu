@@ -1642,6 +1642,25 @@ int cf_batch_launches_per_substep(const cf_batch* B)
     return (int) ((B->half[0].ops.size() + B->half[1].ops.size()) / 6);
 }
 
+unsigned long long cf_instance_bytes(const cf_config* c)
+{
+    if (check_config(c) != CF_OK) return 0;
+    // the allocations of create_impl and build_tables
+    const unsigned long long n2 = c->nz + 2 * GZ, plane = (unsigned long long) c->nx * c->ny;
+    const unsigned long long splane = (unsigned long long) (c->nx / 2 + 1) * c->ny;
+    const unsigned long long fb = plane * n2 * 8;
+    unsigned long long b = 5 * fb + 8 * fb;                                     // u v w c p, f and g blocks
+    b += (c->scheme == CF_SCHEME_CHANNEL ? 4 : 1) * splane * n2 * 16;          // spectra
+    b += (c->order == 4 ? 3 : 1) * splane * n2 * 8;                            // band-solve scratch
+    const unsigned long long nwarps = (plane + SOLVE_THREADS - 1) / SOLVE_THREADS * (SOLVE_THREADS / 32);
+    b += 2 * nwarps * n2 * 8 + 2 * n2 * 8 + 64 + 8;                            // row sums, averages, scalars
+    b += 3ull * 4096 * LOG_COLS * 8;                                           // log ring
+    b += (unsigned long long) (c->nx + c->ny) * 16;                            // twiddles
+    b += n2 * 8 * 512 + (unsigned long long) (c->nx + c->ny) * 8;              // coefficient tables (bound)
+    b += (unsigned long long) (c->nx + 2 * c->ngx) * (c->ny + 2 * c->ngy) * n2 * 8;   // staging
+    return b;
+}
+
 int cf_launches_per_substep(const cf_instance* I)
 {
     // pressure: div+fftx (two launches for power-of-two nx), ffty, poisson,
