@@ -54,7 +54,10 @@ def params(order, nx, ny, nz, **kw):
     return cn.Params(order=order, nx=nx, ny=ny, nz=nz, **base)
 
 
-CASES = [(2, 16, 12, 10), (2, 32, 32, 32), (4, 18, 24, 12), (4, 64, 48, 40)]
+# the last four cover every fixed-size non-power-of-two transform (48, 96, 160,
+# 192, 320, 384) in x and in y
+CASES = [(2, 16, 12, 10), (2, 32, 32, 32), (4, 18, 24, 12), (4, 64, 48, 40),
+         (2, 96, 96, 16), (4, 192, 160, 12), (2, 384, 48, 8), (4, 48, 320, 8)]
 
 
 @pytest.mark.parametrize("order,nx,ny,nz", CASES)

@@ -238,7 +238,9 @@ void launch_row_average_batch(const BatchLaunch& L, cudaStream_t st);
 void launch_mass_control_batch(const BatchLaunch& L, cudaStream_t st);
 void launch_div_batch(const BatchLaunch& L, int order, cudaStream_t st);
 void launch_r2c_batch(const BatchLaunch& L, int nx, cudaStream_t st);
-void launch_div_fftx_batch(const BatchLaunch& L, int order, cudaStream_t st);
+void launch_div_fftx_batch(const BatchLaunch& L, int order, int nx, cudaStream_t st);
+int fft_kernel_key(int n);                          // n with its own transform kernels, else 0
+size_t fft_generic_smem(int n, bool line_major);    // shared memory of the non-power-of-two transforms
 void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st);   // ny: power of two, else generic
 void launch_poisson_batch(const BatchLaunch& L, int order, cudaStream_t st);
 void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st);    // nx: power of two, else generic

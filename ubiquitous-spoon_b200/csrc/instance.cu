@@ -910,10 +910,11 @@ void compile(const BatchSink& K, BatchProgram& P)
 {
     auto order = [](const auto& r) { return r.G.order; };
     auto none = [](const auto&) { return 0; };
-    auto p2nx = [](const auto& r) { return batch_pow2(r.G.nx) ? r.G.nx : 0; };
-    auto p2ny = [](const auto& r) { return batch_pow2(r.G.ny) ? r.G.ny : 0; };
-    auto smem_nx = [](const auto& r) { return batch_pow2(r.G.nx) ? (size_t) 0 : fft_smem_bytes(r.G.nx); };
-    auto smem_ny = [](const auto& r) { return batch_pow2(r.G.ny) ? (size_t) 0 : fft_smem_bytes(r.G.ny); };
+    // transform kernels are per size where the size has its own kernels
+    auto keynx = [](const auto& r) { return fft_kernel_key(r.G.nx); };
+    auto keyny = [](const auto& r) { return fft_kernel_key(r.G.ny); };
+    auto smem_nx = [](const auto& r) { return batch_pow2(r.G.nx) ? (size_t) 0 : fft_generic_smem(r.G.nx, false); };
+    auto smem_ny = [](const auto& r) { return batch_pow2(r.G.ny) ? (size_t) 0 : fft_generic_smem(r.G.ny, true); };
     for (const BatchStage& S : K.stages) {
         switch (S.kind) {
         case ST_GHOSTS: add_groups(P, BK_GHOSTS, S.ghosts, order, none); break;
@@ -925,12 +926,13 @@ void compile(const BatchSink& K, BatchProgram& P)
             break;
         case ST_DIV:
             add_groups(P, BK_DIV, S.div, order, none);
-            add_groups(P, BK_R2C, S.r2c, p2nx, none);
-            add_groups(P, BK_DIV_FFTX, S.div_fftx, order, smem_nx);
+            add_groups(P, BK_R2C, S.r2c, keynx, none);
+            add_groups(P, BK_DIV_FFTX, S.div_fftx, [](const auto& r) { return 1024 * fft_kernel_key(r.G.nx) + r.G.order; },
+                       smem_nx);
             break;
-        case ST_FFTY: add_groups(P, BK_FFTY, S.ffty, p2ny, smem_ny); break;
+        case ST_FFTY: add_groups(P, BK_FFTY, S.ffty, keyny, smem_ny); break;
         case ST_POISSON: add_groups(P, BK_POISSON, S.poisson, order, none); break;
-        case ST_C2R: add_groups(P, BK_C2R, S.c2r, p2nx, smem_nx); break;
+        case ST_C2R: add_groups(P, BK_C2R, S.c2r, keynx, smem_nx); break;
         default: add_groups(P, BK_PROJECT, S.project, order, none); break;
         }
     }
@@ -957,7 +959,7 @@ void run_program(const BatchProgram& P, cudaStream_t st)
         case BK_CONTROL: launch_mass_control_batch(L, st); break;
         case BK_DIV: launch_div_batch(L, op.key, st); break;
         case BK_R2C: launch_r2c_batch(L, op.key, st); break;
-        case BK_DIV_FFTX: launch_div_fftx_batch(L, op.key, st); break;
+        case BK_DIV_FFTX: launch_div_fftx_batch(L, op.key % 1024, op.key / 1024, st); break;
         case BK_FFTY: launch_ffty_batch(L, op.key, st); break;
         case BK_POISSON: launch_poisson_batch(L, op.key, st); break;
         case BK_C2R: launch_c2r_batch(L, op.key, st); break;

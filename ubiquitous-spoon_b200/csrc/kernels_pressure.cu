@@ -16,6 +16,8 @@
 //
 // FFTs run in shared memory: a Stockham autosort mixed-radix (2/3/4/5/8)
 // transform over L lines of one thread block, twiddles from a host table.
+#include <algorithm>
+
 #include "engine.cuh"
 #include "host_band.h"
 #include "wall.cuh"
@@ -166,16 +168,131 @@ constexpr int FFT_L = 8;        // lines per block (x transforms: 8 consecutive 
 constexpr int FFT_THREADS = 256;
 constexpr int FFT_MAXC = 16;    // N * L / threads for N <= 512
 
+// ---------------------------------------------- transforms of a fixed size
+//
+// The same Stockham stages with the size known at compile time: the radix
+// sequence (that of fft_radices: 8s, then 4s, 2s, 3s, 5s), every index and
+// twiddle exponent fold to constants, and the y transforms' line-major
+// buffer is padded by one slot per 8 (plus one per line) so that the
+// first stages' strided writes spread over the banks.  Used for the sizes
+// of STATIC_FFT_SIZES; other non-power-of-two sizes take the runtime plan.
+
+__host__ __device__ constexpr int radix_count(int n)
+{
+    int c = 0;
+    while (n % 8 == 0 && n > 8) { c++; n /= 8; }
+    if (n == 8) { c++; n = 1; }
+    while (n % 4 == 0) { c++; n /= 4; }
+    while (n % 2 == 0) { c++; n /= 2; }
+    while (n % 3 == 0) { c++; n /= 3; }
+    while (n % 5 == 0) { c++; n /= 5; }
+    return c;
+}
+
+__host__ __device__ constexpr int radix_at(int n, int s)
+{
+    int c = 0;
+    while (n % 8 == 0 && n > 8) { if (c++ == s) return 8; n /= 8; }
+    if (n == 8) { if (c++ == s) return 8; n = 1; }
+    while (n % 4 == 0) { if (c++ == s) return 4; n /= 4; }
+    while (n % 2 == 0) { if (c++ == s) return 2; n /= 2; }
+    while (n % 3 == 0) { if (c++ == s) return 3; n /= 3; }
+    while (n % 5 == 0) { if (c++ == s) return 5; n /= 5; }
+    return 1;
+}
+
+template <int N>
+__host__ __device__ constexpr int lm_stride() { return N + N / 8 + 1; }
+
+// Slot of element `pos` of line `line`: line-major padded (y transforms)
+// or position-major with FFT_L interleaved lines (x transforms).
+template <int N, bool LM>
+__device__ __forceinline__ int sslot(int pos, int line)
+{
+    return LM ? line * lm_stride<N>() + pos + (pos >> 3) : pos * FFT_L + line;
+}
+
+template <int N, bool LM, int R, int NS>
+__device__ __forceinline__ void fft_stage_s(double2* buf, const FftCtx& F)
+{
+    constexpr int NR = N / R, NB = NR * FFT_L;
+    constexpr int MAXB = (NB + FFT_THREADS - 1) / FFT_THREADS;
+    constexpr int TSTEP = N / (NS * R);
+    const int tid = threadIdx.x;
+    double2 v[MAXB][R];
+#pragma unroll
+    for (int t = 0; t < MAXB; t++) {
+        const int b = tid + t * FFT_THREADS;
+        if (b < NB) {
+            const int line = LM ? b / NR : b % FFT_L;
+            const int j = LM ? b - line * NR : b / FFT_L;
+            const int k = j % NS;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                double2 a = buf[sslot<N, LM>(j + r * NR, line)];
+                if (r > 0 && k > 0) a = cmul(a, twid(F, r * k * TSTEP));
+                v[t][r] = a;
+            }
+            dft_small<R>(v[t], F);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < MAXB; t++) {
+        const int b = tid + t * FFT_THREADS;
+        if (b < NB) {
+            const int line = LM ? b / NR : b % FFT_L;
+            const int j = LM ? b - line * NR : b / FFT_L;
+            const int k = j % NS;
+            const int idxD = (j / NS) * NS * R + k;
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[sslot<N, LM>(idxD + r * NS, line)] = v[t][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int N, bool LM, int S = 0, int NS = 1>
+__device__ __forceinline__ void fft_static(double2* buf, const FftCtx& F)
+{
+    if constexpr (S < radix_count(N)) {
+        constexpr int R = radix_at(N, S);
+        fft_stage_s<N, LM, R, NS>(buf, F);
+        fft_static<N, LM, S + 1, NS * R>(buf, F);
+    }
+}
+
+// Sizes with a fixed-size transform kernel (besides the power-of-two ones).
+#define STATIC_FFT_SIZES(X) X(48) X(96) X(192) X(384) X(160) X(320)
+
+static bool static_fft_size(int n)
+{
+#define CASE_(n_) case n_:
+    switch (n) {
+    STATIC_FFT_SIZES(CASE_) return true;
+    default: return false;
+    }
+#undef CASE_
+}
+
+// Dynamic shared memory of the generic transforms of size n.
+size_t fft_generic_smem(int n, bool line_major)
+{
+    if (static_fft_size(n) && line_major) return (size_t) FFT_L * (n + n / 8 + 1) * sizeof(double2);
+    return (size_t) n * FFT_L * sizeof(double2);
+}
+
 // --------------------------------------------------------- divergence + x FFT
 
 
-template <int ORDER>
+// N: the transform size when it is fixed at compile time, 0 for the runtime plan
+template <int ORDER, int N>
 __device__ __forceinline__ void k_div_fftx_body(const Geo& G, const DivArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
     const int k = GZ + bid.y;
     const int j0 = bid.x * FFT_L;
-    const int nx = G.nx, ny = G.ny, n2 = G.n2;
+    const int nx = N ? N : G.nx, ny = G.ny, n2 = G.n2;
     const double dx = G.dx, dy = G.dy, dzk = G.dz[k];
     const double uc = A.mu ? A.gu[k] * (*A.mu) : 0.0;   // chanfast.c:516-519
     const bool corr = A.mu != nullptr;
@@ -202,7 +319,8 @@ __device__ __forceinline__ void k_div_fftx_body(const Geo& G, const DivArgs& A, 
     }
     __syncthreads();
     FftCtx F{sbuf, nx, FFT_L, false, -1, A.px.tw, A.c8};
-    fft_run<FFT_MAXC>(F, A.px);
+    if constexpr (N > 0) fft_static<N, false>(sbuf, F);
+    else fft_run<FFT_MAXC>(F, A.px);
     const int nkx = G.nkx;
     const double scale = 1.0 / (double) nx;
     for (int idx = threadIdx.x; idx < nkx * FFT_L; idx += blockDim.x) {
@@ -215,67 +333,80 @@ __device__ __forceinline__ void k_div_fftx_body(const Geo& G, const DivArgs& A, 
     }
 }
 
-template <int ORDER>
+template <int ORDER, int N>
 __global__ void __launch_bounds__(FFT_THREADS) k_div_fftx(Geo G, DivArgs A)
 {
-    k_div_fftx_body<ORDER>(G, A, blockIdx);
+    k_div_fftx_body<ORDER, N>(G, A, blockIdx);
 }
 
-template <int ORDER>
+template <int ORDER, int N>
 __global__ void __launch_bounds__(FFT_THREADS) k_div_fftx_batch(const BatchRec<DivArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<DivArgs>& R = batch_locate(r, n, b);
-    k_div_fftx_body<ORDER>(R.G, R.A, b);
+    k_div_fftx_body<ORDER, N>(R.G, R.A, b);
 }
 
 // ------------------------------------------------------------------ y FFT
 
 
+template <int N>
 __device__ __forceinline__ void k_ffty_body(const Geo& G, const FftyArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
     const int k = A.kfirst + bid.y;
     const int kx0 = bid.x * FFT_L;
-    const int ny = G.ny, nkx = G.nkx;
+    const int ny = N ? N : G.ny, nkx = G.nkx;
     const int nl = min(FFT_L, nkx - kx0);
     double2* base = A.spec + bid.z * A.fstride + ((long long) k * nkx + kx0) * ny;
+    auto slot = [&](int idx) {   // idx = line * ny + pos
+        if constexpr (N > 0) {
+            const int line = idx / N, pos = idx - line * N;
+            return sslot<N, true>(pos, line);
+        } else {
+            return idx;
+        }
+    };
     for (int idx = threadIdx.x; idx < FFT_L * ny; idx += blockDim.x) {
         int line = idx / ny;
-        sbuf[idx] = line < nl ? base[idx] : make_double2(0.0, 0.0);
+        sbuf[slot(idx)] = line < nl ? base[idx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
     FftCtx F{sbuf, ny, FFT_L, true, A.sign, A.py.tw, A.c8};
-    fft_run<FFT_MAXC>(F, A.py);
+    if constexpr (N > 0) fft_static<N, true>(sbuf, F);
+    else fft_run<FFT_MAXC>(F, A.py);
     const double scale = 1.0 / (double) ny;
     for (int idx = threadIdx.x; idx < nl * ny; idx += blockDim.x) {
-        double2 t = sbuf[idx];
+        double2 t = sbuf[slot(idx)];
         if (A.sign < 0) { t.x *= scale; t.y *= scale; }
         base[idx] = t;
     }
 }
 
+template <int N>
 __global__ void __launch_bounds__(FFT_THREADS) k_ffty(Geo G, FftyArgs A)
 {
-    k_ffty_body(G, A, blockIdx);
+    k_ffty_body<N>(G, A, blockIdx);
 }
 
+template <int N>
 __global__ void __launch_bounds__(FFT_THREADS) k_ffty_batch(const BatchRec<FftyArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<FftyArgs>& R = batch_locate(r, n, b);
-    k_ffty_body(R.G, R.A, b);
+    k_ffty_body<N>(R.G, R.A, b);
 }
 
 // ---------------------------------------------------------- inverse x FFT
 
 
+template <int N>
 __device__ __forceinline__ void k_fftx_c2r_body(const Geo& G, const C2rArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
     const int k = A.kfirst + bid.y;
     const int j0 = bid.x * FFT_L;
-    const int nx = G.nx, ny = G.ny, nkx = G.nkx;
+    const int nx = N ? N : G.nx, ny = G.ny, nkx = G.nkx;
     const double2* spec = A.spec + bid.z * A.fstride;
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int pos = idx / FFT_L, jj = idx - pos * FFT_L, j = j0 + jj;
@@ -293,23 +424,26 @@ __device__ __forceinline__ void k_fftx_c2r_body(const Geo& G, const C2rArgs& A, 
     }
     __syncthreads();
     FftCtx F{sbuf, nx, FFT_L, false, +1, A.px.tw, A.c8};
-    fft_run<FFT_MAXC>(F, A.px);
+    if constexpr (N > 0) fft_static<N, false>(sbuf, F);
+    else fft_run<FFT_MAXC>(F, A.px);
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
         if (j < ny) A.p[bid.z][((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
     }
 }
 
+template <int N>
 __global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r(Geo G, C2rArgs A)
 {
-    k_fftx_c2r_body(G, A, blockIdx);
+    k_fftx_c2r_body<N>(G, A, blockIdx);
 }
 
+template <int N>
 __global__ void __launch_bounds__(FFT_THREADS) k_fftx_c2r_batch(const BatchRec<C2rArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<C2rArgs>& R = batch_locate(r, n, b);
-    k_fftx_c2r_body(R.G, R.A, b);
+    k_fftx_c2r_body<N>(R.G, R.A, b);
 }
 
 // ------------------------------------------------------------ Poisson in z
@@ -1075,8 +1209,18 @@ void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st)
     }
     dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.nz);
     size_t sm = fft_smem_bytes(G.nx);
-    if (G.order == 2) k_div_fftx<2><<<grd, FFT_THREADS, sm, st>>>(G, A);
-    else k_div_fftx<4><<<grd, FFT_THREADS, sm, st>>>(G, A);
+#define CASE_(n_) \
+    case n_: \
+        if (G.order == 2) k_div_fftx<2, n_><<<grd, FFT_THREADS, sm, st>>>(G, A); \
+        else k_div_fftx<4, n_><<<grd, FFT_THREADS, sm, st>>>(G, A); \
+        return;
+    switch (G.nx) {
+    STATIC_FFT_SIZES(CASE_)
+    default: break;
+    }
+#undef CASE_
+    if (G.order == 2) k_div_fftx<2, 0><<<grd, FFT_THREADS, sm, st>>>(G, A);
+    else k_div_fftx<4, 0><<<grd, FFT_THREADS, sm, st>>>(G, A);
 }
 
 bool fftx_batched_supported(int nx)
@@ -1105,7 +1249,15 @@ void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st, in
     default: break;
     }
     dim3 grd((G.nkx + FFT_L - 1) / FFT_L, nrows, nfields);
-    k_ffty<<<grd, FFT_THREADS, fft_smem_bytes(G.ny), st>>>(G, A);
+    const size_t sm = fft_generic_smem(G.ny, true);
+#define CASE_(n_) \
+    case n_: k_ffty<n_><<<grd, FFT_THREADS, sm, st>>>(G, A); return;
+    switch (G.ny) {
+    STATIC_FFT_SIZES(CASE_)
+    default: break;
+    }
+#undef CASE_
+    k_ffty<0><<<grd, FFT_THREADS, sm, st>>>(G, A);
 }
 
 void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st, int nfields)
@@ -1118,7 +1270,15 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st,
     default: break;
     }
     dim3 grd((G.ny + FFT_L - 1) / FFT_L, nrows, nfields);
-    k_fftx_c2r<<<grd, FFT_THREADS, fft_smem_bytes(G.nx), st>>>(G, A);
+    const size_t sm = fft_smem_bytes(G.nx);
+#define CASE_(n_) \
+    case n_: k_fftx_c2r<n_><<<grd, FFT_THREADS, sm, st>>>(G, A); return;
+    switch (G.nx) {
+    STATIC_FFT_SIZES(CASE_)
+    default: break;
+    }
+#undef CASE_
+    k_fftx_c2r<0><<<grd, FFT_THREADS, sm, st>>>(G, A);
 }
 
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
@@ -1200,10 +1360,21 @@ void launch_r2c_batch(const BatchLaunch& L, int nx, cudaStream_t st)
     }
 }
 
-void launch_div_fftx_batch(const BatchLaunch& L, int order, cudaStream_t st)
+void launch_div_fftx_batch(const BatchLaunch& L, int order, int nx, cudaStream_t st)
 {
-    if (order == 2) k_div_fftx_batch<2><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<DivArgs>(L), L.n);
-    else k_div_fftx_batch<4><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<DivArgs>(L), L.n);
+    auto r = recs_of<DivArgs>(L);
+#define CASE_(n_) \
+    case n_: \
+        if (order == 2) k_div_fftx_batch<2, n_><<<L.blocks, FFT_THREADS, L.smem, st>>>(r, L.n); \
+        else k_div_fftx_batch<4, n_><<<L.blocks, FFT_THREADS, L.smem, st>>>(r, L.n); \
+        return;
+    switch (nx) {
+    STATIC_FFT_SIZES(CASE_)
+    default: break;
+    }
+#undef CASE_
+    if (order == 2) k_div_fftx_batch<2, 0><<<L.blocks, FFT_THREADS, L.smem, st>>>(r, L.n);
+    else k_div_fftx_batch<4, 0><<<L.blocks, FFT_THREADS, L.smem, st>>>(r, L.n);
 }
 
 void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st)
@@ -1213,7 +1384,11 @@ void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st)
     case 128: k_ffty_p2_batch<128><<<L.blocks, 256, p2_smem_y<128>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
     case 256: k_ffty_p2_batch<256><<<L.blocks, 256, p2_smem_y<256>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
     case 512: k_ffty_p2_batch<512><<<L.blocks, 256, p2_smem_y<512>(), st>>>(recs_of<FftyArgs>(L), L.n); break;
-    default: k_ffty_batch<<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<FftyArgs>(L), L.n); break;
+#define CASE_(n_) \
+    case n_: k_ffty_batch<n_><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<FftyArgs>(L), L.n); break;
+    STATIC_FFT_SIZES(CASE_)
+#undef CASE_
+    default: k_ffty_batch<0><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<FftyArgs>(L), L.n); break;
     }
 }
 
@@ -1230,7 +1405,11 @@ void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st)
     case 128: k_fftx_c2r_p2_batch<128><<<L.blocks, 256, p2_smem_x<64>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
     case 256: k_fftx_c2r_p2_batch<256><<<L.blocks, 256, p2_smem_x<128>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
     case 512: k_fftx_c2r_p2_batch<512><<<L.blocks, 256, p2_smem_x<256>(), st>>>(recs_of<C2rArgs>(L), L.n); break;
-    default: k_fftx_c2r_batch<<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<C2rArgs>(L), L.n); break;
+#define CASE_(n_) \
+    case n_: k_fftx_c2r_batch<n_><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<C2rArgs>(L), L.n); break;
+    STATIC_FFT_SIZES(CASE_)
+#undef CASE_
+    default: k_fftx_c2r_batch<0><<<L.blocks, FFT_THREADS, L.smem, st>>>(recs_of<C2rArgs>(L), L.n); break;
     }
 }
 
@@ -1243,6 +1422,8 @@ void launch_project_batch(const BatchLaunch& L, int order, cudaStream_t st)
 
 bool batch_pow2(int n) { return pow2_kernel_size(n); }
 
+int fft_kernel_key(int n) { return pow2_kernel_size(n) || static_fft_size(n) ? n : 0; }
+
 cudaError_t fft_set_smem_limits(int max_n)
 {
     size_t sm = fft_smem_bytes(max_n);
@@ -1250,20 +1431,21 @@ cudaError_t fft_set_smem_limits(int max_n)
     if (e == cudaSuccess) e = p2_set_smem<128>();
     if (e == cudaSuccess) e = p2_set_smem<256>();
     if (e == cudaSuccess) e = p2_set_smem<512>();
-    if (e == cudaSuccess && sm > 48 * 1024) {
-        int v = (int) sm;
-        e = cudaFuncSetAttribute(k_div_fftx<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    }
-    if (e == cudaSuccess) {   // batched generic transforms: room for the largest size
-        int v = (int) fft_smem_bytes(FFT_MAX_N);
-        e = cudaFuncSetAttribute(k_div_fftx_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_div_fftx_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    }
+    (void) sm;
+    // generic transforms (single and batched): room for the largest size
+    // handled by the runtime plan and for the padded fixed-size buffers
+    const int v = (int) std::max(fft_smem_bytes(FFT_MAX_N), fft_generic_smem(384, true));
+    auto set = [&](const void* f) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    };
+#define SET_(n_) \
+    set((const void*) k_div_fftx<2, n_>); set((const void*) k_div_fftx<4, n_>); \
+    set((const void*) k_ffty<n_>); set((const void*) k_fftx_c2r<n_>); \
+    set((const void*) k_div_fftx_batch<2, n_>); set((const void*) k_div_fftx_batch<4, n_>); \
+    set((const void*) k_ffty_batch<n_>); set((const void*) k_fftx_c2r_batch<n_>);
+    SET_(0)
+    STATIC_FFT_SIZES(SET_)
+#undef SET_
     return e;
 }
 
