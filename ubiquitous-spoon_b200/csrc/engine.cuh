@@ -181,10 +181,10 @@ struct PoissonArgs {
     double abc_bot, abc_top;  // and its wall values
 };
 
-constexpr int POIS_THREADS = 128;  // k_poisson block: one thread per (kx, ky) column
-constexpr int POIS_PF = 8;         // forward rows in flight per thread
+constexpr int POIS_THREADS = 128;  // k_poisson block: one thread per (kx, +-ky) column pair
+constexpr int POIS_PF = 8;         // forward rows in flight per thread (both columns)
 constexpr int POIS_PB = 2;         // back-substitution rows loaded ahead (registers)
-inline size_t pois_smem_bytes() { return (size_t) POIS_PF * POIS_THREADS * 16; }
+inline size_t pois_smem_bytes() { return (size_t) POIS_PF * 2 * POIS_THREADS * 16; }
 
 struct ProjArgs {
     double *u, *v, *w, *c;

@@ -514,28 +514,38 @@ __device__ void average_walls(const PoissonArgs& A, int n2)
     if (ORDER == 4) { avg[kt + 1] = g2; avg[kt + 2] = g3; }
 }
 
-// Banded solve of one (kx, ky) column over spectrum rows GZ .. GZ+n-1:
-// pressure_poisson{2,4} (pressure.c:293-443) with FILL (the wall ghost rows
-// of the solution are filled from the closure, as p needs them), or
-// solve_helmholtz_{u,w}{2,4} (diffuseu.c:398-614, diffusew.c:466-614) without
-// (the field's apply_bc follows the inverse transform).  One thread per
-// column, Re and Im sharing one factorisation.
+// Banded solve of a pair of (kx, ky) columns over spectrum rows
+// GZ .. GZ+n-1: pressure_poisson{2,4} (pressure.c:293-443) with FILL (the
+// wall ghost rows of the solution are filled from the closure, as p needs
+// them), or solve_helmholtz_{u,w}{2,4} (diffuseu.c:398-614,
+// diffusew.c:466-614) without (the field's apply_bc follows the inverse
+// transform).  The band matrix depends on ky only through cos(2 pi ky / ny),
+// so columns ky and ny - ky share one factorisation: one thread per pair
+// eliminates both (Re and Im of each), storing the multipliers once.  ky = 0
+// and, for even ny, ky = ny/2 pair with themselves (solved twice, stored
+// identically).
 template <int ORDER, bool FILL>
 __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, uint3 bid)
 {
     const long long ncol = G.splane;
-    const long long col = (long long) bid.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
     const int ny = G.ny, n2 = G.n2, n = A.nrows;
-    const int kx = (int) (col / ny), ky = (int) (col - (long long) kx * ny);
+    const int nky = ny / 2 + 1;                       // pairs per kx
+    const long long npair = (long long) G.nkx * nky;
+    const long long pair = (long long) bid.x * blockDim.x + threadIdx.x;
+    if (pair >= npair) return;
+    const int kx = (int) (pair / nky), ky = (int) (pair - (long long) kx * nky);
+    const int kyb = (ny - ky) % ny;
+    const long long colA = (long long) kx * ny + ky, colB = (long long) kx * ny + kyb;
     const int var = (kx == 0 && ky == 0) ? 1 : 0;   // pressure.c:331-338
     const double lamx = A.lamx[kx], lamy = A.lamy[ky];
-    const bool stats = !FILL && A.avg != nullptr && col == 0;
+    const bool stats = !FILL && A.avg != nullptr && pair == 0;
     double2* sp = A.spec;
-    auto S = [&](int k) -> double2& { return sp[(long long) k * ncol + col]; };
+    auto SA = [&](int k) -> double2& { return sp[(long long) k * ncol + colA]; };
+    auto SB = [&](int k) -> double2& { return sp[(long long) k * ncol + colB]; };
     auto bq = [&](int i) { return i < 3 ? i : (i >= n - 3 ? 6 - (n - i) : -1); };
+    auto scal = [](double2 v, double f) { return make_double2(v.x * f, v.y * f); };
 
-    // Coefficients of interior row i (k = GZ + i) for this column.
+    // Coefficients of interior row i (k = GZ + i) for this pair.
     auto coef = [&](int i, double* cf) {
         const int k = GZ + i;
         const int q = bq(i);
@@ -549,6 +559,7 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
         }
         cf[3] = d;
     };
+    auto at = [&](double* base, int k) -> double& { return base[(long long) k * npair + pair]; };
 
     if (ORDER == 2) {
         // tridag.c:4-26; the diagonal is cf[3], the off-diagonals cf[0], cf[2]
@@ -556,88 +567,103 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
         double cfv[7];
         coef(0, cfv);
         double ibet = 1.0 / cfv[3];
-        double2 r0 = S(GZ);
         const double dv0 = A.dvol[GZ];
-        double2 u = make_double2(r0.x * dv0 * ibet, r0.y * dv0 * ibet);
-        S(GZ) = u;
+        const double2 r0A = SA(GZ), r0B = SB(GZ);
+        double2 uA = make_double2(r0A.x * dv0 * ibet, r0A.y * dv0 * ibet);
+        double2 uB = make_double2(r0B.x * dv0 * ibet, r0B.y * dv0 * ibet);
+        SA(GZ) = uA;
+        SB(GZ) = uB;
         double cprev = cfv[2];
         for (int i = 1; i < n; i++) {
             const int k = GZ + i;
             coef(i, cfv);
             double gm = cprev * ibet;
             ibet = 1.0 / (cfv[3] - cfv[0] * gm);
-            gam[(long long) k * ncol + col] = gm;
-            double2 r = S(k);
+            at(gam, k) = gm;
             const double dv = A.dvol[k];
-            u = make_double2((r.x * dv - cfv[0] * u.x) * ibet, (r.y * dv - cfv[0] * u.y) * ibet);
-            S(k) = u;
+            const double2 rA = SA(k), rB = SB(k);
+            uA = make_double2((rA.x * dv - cfv[0] * uA.x) * ibet, (rA.y * dv - cfv[0] * uA.y) * ibet);
+            uB = make_double2((rB.x * dv - cfv[0] * uB.x) * ibet, (rB.y * dv - cfv[0] * uB.y) * ibet);
+            SA(k) = uA;
+            SB(k) = uB;
             cprev = cfv[2];
         }
-        double2 nxt = u;
-        double2 top1 = u;
-        double2 b0 = u;
-        if (stats) A.avg[GZ + n - 1] = u.x;
+        double2 nA = uA, nB = uB;
+        const double2 topA = uA, topB = uB;
+        double2 b0A = uA, b0B = uB;
+        if (stats) A.avg[GZ + n - 1] = uA.x;
         for (int i = n - 2; i >= 0; i--) {
             const int k = GZ + i;
-            double gm = gam[(long long) (k + 1) * ncol + col];
-            double2 t = S(k);
-            t.x -= gm * nxt.x;
-            t.y -= gm * nxt.y;
-            S(k) = t;
-            nxt = t;
-            if (stats) A.avg[k] = t.x;
-            if (i == 0) b0 = t;
+            const double gm = at(gam, k + 1);
+            double2 tA = SA(k), tB = SB(k);
+            tA.x -= gm * nA.x;
+            tA.y -= gm * nA.y;
+            tB.x -= gm * nB.x;
+            tB.y -= gm * nB.y;
+            SA(k) = tA;
+            SB(k) = tB;
+            nA = tA;
+            nB = tB;
+            if (stats) A.avg[k] = tA.x;
+            if (i == 0) { b0A = tA; b0B = tB; }
         }
-        if (n == 1) b0 = top1;
         if (FILL) {
-            double g1, g2, g3;
-            fill_bot<2>(A.bot[var], b0.x, 0.0, 0.0, g1, g2, g3);
-            double h1;
-            fill_bot<2>(A.bot[var], b0.y, 0.0, 0.0, h1, g2, g3);
-            S(GZ - 1) = make_double2(g1, h1);
-            fill_top<2>(A.top, top1.x, 0.0, 0.0, g1, g2, g3);
-            fill_top<2>(A.top, top1.y, 0.0, 0.0, h1, g2, g3);
-            S(n2 - GZ) = make_double2(g1, h1);
-            for (int k = 0; k < GZ - 1; k++) S(k) = make_double2(0.0, 0.0);
-            for (int k = n2 - GZ + 1; k < n2; k++) S(k) = make_double2(0.0, 0.0);
+            auto fill = [&](auto S, double2 b0, double2 top) {
+                double g1, g2, g3, h1;
+                fill_bot<2>(A.bot[var], b0.x, 0.0, 0.0, g1, g2, g3);
+                fill_bot<2>(A.bot[var], b0.y, 0.0, 0.0, h1, g2, g3);
+                S(GZ - 1) = make_double2(g1, h1);
+                fill_top<2>(A.top, top.x, 0.0, 0.0, g1, g2, g3);
+                fill_top<2>(A.top, top.y, 0.0, 0.0, h1, g2, g3);
+                S(n2 - GZ) = make_double2(g1, h1);
+                for (int k = 0; k < GZ - 1; k++) S(k) = make_double2(0.0, 0.0);
+                for (int k = n2 - GZ + 1; k < n2; k++) S(k) = make_double2(0.0, 0.0);
+            };
+            fill(SA, b0A, topA);
+            fill(SB, b0B, topB);
         } else {
-            if (GZ + n < n2 - GZ) S(GZ + n) = make_double2(0.0, 0.0);   // w: the top wall face
+            if (GZ + n < n2 - GZ) {   // w: the top wall face
+                SA(GZ + n) = make_double2(0.0, 0.0);
+                SB(GZ + n) = make_double2(0.0, 0.0);
+            }
             if (stats) average_walls<2>(A, n2);
         }
         return;
     }
 
-    // heptdag.c:5-61 with per-column pivots; p, q, r spill to scratch.  One
+    // heptdag.c:5-61 with per-pair pivots; p, q, r spill to scratch.  One
     // elimination formula serves every row: with zero history (p, q, r, s of
     // rows -3..-1) it reduces exactly to the special forms of rows 0..2.
     // In the forward sweep each thread keeps the spectrum values of the next
-    // POIS_PF rows in flight as cp.async copies into its own slots of a
-    // shared-memory ring; none of those rows has been rewritten yet.
+    // POIS_PF rows of both columns in flight as cp.async copies into its own
+    // slots of a shared-memory ring; none of those rows has been rewritten yet.
     double* Pp = A.scratch;
-    double* Qp = A.scratch + (long long) n2 * ncol;
-    double* Rp = A.scratch + 2 * (long long) n2 * ncol;
-    auto at = [&](double* base, int k) -> double& { return base[(long long) k * ncol + col]; };
+    double* Qp = A.scratch + (long long) n2 * npair;
+    double* Rp = A.scratch + 2 * (long long) n2 * npair;
     extern __shared__ double2 pring[];
     const int t = threadIdx.x;
-    auto fslot = [&](int i) { return pring + (i % POIS_PF) * POIS_THREADS + t; };
+    auto fslot = [&](int i, int c) { return pring + ((i % POIS_PF) * 2 + c) * POIS_THREADS + t; };
     auto ffetch = [&](int i) {
-        if (i < n) cp_async16_ordered(fslot(i), &S(GZ + i));
+        if (i < n) {
+            cp_async16_ordered(fslot(i, 0), &SA(GZ + i));
+            cp_async16_ordered(fslot(i, 1), &SB(GZ + i));
+        }
         cp_async_commit_ordered();
     };
     for (int i = 0; i < POIS_PF; i++) ffetch(i);
     double p3 = 0, q3 = 0, r3 = 0, p2 = 0, q2 = 0, r2 = 0, p1 = 0, q1 = 0, r1 = 0;   // rows i-3, i-2, i-1
-    double2 s3 = make_double2(0, 0), s2 = s3, s1 = s3;
+    double2 s3A = make_double2(0, 0), s2A = s3A, s1A = s3A, s3B = s3A, s2B = s3A, s1B = s3A;
     double cf[7];
     for (int i = 0; i < n; i++) {
         const int k = GZ + i;
         cp_async_wait_ordered<POIS_PF - 1>();
-        double2 h = *fslot(i);
+        double2 hA = *fslot(i, 0), hB = *fslot(i, 1);
         ffetch(i + POIS_PF);
         coef(i, cf);
         const double a = cf[0], b = cf[1], c = cf[2], d = cf[3], e = cf[4], f = cf[5], g = cf[6];
         const double dv = A.dvol[k];
-        h.x = h.x * dv;
-        h.y = h.y * dv;
+        hA = scal(hA, dv);
+        hB = scal(hB, dv);
         const double alp = b - a * p3;
         const double bet = c - a * q3 - alp * p2;
         const double den = d - a * r3 - alp * q2 - bet * p1;
@@ -645,79 +671,95 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
         const double p = (e - alp * r2 - bet * q1) * iden;
         const double q = (f - bet * r1) * iden;
         const double r = g * iden;
-        const double2 sv = make_double2((h.x - a * s3.x - alp * s2.x - bet * s1.x) * iden,
-                                        (h.y - a * s3.y - alp * s2.y - bet * s1.y) * iden);
+        const double2 svA = make_double2((hA.x - a * s3A.x - alp * s2A.x - bet * s1A.x) * iden,
+                                         (hA.y - a * s3A.y - alp * s2A.y - bet * s1A.y) * iden);
+        const double2 svB = make_double2((hB.x - a * s3B.x - alp * s2B.x - bet * s1B.x) * iden,
+                                         (hB.y - a * s3B.y - alp * s2B.y - bet * s1B.y) * iden);
         at(Pp, k) = p; at(Qp, k) = q; at(Rp, k) = r;
-        S(k) = sv;
+        SA(k) = svA;
+        SB(k) = svB;
         p3 = p2; q3 = q2; r3 = r2; p2 = p1; q2 = q1; r2 = r1; p1 = p; q1 = q; r1 = r;
-        s3 = s2; s2 = s1; s1 = sv;
+        s3A = s2A; s2A = s1A; s1A = svA;
+        s3B = s2B; s2B = s1B; s1B = svB;
     }
     cp_async_wait_ordered<0>();
 
     // back substitution (heptdag.c:50-55), same general form (x2 = x3 = 0 at
     // the top).  s, p, q, r of row i - POIS_PB are loaded into registers while
     // row i is computed (plain loads: these rows were stored by this thread).
-    double2 ls[POIS_PB];
+    double2 lsA[POIS_PB], lsB[POIS_PB];
     double lp[POIS_PB], lq[POIS_PB], lr[POIS_PB];
     auto bload = [&](int i, int u) {
         if (i >= 0) {
             const int k = GZ + i;
-            ls[u] = S(k); lp[u] = at(Pp, k); lq[u] = at(Qp, k); lr[u] = at(Rp, k);
+            lsA[u] = SA(k); lsB[u] = SB(k); lp[u] = at(Pp, k); lq[u] = at(Qp, k); lr[u] = at(Rp, k);
         }
     };
 #pragma unroll
     for (int u = 0; u < POIS_PB; u++) bload(n - 2 - u, u);
-    double2 x1 = S(GZ + n - 1), x2 = make_double2(0, 0), x3 = x2;
-    if (stats) A.avg[GZ + n - 1] = x1.x;
+    double2 x1A = SA(GZ + n - 1), x2A = make_double2(0, 0), x3A = x2A;
+    double2 x1B = SB(GZ + n - 1), x2B = x2A, x3B = x2A;
+    if (stats) A.avg[GZ + n - 1] = x1A.x;
     for (int i0 = n - 2; i0 >= 0; i0 -= POIS_PB) {
 #pragma unroll
         for (int u = 0; u < POIS_PB; u++) {
             const int i = i0 - u;
             if (i >= 0) {
-                const double2 sv = ls[u];
+                const double2 svA = lsA[u], svB = lsB[u];
                 const double p = lp[u], q = lq[u], r = lr[u];
                 bload(i - POIS_PB, u);
-                const double2 xv = make_double2(sv.x - p * x1.x - q * x2.x - r * x3.x,
-                                                sv.y - p * x1.y - q * x2.y - r * x3.y);
-                S(GZ + i) = xv;
-                if (stats) A.avg[GZ + i] = xv.x;
-                x3 = x2; x2 = x1; x1 = xv;
+                const double2 xA = make_double2(svA.x - p * x1A.x - q * x2A.x - r * x3A.x,
+                                                svA.y - p * x1A.y - q * x2A.y - r * x3A.y);
+                const double2 xB = make_double2(svB.x - p * x1B.x - q * x2B.x - r * x3B.x,
+                                                svB.y - p * x1B.y - q * x2B.y - r * x3B.y);
+                SA(GZ + i) = xA;
+                SB(GZ + i) = xB;
+                if (stats) A.avg[GZ + i] = xA.x;
+                x3A = x2A; x2A = x1A; x1A = xA;
+                x3B = x2B; x2B = x1B; x1B = xB;
             }
         }
     }
     if (!FILL) {
-        if (GZ + n < n2 - GZ) S(GZ + n) = make_double2(0.0, 0.0);   // w: the top wall face
+        if (GZ + n < n2 - GZ) {   // w: the top wall face
+            SA(GZ + n) = make_double2(0.0, 0.0);
+            SB(GZ + n) = make_double2(0.0, 0.0);
+        }
         if (stats) average_walls<4>(A, n2);
         return;
     }
     // wall rows of the solution: bottom rows 0..2 are the last three results,
     // top rows n-1..n-3 are read back
-    double2 bt[3] = {x1, x2, x3};
-    if (n < 3)
-        for (int i = 0; i < 3; i++) bt[i] = i < n ? S(GZ + i) : make_double2(0.0, 0.0);
-    double2 tp[3];
-    for (int i = 0; i < 3; i++) tp[i] = n - 1 - i >= 0 ? S(GZ + n - 1 - i) : make_double2(0.0, 0.0);
-    double g1, g2, g3, h1, h2, h3;
-    fill_bot<4>(A.bot[var], bt[0].x, bt[1].x, bt[2].x, g1, g2, g3);
-    fill_bot<4>(A.bot[var], bt[0].y, bt[1].y, bt[2].y, h1, h2, h3);
-    S(GZ - 1) = make_double2(g1, h1);
-    S(GZ - 2) = make_double2(g2, h2);
-    S(GZ - 3) = make_double2(g3, h3);
-    fill_top<4>(A.top, tp[0].x, tp[1].x, tp[2].x, g1, g2, g3);
-    fill_top<4>(A.top, tp[0].y, tp[1].y, tp[2].y, h1, h2, h3);
-    S(n2 - GZ) = make_double2(g1, h1);
-    S(n2 - GZ + 1) = make_double2(g2, h2);
-    S(n2 - GZ + 2) = make_double2(g3, h3);
+    auto fill = [&](auto S, double2 x1, double2 x2, double2 x3) {
+        double2 bt[3] = {x1, x2, x3};
+        if (n < 3)
+            for (int i = 0; i < 3; i++) bt[i] = i < n ? S(GZ + i) : make_double2(0.0, 0.0);
+        double2 tp[3];
+        for (int i = 0; i < 3; i++) tp[i] = n - 1 - i >= 0 ? S(GZ + n - 1 - i) : make_double2(0.0, 0.0);
+        double g1, g2, g3, h1, h2, h3;
+        fill_bot<4>(A.bot[var], bt[0].x, bt[1].x, bt[2].x, g1, g2, g3);
+        fill_bot<4>(A.bot[var], bt[0].y, bt[1].y, bt[2].y, h1, h2, h3);
+        S(GZ - 1) = make_double2(g1, h1);
+        S(GZ - 2) = make_double2(g2, h2);
+        S(GZ - 3) = make_double2(g3, h3);
+        fill_top<4>(A.top, tp[0].x, tp[1].x, tp[2].x, g1, g2, g3);
+        fill_top<4>(A.top, tp[0].y, tp[1].y, tp[2].y, h1, h2, h3);
+        S(n2 - GZ) = make_double2(g1, h1);
+        S(n2 - GZ + 1) = make_double2(g2, h2);
+        S(n2 - GZ + 2) = make_double2(g3, h3);
+    };
+    fill(SA, x1A, x2A, x3A);
+    fill(SB, x1B, x2B, x3B);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson(Geo G, PoissonArgs A)
+__global__ void __launch_bounds__(POIS_THREADS, 4) k_poisson(Geo G, PoissonArgs A)
 {
     band_column<ORDER, true>(G, A, blockIdx);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson_batch(const BatchRec<PoissonArgs>* r, int n)
+__global__ void __launch_bounds__(POIS_THREADS, 4) k_poisson_batch(const BatchRec<PoissonArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<PoissonArgs>& R = batch_locate(r, n, b);
@@ -725,7 +767,7 @@ __global__ void __launch_bounds__(POIS_THREADS, 7) k_poisson_batch(const BatchRe
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 7) k_helmholtz_spectral(Geo G, PoissonArgs A)
+__global__ void __launch_bounds__(POIS_THREADS, 4) k_helmholtz_spectral(Geo G, PoissonArgs A)
 {
     band_column<ORDER, false>(G, A, blockIdx);
 }
@@ -1283,14 +1325,14 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st,
 
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
 {
-    unsigned nb = (unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS);
+    unsigned nb = grid_poisson(G).x;
     if (G.order == 2) k_poisson<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
     else k_poisson<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
 }
 
 void launch_helmholtz_spectral(const Geo& G, const PoissonArgs& A, cudaStream_t st)
 {
-    unsigned nb = (unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS);
+    unsigned nb = grid_poisson(G).x;
     if (G.order == 2) k_helmholtz_spectral<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
     else k_helmholtz_spectral<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
 }
@@ -1336,7 +1378,12 @@ dim3 grid_c2r(const Geo& G, int nrows, int nfields)
     return dim3((G.ny + L - 1) / L, nrows, nfields);
 }
 
-dim3 grid_poisson(const Geo& G) { return dim3((unsigned) ((G.splane + POIS_THREADS - 1) / POIS_THREADS)); }
+// one thread per pair of columns (kx, ky), (kx, ny - ky)
+dim3 grid_poisson(const Geo& G)
+{
+    const long long npair = (long long) G.nkx * (G.ny / 2 + 1);
+    return dim3((unsigned) ((npair + POIS_THREADS - 1) / POIS_THREADS));
+}
 
 dim3 grid_project(const Geo& G) { return dim3((G.ny + 31) / 32, (G.nx + 3) / 4, G.n2); }
 

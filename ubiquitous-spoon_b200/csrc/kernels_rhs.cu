@@ -119,7 +119,7 @@ constexpr double L1 = A1 * A1 - 2.0 * A1 * A2, L2 = 2.0 * A1 * A2, L3 = A2 * A2;
 constexpr int RT_FIELD = RT_SLOTS * RT_PLANE;                      // one field's ring
 constexpr int RT_LOADS = (RT_PLANE + RT_THREADS - 1) / RT_THREADS;  // plane points per thread
 
-constexpr int RT_FWMAX = 13;   // widest fused forward row (order 4)
+constexpr int RT_FWMAX = 14;   // widest fused forward row (order 4: 13), padded to 16-byte pairs
 // ring of haloed planes + two rows of each thread's g values + two rows of
 // the four fused coefficient rows
 size_t rhs_smem_bytes()
@@ -280,10 +280,16 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 
     const double qk = -0.125;   // QUICK coefficient (scalar.c:79-162)
     auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
+        // the upwind curvature x - 2y + z: (c1, c0, cm1) for m > 0, else
+        // (c2, c1, c0); the operands are chosen first, then one evaluation
+        const bool up = m > 0.0;
+        const double x = up ? c1 : c2, y = up ? c0 : c1, z = up ? cm1 : c0;
         double cph = 0.5 * (c0 + c1);
-        cph += m > 0.0 ? qk * (c1 - 2.0 * c0 + cm1) : qk * (c2 - 2.0 * c1 + c0);
+        cph += qk * (x - 2.0 * y + z);
         return m * cph;
     };
+    // add_buoyancy is skipped when every betg is zero (adding exact zeros)
+    const bool buoyancy = A.betg_x != 0.0 || A.betg_y != 0.0 || A.betg_z != 0.0;
 
     // z fluxes carried up the column: the queues and the scalar flux
     // through the bottom face, primed for the first row.
@@ -308,7 +314,16 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     bc_w_bot<ORDER>(A.wbot, A.wbc_bot, W(0, 0, 0), W(0, 0, 1), gb0, gb1, gb2);
     (void) gb0;
     auto sweep = [&](int f, auto X, double fk, double gk, double lk, double& s1, double& s2, double& s3) {
-        const double* r = cst + ((k & 1) * 4 + f) * RT_FWMAX;   // staged coefficient row
+        // staged coefficient row, read as 16-byte pairs (same value for the
+        // whole block: broadcast loads)
+        const double2* r2 = reinterpret_cast<const double2*>(cst + ((k & 1) * 4 + f) * RT_FWMAX);
+        double r[RT_FWMAX];
+#pragma unroll
+        for (int q = 0; q < (FWR + 1) / 2; q++) {
+            const double2 t = r2[q];
+            r[2 * q] = t.x;
+            r[2 * q + 1] = t.y;
+        }
         double sk = r[2 * H + 3] + r[2 * H + 1] * fk + r[2 * H + 2] * gk;
 #pragma unroll
         for (int q = 0; q < 2 * H + 1; q++) sk += r[q] * X(q - H);
@@ -482,7 +497,8 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
             fzp_prev = fzp;
             fc = -((fxp - fxm) + (fyp - fym) + (fzp - fzm)) * ivol + fc;
             // add_buoyancy{2,4} (scalar.c:6-76)
-            if (ORDER == 2) {
+            if (!buoyancy) {
+            } else if (ORDER == 2) {
                 fu += 0.5 * (c0 + C(1, 0, 0)) * A.betg_x;
                 fv += 0.5 * (c0 + C(0, 1, 0)) * A.betg_y;
                 if (do_w) fw += 0.5 * (c0 + C(0, 0, 1)) * A.betg_z;
