@@ -114,7 +114,8 @@ constexpr int RT_PLANE = RT_PI * RT_PJ;
 constexpr int RT_THREADS = RT_I * RT_J;
 constexpr double B1h = 0.5 * B1, B2h = 0.5 * B2;   // halved interpolation weights (exact)
 // 7-point form of the fourth-order staggered second difference:
-// A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) = L1 (F1+F-1-2F0) + L2 (F2+F-2-2F0) + L3 (F3+F-3-2F0)
+// A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) = L1 (F1+F-1-2F0) + L2 (F2+F-2-2F0) + L3 (F3+F-3-2F0),
+// evaluated as L1 (F1+F-1) + L2 (F2+F-2) + L3 (F3+F-3) - 2 (L1+L2+L3) F0
 constexpr double L1 = A1 * A1 - 2.0 * A1 * A2, L2 = 2.0 * A1 * A2, L3 = A2 * A2;
 constexpr int RT_FIELD = RT_SLOTS * RT_PLANE;                      // one field's ring
 constexpr int RT_LOADS = (RT_PLANE + RT_THREADS - 1) / RT_THREADS;  // plane points per thread
@@ -233,6 +234,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     const bool out = i < nx && j < ny;
     const double dxdy = G.dxdy, idx = G.idx, idy = G.idy;
     const double idx2 = idx * idx, idy2 = idy * idy;
+    const double lapc = -2.0 * (L1 + L2 + L3) * (idx2 + idy2);   // centre weight of the sum-form Laplacian
     const double* __restrict__ dydz = G.dydz;
     const double* __restrict__ dxdz = G.dxdz;
     const int kb_w = GZ - 1, kt_u = n2 - GZ;   // wall ghost rows of cell-centred fields
@@ -464,15 +466,17 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
             }
             // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363):
             // A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) of the staggered first
-            // differences is the 7-point stencil L1, L2, L3 on differences
-            // from the centre value (mathematically the same; rounds differently)
+            // differences is the 7-point stencil L1, L2, L3, here in sum form:
+            // the symmetric pairs, then the centre weight -2 (L1 + L2 + L3)
+            // folded with both directions (lapc).  Mathematically the same;
+            // it rounds differently (the centre term no longer cancels
+            // exactly, an error of a few ulps of |u| (1/dx^2 + 1/dy^2) nu).
             auto lap4 = [&](auto F, double nu) {
-                const double q0 = F(0, 0, 0);
-                const double lx = L3 * ((F(3, 0, 0) - q0) + (F(-3, 0, 0) - q0)) + L2 * ((F(2, 0, 0) - q0) + (F(-2, 0, 0) - q0))
-                                + L1 * ((F(1, 0, 0) - q0) + (F(-1, 0, 0) - q0));
-                const double ly = L3 * ((F(0, 3, 0) - q0) + (F(0, -3, 0) - q0)) + L2 * ((F(0, 2, 0) - q0) + (F(0, -2, 0) - q0))
-                                + L1 * ((F(0, 1, 0) - q0) + (F(0, -1, 0) - q0));
-                return nu * (lx * idx2 + ly * idy2);
+                const double lx = L3 * (F(3, 0, 0) + F(-3, 0, 0)) + L2 * (F(2, 0, 0) + F(-2, 0, 0))
+                                + L1 * (F(1, 0, 0) + F(-1, 0, 0));
+                const double ly = L3 * (F(0, 3, 0) + F(0, -3, 0)) + L2 * (F(0, 2, 0) + F(0, -2, 0))
+                                + L1 * (F(0, 1, 0) + F(0, -1, 0));
+                return nu * ((lx * idx2 + ly * idy2) + lapc * F(0, 0, 0));
             };
             lu = lap4(U, A.nu);
             lv = lap4(V, A.nu);
