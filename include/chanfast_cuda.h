@@ -167,6 +167,20 @@ int cf_launches_per_substep(const cf_instance *inst);
 const char *cf_strerror(int status);
 
 /* ------------------------------------------------------------------------
+ * Statistics written every istat steps by the drivers (chanfast.c:658-857,
+ * get.c), computed on the device; output to host arrays, synchronous.
+ * Profiles have n2 = nz + 2*ngz entries (wall-normal rows, ghosts included),
+ * spectra (nx/2+1)*n2*2 and (ny/2+1)*n2*2 doubles laid out [i][k][re, im].
+ * Sums run in a fixed order different from the reference's serial loops,
+ * so results agree to rounding.
+ * ------------------------------------------------------------------------ */
+int cf_xy_avg(cf_instance *inst, int field, double *avg);                 /* get_xy_avg */
+int cf_xy_corr(cf_instance *inst, int fa, int fb, double *corr);          /* get_xy_corr */
+int cf_xy_moment(cf_instance *inst, int field, double en, double *mom);   /* get_xy_moment */
+int cf_xy_spec(cf_instance *inst, int fa, int fb, double *specx, double *specy);  /* FFT3D_FWD + get_xy_spec */
+int cf_z_coords(const cf_instance *inst, double *zp, double *zw);         /* get_z_at_p / get_z_at_w */
+
+/* ------------------------------------------------------------------------
  * Batches: many independent instances stepped together, one kernel launch
  * per stage of the substep covering all of them (per-instance work records
  * in device memory: geometry, arguments, own grid).  Members may differ in

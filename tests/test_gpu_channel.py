@@ -11,7 +11,7 @@ import os
 import numpy as np
 import pytest
 
-from test_gpu_parity import interior, logs_close, params, projected_state, rel
+from test_gpu_parity import assert_stats_files_match, interior, logs_close, params, projected_state, rel
 
 import ic
 
@@ -97,3 +97,4 @@ def test_channel_drop_in_driver_matches_reference_driver(cf, ref, gpu, tmp_path,
         a = np.loadtxt(str(outs["gpu"] / f))
         b = np.loadtxt(str(outs["ref"] / f))
         assert a.shape == b.shape and np.allclose(a, b, rtol=2e-6, atol=1e-12), f
+    assert_stats_files_match(outs["gpu"], outs["ref"], 2)

@@ -175,6 +175,29 @@ def test_drop_in_driver_matches_reference_driver(cf, ref, gpu, tmp_path, order):
         a = np.loadtxt(str(outs["gpu"] / f))
         b = np.loadtxt(str(outs["ref"] / f))
         assert a.shape == b.shape and np.allclose(a, b, rtol=2e-6, atol=1e-12), f
+    assert_stats_files_match(outs["gpu"], outs["ref"], 2)
+
+
+STATS_FILES = ([f"{f}_avg" for f in "uvwcp"] + [f"{p}_corr" for p in ("uu", "vv", "ww", "cc", "pp", "wu", "uc", "wc")]
+               + ["u_mom3", "u_mom4"]
+               + [f"{p}_spec{d}" for p in ("uu", "vv", "ww", "cc", "pp", "wu", "uc", "wc") for d in "xy"])
+
+
+def assert_stats_files_match(gpu_dir, ref_dir, it):
+    """The istat statistics files (chanfast.c:658-843): %+e text, 7 digits.
+    Entries agree to 2e-6 relative, or to 1e-12 absolute where the quantity
+    is zero up to rounding on both sides (the xy mean of w, spectra of
+    modes without energy) -- the fields themselves are O(1)."""
+    for name in STATS_FILES:
+        a = np.loadtxt(str(gpu_dir / f"{name}_it{it}.dat"))
+        b = np.loadtxt(str(ref_dir / f"{name}_it{it}.dat"))
+        assert a.shape == b.shape, name
+        bad = np.abs(a - b) > 2e-6 * np.abs(b) + 1e-12
+        assert not bad.any(), (name, int(np.argmax(bad)), a[bad][:3], b[bad][:3])
+    for name in ("zp", "zw"):
+        a = np.loadtxt(str(gpu_dir / f"{name}.dat"))
+        b = np.loadtxt(str(ref_dir / f"{name}.dat"))
+        assert np.allclose(a, b, rtol=2e-6, atol=1e-12), name
 
 
 @pytest.mark.slow

@@ -13,9 +13,10 @@
  *     substeps on the GPU; append the mass-flux and scalar-mean statistics of
  *     the last substep to outputdir/pstat.dat and outputdir/cstat.dat
  *     (chanfast.c:525-528, 612-615)
- *   - every istat steps write outputdir/{u,v,w,c}_it<it+1>.dat (io.c:211-257)
- * The per-istat statistics profiles and spectra of chanfast.c:658-857
- * (channel.c:692-891) are not produced.
+ *   - every istat steps: the statistics of chanfast.c:658-857 (channel.c:
+ *     692-891) as ASCII files (io.c:22-35, one %+e per line): xy averages,
+ *     correlations, moments and x / y spectra, zp.dat and zw.dat, then the
+ *     restart files outputdir/{u,v,w,c}_it<it+1>.dat (io.c:211-257)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -54,6 +55,64 @@ static int write_field(cf_instance *inst, int field, const char *name, int it, s
         }
     }
     free(buf);
+    return rc;
+}
+
+/* io_write_ascii (io.c:22-35) */
+static int write_ascii(const double *u, size_t n, const char *name, int it)
+{
+    char fname[256];
+    if (it >= 0) snprintf(fname, sizeof fname, "outputdir/%s_it%d.dat", name, it);
+    else snprintf(fname, sizeof fname, "outputdir/%s.dat", name);
+    FILE *fp = fopen(fname, "w");
+    if (!fp) return CF_EIO;
+    for (size_t i = 0; i < n; i++) fprintf(fp, "%+e\n", u[i]);
+    return fclose(fp) == 0 ? CF_OK : CF_EIO;
+}
+
+/* The istat block of chanfast.c:658-843 in its order. */
+static int write_stats(cf_instance *inst, const cf_config *cfg, int it)
+{
+    const size_t n2 = (size_t) cfg->nz + 2 * cfg->ngz;
+    const size_t nsx = (size_t) (cfg->nx / 2 + 1) * n2 * 2, nsy = (size_t) (cfg->ny / 2 + 1) * n2 * 2;
+    double *prof = (double *) malloc(n2 * sizeof(double));
+    double *sx = (double *) malloc(nsx * sizeof(double)), *sy = (double *) malloc(nsy * sizeof(double));
+    double *zw = (double *) malloc(n2 * sizeof(double));
+    int rc = prof && sx && sy && zw ? CF_OK : CF_ENOMEM;
+    static const struct { const char *name; int f; } avg[] = {
+        {"u_avg", CF_U}, {"v_avg", CF_V}, {"w_avg", CF_W}, {"c_avg", CF_C}, {"p_avg", CF_P}};
+    static const struct { const char *name; int a, b; } pairs[] = {
+        {"uu", CF_U, CF_U}, {"vv", CF_V, CF_V}, {"ww", CF_W, CF_W}, {"cc", CF_C, CF_C},
+        {"pp", CF_P, CF_P}, {"wu", CF_W, CF_U}, {"uc", CF_U, CF_C}, {"wc", CF_W, CF_C}};
+    char name[64];
+    for (int q = 0; q < 5 && rc == CF_OK; q++) {
+        rc = cf_xy_avg(inst, avg[q].f, prof);
+        if (rc == CF_OK) rc = write_ascii(prof, n2, avg[q].name, it);
+    }
+    for (int q = 0; q < 8 && rc == CF_OK; q++) {
+        rc = cf_xy_corr(inst, pairs[q].a, pairs[q].b, prof);
+        snprintf(name, sizeof name, "%s_corr", pairs[q].name);
+        if (rc == CF_OK) rc = write_ascii(prof, n2, name, it);
+    }
+    for (int q = 3; q <= 4 && rc == CF_OK; q++) {
+        rc = cf_xy_moment(inst, CF_U, (double) q, prof);
+        snprintf(name, sizeof name, "u_mom%d", q);
+        if (rc == CF_OK) rc = write_ascii(prof, n2, name, it);
+    }
+    for (int q = 0; q < 8 && rc == CF_OK; q++) {
+        rc = cf_xy_spec(inst, pairs[q].a, pairs[q].b, sx, sy);
+        snprintf(name, sizeof name, "%s_specx", pairs[q].name);
+        if (rc == CF_OK) rc = write_ascii(sx, nsx, name, it);
+        snprintf(name, sizeof name, "%s_specy", pairs[q].name);
+        if (rc == CF_OK) rc = write_ascii(sy, nsy, name, it);
+    }
+    if (rc == CF_OK) rc = cf_z_coords(inst, prof, zw);
+    if (rc == CF_OK) rc = write_ascii(prof, n2, "zp", -1);
+    if (rc == CF_OK) rc = write_ascii(zw, n2, "zw", -1);
+    free(prof);
+    free(sx);
+    free(sy);
+    free(zw);
     return rc;
 }
 
@@ -122,8 +181,10 @@ static int run(int order, int scheme, int p_row, int p_col, int nx, int ny, int 
         double cs[6] = {(double) (it + 1), log[5], log[6], log[7], log[8], log[9]};
         rc = append_ascii(ps, 6, "outputdir/pstat.dat");
         if (rc == CF_OK) rc = append_ascii(cs, 6, "outputdir/cstat.dat");
-        if (rc == CF_OK && (it + 1) % istat == 0)
+        if (rc == CF_OK && (it + 1) % istat == 0) {
+            rc = write_stats(inst, &cfg, it + 1);
             for (int f = 0; f < 4 && rc == CF_OK; f++) rc = write_field(inst, fields[f], names[f], it + 1, n);
+        }
     }
     int rc2 = cf_destroy(inst);
     return rc ? rc : rc2;

@@ -130,6 +130,8 @@ struct DivArgs {
     FftPlan px;
     double c8;
     double* dv;            // real divergence field [n2][nx][ny] (power-of-two nx path)
+    const double* src;     // non-null: transform this field instead of the divergence
+    int kshift;            // rows GZ + kshift ..: 0 for the divergence, -GZ for all n2 rows
 };
 
 // Real-to-complex x transform of rows kfirst .. of nfields real fields
@@ -210,6 +212,9 @@ void launch_mass_control(const MassArgs& M, cudaStream_t st);
 void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st);
 bool fftx_batched_supported(int nx);
 void launch_fftx_r2c(const Geo& G, const R2cArgs& A, int nrows, int nfields, cudaStream_t st);
+// forward 2-D transform (x then y, scaled by 1/(nx ny)) of all n2 rows of one field into spec
+void launch_fft2d_field(const Geo& G, const double* field, double2* spec, const FftPlan& px,
+                        const FftPlan& py, double c8, cudaStream_t st);
 void launch_ffty(const Geo& G, const FftyArgs& A, int nrows, cudaStream_t st, int nfields = 1);
 void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st, int nfields = 1);
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st);

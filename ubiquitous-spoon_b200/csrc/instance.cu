@@ -245,6 +245,120 @@ __global__ void k_max_rows_final(const double* rowmax, int n, double* result)
     if (threadIdx.x == 0) *result = red[0];
 }
 
+// ----------------------------------------------------------- statistics
+//
+// Plane statistics of get.c on the device, one block per row k, fixed
+// summation order (the reference sums serially, so they agree to rounding):
+// mode 0 the mean of a (get_xy_avg, :281-302), mode 1 the mean of
+// (a - abar)(b - bbar) (get_xy_corr, :132-172), mode 2 the mean of
+// pow(a - abar, en) (get_xy_moment, :94-129).
+__global__ void k_row_stat(Geo G, const double* __restrict__ a, const double* __restrict__ b,
+                           const double* __restrict__ abar, const double* __restrict__ bbar, int mode, double en,
+                           double* __restrict__ out)
+{
+    __shared__ double red[256];
+    const int k = blockIdx.x;
+    const long long P = G.plane;
+    const double* ak = a + k * P;
+    const double* bk = b ? b + k * P : nullptr;
+    const double am = abar ? abar[k] : 0.0, bm = bbar ? bbar[k] : 0.0;
+    double s = 0.0;
+    for (long long c = threadIdx.x; c < P; c += blockDim.x) {
+        const double x = ak[c];
+        if (mode == 0) s += x;
+        else if (mode == 1) s += (x - am) * (bk[c] - bm);
+        else s += pow(x - am, en);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = red[0] * (1.0 / ((double) G.nx * (double) G.ny));
+}
+
+// Cross spectrum of one column: Re, Im of uhat conj(vhat) (get.c:26-31).
+__device__ __forceinline__ double2 cross(const double2 u, const double2 v)
+{
+    return make_double2(u.x * v.x + u.y * v.y, u.y * v.x - u.x * v.y);
+}
+
+// get_xy_spec (get.c:5-91), x spectrum: specx[ix][k] = sum over iy of the
+// cross spectrum, the (0, 0) mode left out.  One block per (ix, k).
+__global__ void k_specx(Geo G, const double2* __restrict__ uh, const double2* __restrict__ vh,
+                        double* __restrict__ specx)
+{
+    __shared__ double2 red[256];
+    const int ix = blockIdx.x, k = blockIdx.y, ny = G.ny;
+    const long long base = ((long long) k * G.nkx + ix) * ny;
+    double2 s = make_double2(0.0, 0.0);
+    for (int iy = threadIdx.x; iy < ny; iy += blockDim.x) {
+        if (ix == 0 && iy == 0) continue;
+        const double2 c = cross(uh[base + iy], vh[base + iy]);
+        s.x += c.x;
+        s.y += c.y;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) {
+            red[threadIdx.x].x += red[threadIdx.x + o].x;
+            red[threadIdx.x].y += red[threadIdx.x + o].y;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        specx[((long long) ix * G.n2 + k) * 2] = red[0].x;
+        specx[((long long) ix * G.n2 + k) * 2 + 1] = red[0].y;
+    }
+}
+
+// y spectrum: specy[iy][k], iy in [0, ny/2], sums over ix the column iy and,
+// for the modes whose conjugate column is not stored (0 < ix, except
+// ix = nx/2 with nx even), the column ny - iy with its imaginary part
+// negated; ix = 0 contributes for iy > 0 only.  One block per (iy, k).
+__global__ void k_specy(Geo G, const double2* __restrict__ uh, const double2* __restrict__ vh,
+                        double* __restrict__ specy)
+{
+    __shared__ double2 red[256];
+    const int iyt = blockIdx.x, k = blockIdx.y, nx = G.nx, ny = G.ny, nkx = G.nkx;
+    const int iyc = (ny - iyt) % ny;
+    double2 s = make_double2(0.0, 0.0);
+    for (int ix = threadIdx.x; ix < nkx; ix += blockDim.x) {
+        const long long base = ((long long) k * nkx + ix) * ny;
+        if (ix == 0) {
+            if (iyt > 0) {
+                const double2 c = cross(uh[base + iyt], vh[base + iyt]);
+                s.x += c.x;
+                s.y += c.y;
+            }
+        } else if (nx % 2 == 0 && ix == nx / 2) {
+            const double2 c = cross(uh[base + iyt], vh[base + iyt]);
+            s.x += c.x;
+            s.y += c.y;
+        } else {
+            const double2 c = cross(uh[base + iyt], vh[base + iyt]);
+            const double2 d = cross(uh[base + iyc], vh[base + iyc]);
+            s.x += c.x + d.x;
+            s.y += c.y - d.y;
+        }
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int) threadIdx.x < o) {
+            red[threadIdx.x].x += red[threadIdx.x + o].x;
+            red[threadIdx.x].y += red[threadIdx.x + o].y;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        specy[((long long) iyt * G.n2 + k) * 2] = red[0].x;
+        specy[((long long) iyt * G.n2 + k) * 2 + 1] = red[0].y;
+    }
+}
+
 // ------------------------------------------------------------ host helpers
 
 // Packs host vectors into one device allocation.
@@ -1642,6 +1756,77 @@ int cf_batch_launches_per_substep(const cf_batch* B)
 {
     if (!B) return CF_EINVAL;
     return (int) ((B->half[0].ops.size() + B->half[1].ops.size()) / 6);
+}
+
+// Row statistics into host `out` (n2 values); mode as k_row_stat.
+static int row_stat(cf_instance* I, int fa, int fb, int mode, double en, double* out)
+{
+    if (!I || !out) return CF_EINVAL;
+    const double* a = field_ptr(I, fa);
+    const double* b = mode == 1 ? field_ptr(I, fb) : nullptr;
+    if (!a || (mode == 1 && !b)) return CF_EINVAL;
+    const Geo& G = I->geo;
+    cudaStream_t st = I->stream;
+    double* d = nullptr;
+    CF_CUDA(cudaMallocAsync(&d, 3 * (size_t) G.n2 * sizeof(double), st));
+    double *abar = d + G.n2, *bbar = d + 2 * G.n2;
+    if (mode != 0) k_row_stat<<<G.n2, 256, 0, st>>>(G, a, nullptr, nullptr, nullptr, 0, 0.0, abar);
+    if (mode == 1) k_row_stat<<<G.n2, 256, 0, st>>>(G, b, nullptr, nullptr, nullptr, 0, 0.0, bbar);
+    k_row_stat<<<G.n2, 256, 0, st>>>(G, a, b, mode ? abar : nullptr, mode == 1 ? bbar : nullptr, mode, en, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, (size_t) G.n2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    CF_CUDA(e);
+    return CF_OK;
+}
+
+int cf_xy_avg(cf_instance* I, int field, double* avg) { return row_stat(I, field, -1, 0, 0.0, avg); }
+
+int cf_xy_corr(cf_instance* I, int fa, int fb, double* corr) { return row_stat(I, fa, fb, 1, 0.0, corr); }
+
+int cf_xy_moment(cf_instance* I, int field, double en, double* moment)
+{
+    return row_stat(I, field, -1, 2, en, moment);
+}
+
+int cf_xy_spec(cf_instance* I, int fa, int fb, double* specx, double* specy)
+{
+    if (!I || !specx || !specy) return CF_EINVAL;
+    const double* a = field_ptr(I, fa);
+    const double* b = field_ptr(I, fb);
+    if (!a || !b) return CF_EINVAL;
+    const Geo& G = I->geo;
+    cudaStream_t st = I->stream;
+    const size_t nsx = (size_t) (G.nx / 2 + 1) * G.n2 * 2, nsy = (size_t) (G.ny / 2 + 1) * G.n2 * 2;
+    const size_t nspec = (size_t) G.splane * G.n2;
+    double2* vh = nullptr;
+    double* out = nullptr;
+    CF_CUDA(cudaMallocAsync(&out, (nsx + nsy) * sizeof(double), st));
+    if (fb != fa) CF_CUDA(cudaMallocAsync(&vh, nspec * sizeof(double2), st));
+    // FFT3D_FWD of both fields over all n2 rows (chanfast.c:758-765)
+    launch_fft2d_field(G, a, I->spec, I->px, I->py, I->c8, st);
+    if (vh) launch_fft2d_field(G, b, vh, I->px, I->py, I->c8, st);
+    const double2* v2 = vh ? vh : I->spec;
+    k_specx<<<dim3(G.nkx, G.n2), 256, 0, st>>>(G, I->spec, v2, out);
+    k_specy<<<dim3(G.ny / 2 + 1, G.n2), 256, 0, st>>>(G, I->spec, v2, out + nsx);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(specx, out, nsx * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(specy, out + nsx, nsy * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(out, st);
+    if (vh) cudaFreeAsync(vh, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    CF_CUDA(e);
+    return CF_OK;
+}
+
+int cf_z_coords(const cf_instance* I, double* zp, double* zw)
+{
+    if (!I) return CF_EINVAL;
+    const std::vector<double> p = z_at_p(I->m), w = z_at_w(I->m);
+    if (zp) std::memcpy(zp, p.data(), p.size() * sizeof(double));
+    if (zw) std::memcpy(zw, w.data(), w.size() * sizeof(double));
+    return CF_OK;
 }
 
 unsigned long long cf_instance_bytes(const cf_config* c)

@@ -290,7 +290,7 @@ template <int ORDER, int N>
 __device__ __forceinline__ void k_div_fftx_body(const Geo& G, const DivArgs& A, uint3 bid)
 {
     extern __shared__ double2 sbuf[];
-    const int k = GZ + bid.y;
+    const int k = GZ + A.kshift + bid.y;
     const int j0 = bid.x * FFT_L;
     const int nx = N ? N : G.nx, ny = G.ny, n2 = G.n2;
     const double dx = G.dx, dy = G.dy, dzk = G.dz[k];
@@ -301,7 +301,9 @@ __device__ __forceinline__ void k_div_fftx_body(const Geo& G, const DivArgs& A, 
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
         double d = 0.0;
-        if (j < ny) {
+        if (j < ny && A.src) {
+            d = __ldg(A.src + I(k, i, j));
+        } else if (j < ny) {
             auto U = [&](int di) { double t = __ldg(A.u + I(k, wrapp(i + di, nx), j)); return corr ? t + uc : t; };
             auto V = [&](int dj) { return __ldg(A.v + I(k, i, wrapp(j + dj, ny))); };
             auto Wr = [&](int kk) { return __ldg(A.w + I(kk, i, j)); };
@@ -1263,6 +1265,33 @@ void launch_div_fftx(const Geo& G, const DivArgs& A, cudaStream_t st)
 #undef CASE_
     if (G.order == 2) k_div_fftx<2, 0><<<grd, FFT_THREADS, sm, st>>>(G, A);
     else k_div_fftx<4, 0><<<grd, FFT_THREADS, sm, st>>>(G, A);
+}
+
+void launch_fft2d_field(const Geo& G, const double* field, double2* spec, const FftPlan& px,
+                        const FftPlan& py, double c8, cudaStream_t st)
+{
+    if (pow2_kernel_size(G.nx)) {
+        R2cArgs R{field, spec, px, c8, 0, 0, 0};
+        launch_fftx_r2c(G, R, G.n2, 1, st);
+    } else {
+        DivArgs D{};
+        D.spec = spec;
+        D.px = px;
+        D.c8 = c8;
+        D.src = field;
+        D.kshift = -GZ;
+        dim3 grd((G.ny + FFT_L - 1) / FFT_L, G.n2);
+        const size_t sm = fft_smem_bytes(G.nx);
+#define CASE_(n_) \
+    case n_: k_div_fftx<2, n_><<<grd, FFT_THREADS, sm, st>>>(G, D); break;
+        switch (G.nx) {
+        STATIC_FFT_SIZES(CASE_)
+        default: k_div_fftx<2, 0><<<grd, FFT_THREADS, sm, st>>>(G, D); break;
+        }
+#undef CASE_
+    }
+    FftyArgs Y{spec, py, -1, 0, c8, 0};
+    launch_ffty(G, Y, G.n2, st);
 }
 
 bool fftx_batched_supported(int nx)
