@@ -199,6 +199,23 @@ def ensure_reference():
 
 # ---------------------------------------------------------------- GPU arm
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest x over all ranks: a multi-GPU run takes as long as its
+    slowest replica."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(pts, substeps, world, seconds):
+    """Whole-job throughput in Mpt-substeps/s: every replica advances its
+    own `pts`-point instance by `substeps` in the job's time."""
+    return pts * substeps * world / seconds / 1e6
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -241,14 +258,10 @@ def run_ours(args):
         end.record(stream)
         end.synchronize()
         barrier()
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(end), dist)
     pts = w["nx"] * w["ny"] * w["nz"]
     substeps = 3 * args.steps
-    value = pts * substeps * world / (ms * 1e-3) / 1e6
+    value = job_value(pts, substeps, world, ms * 1e-3)
     ms_per_step = ms / args.steps
 
     # per-kernel device times (CUDA events between the launch groups)
@@ -295,13 +308,9 @@ def run_ours(args):
         for nm in "uvwc":
             inst2.get_field(nm, out=host[nm])
         barrier()
-        t_e2e = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([t_e2e], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
+        t_e2e = max_over_ranks(time.perf_counter() - t0, dist)
         nbytes = 4 * host["u"].nbytes
-        e2e = {"value": round(pts * 3 * nrun * world / t_e2e / 1e6, 1), "unit": METRIC,
+        e2e = {"value": round(job_value(pts, 3 * nrun, world, t_e2e), 1), "unit": METRIC,
                "h2d_bytes_per_step": nbytes // nrun, "d2h_bytes_per_step": nbytes // nrun,
                "run_steps": nrun,
                "how": "cf_set_field x4 (pinned host, reference padded layout) + cf_step_graph(run_steps) "
