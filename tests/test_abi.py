@@ -17,6 +17,7 @@ def declared_functions():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"^\s*typedef[^;]*;", "", src, flags=re.M)   # function-pointer and struct typedefs
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", src, flags=re.M):
             names.add(m.group(1))
     names.discard("if")
