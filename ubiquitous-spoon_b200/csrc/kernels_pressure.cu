@@ -710,10 +710,11 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
                 const double2 svA = lsA[u], svB = lsB[u];
                 const double p = lp[u], q = lq[u], r = lr[u];
                 bload(i - POIS_PB, u);
-                const double2 xA = make_double2(svA.x - p * x1A.x - q * x2A.x - r * x3A.x,
-                                                svA.y - p * x1A.y - q * x2A.y - r * x3A.y);
-                const double2 xB = make_double2(svB.x - p * x1B.x - q * x2B.x - r * x3B.x,
-                                                svB.y - p * x1B.y - q * x2B.y - r * x3B.y);
+                // the previous row's x1 enters last: one dependent operation per row
+                const double2 xA = make_double2(((svA.x - r * x3A.x) - q * x2A.x) - p * x1A.x,
+                                                ((svA.y - r * x3A.y) - q * x2A.y) - p * x1A.y);
+                const double2 xB = make_double2(((svB.x - r * x3B.x) - q * x2B.x) - p * x1B.x,
+                                                ((svB.y - r * x3B.y) - q * x2B.y) - p * x1B.y);
                 SA(GZ + i) = xA;
                 SB(GZ + i) = xB;
                 if (stats) A.avg[GZ + i] = xA.x;

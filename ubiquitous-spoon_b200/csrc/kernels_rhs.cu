@@ -330,8 +330,8 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 #pragma unroll
         for (int q = 0; q < 2 * H + 1; q++) sk += r[q] * X(q - H);
         if (IMPL3D) return sk + lk;   // h of this point (channel_rows: no elimination)
-        sk -= r[2 * H + 4] * s1;
         if (ORDER == 4) sk -= r[2 * H + 5] * s2 + r[2 * H + 6] * s3;
+        sk -= r[2 * H + 4] * s1;   // the previous row's s enters last
         s3 = s2; s2 = s1; s1 = sk;
         return sk;
     };

@@ -42,8 +42,9 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A, ui
     const double* __restrict__ sv = A.s;
     const long long cc = active ? col : 0;
 
-    // x_i = ((s_i - P_i x_{i+1}) - Q_i x_{i+2}) - R_i x_{i+3}, s of row
-    // i - PD loaded into registers while row i is computed.
+    // x_i = s_i - P_i x_{i+1} - Q_i x_{i+2} - R_i x_{i+3}, evaluated with
+    // x_{i+1} last (one dependent operation per row on the critical path);
+    // s of row i - PD loaded into registers while row i is computed.
     constexpr int PD = 4;
     double ps[PD];
     auto fetch_s = [&](int i, int slot) {
@@ -65,7 +66,7 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A, ui
                 fetch_s(i - PD, u);
                 double y;
                 if (ORDER == 2) y = s - __ldg(A.fac.P + i) * y1;
-                else y = s - __ldg(A.fac.P + i) * y1 - __ldg(A.fac.Q + i) * y2 - __ldg(A.fac.R + i) * y3;
+                else y = ((s - __ldg(A.fac.R + i) * y3) - __ldg(A.fac.Q + i) * y2) - __ldg(A.fac.P + i) * y1;   // y1 last
                 y3 = y2; y2 = y1; y1 = y;
                 if (active) x[(long long) k * P + col] = y;
                 if (i == n - 1) top0 = y;
