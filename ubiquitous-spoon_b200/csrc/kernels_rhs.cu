@@ -108,24 +108,40 @@ __global__ void k_ghosts_batch(const BatchRec<GhostArgs>* r, int n)
 // overwrites g; A.nu and A.kappa then carry nuadt and nuadt / prandtl.  The
 // spectral solves follow (kernels_pressure.cu).
 
-constexpr int RT_I = 8, RT_J = 32, RT_H = 3, RT_SLOTS = 8;
-constexpr int RT_PI = RT_I + 2 * RT_H, RT_PJ = RT_J + 2 * RT_H;   // 14 x 38
-constexpr int RT_PLANE = RT_PI * RT_PJ;
+constexpr int RT_I = 8, RT_J = 32;
 constexpr int RT_THREADS = RT_I * RT_J;
+
+// Ring geometry per order: the x-y halo and z reach of the stencils (order
+// 4: 3, the fourth-order fluxes and Laplacian; order 2: 2, the QUICK scalar
+// fluxes), a ring of the 2 ZH + 1 planes a row reads plus the one in flight
+// (8 and 6 slots).  Order 2 thus needs 83 KB of ring instead of 136 KB.
+// One block per SM for both: capping order 2 at 128 registers for two blocks
+// per SM measured 5-9 % slower (less instruction-level parallelism).
+template <int ORDER>
+struct RhsTile {
+    static constexpr int H = ORDER == 2 ? 2 : 3;
+    static constexpr int ZH = H;
+    static constexpr int SLOTS = 2 * ZH + 2;
+    static constexpr int PI = RT_I + 2 * H, PJ = RT_J + 2 * H;   // 14 x 38 / 12 x 36
+    static constexpr int PLANE = PI * PJ;
+    static constexpr int FIELD = SLOTS * PLANE;                  // one field's ring
+    static constexpr int LOADS = (PLANE + RT_THREADS - 1) / RT_THREADS;   // plane points per thread
+    static constexpr int BLOCKS = 1;                             // launch bound: blocks per SM
+    __host__ __device__ static constexpr int slot(int kk) { return kk % SLOTS; }
+};
 constexpr double B1h = 0.5 * B1, B2h = 0.5 * B2;   // halved interpolation weights (exact)
 // 7-point form of the fourth-order staggered second difference:
 // A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) = L1 (F1+F-1-2F0) + L2 (F2+F-2-2F0) + L3 (F3+F-3-2F0),
 // evaluated as L1 (F1+F-1) + L2 (F2+F-2) + L3 (F3+F-3) - 2 (L1+L2+L3) F0
 constexpr double L1 = A1 * A1 - 2.0 * A1 * A2, L2 = 2.0 * A1 * A2, L3 = A2 * A2;
-constexpr int RT_FIELD = RT_SLOTS * RT_PLANE;                      // one field's ring
-constexpr int RT_LOADS = (RT_PLANE + RT_THREADS - 1) / RT_THREADS;  // plane points per thread
 
 constexpr int RT_FWMAX = 14;   // widest fused forward row (order 4: 13), padded to 16-byte pairs
 // ring of haloed planes + two rows of each thread's g values + two rows of
 // the four fused coefficient rows
-size_t rhs_smem_bytes()
+template <int ORDER>
+constexpr size_t rhs_smem_bytes()
 {
-    return (size_t) (4 * RT_SLOTS * RT_PLANE + 2 * 4 * RT_THREADS + 2 * 4 * RT_FWMAX) * sizeof(double);
+    return (size_t) (4 * RhsTile<ORDER>::FIELD + 2 * 4 * RT_THREADS + 2 * 4 * RT_FWMAX) * sizeof(double);
 }
 
 // z fluxes of one advected field (order 4), carried up the column.  With
@@ -175,6 +191,7 @@ template <int ORDER, bool IMPL3D>
 __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 bid)
 {
     extern __shared__ double sm[];
+    using T = RhsTile<ORDER>;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RT_J + tx;
     const int j0 = bid.x * RT_J, i0 = bid.y * RT_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
@@ -183,34 +200,34 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 
     // This thread's points of a haloed plane (same in every plane): their
     // offsets within a field plane, computed once.
-    int goff[RT_LOADS];
+    int goff[T::LOADS];
 #pragma unroll
-    for (int m = 0; m < RT_LOADS; m++) {
+    for (int m = 0; m < T::LOADS; m++) {
         const int r = tid + m * RT_THREADS;
-        const int ii = r / RT_PJ, jj = r - ii * RT_PJ;
-        int gi = (i0 + ii - RT_H) % nx; if (gi < 0) gi += nx;
-        int gj = (j0 + jj - RT_H) % ny; if (gj < 0) gj += ny;
+        const int ii = r / T::PJ, jj = r - ii * T::PJ;
+        int gi = (i0 + ii - T::H) % nx; if (gi < 0) gi += nx;
+        int gj = (j0 + jj - T::H) % ny; if (gj < 0) gj += ny;
         goff[m] = gi * ny + gj;
     }
     auto load_plane = [&](int kk) {
         const long long base = (long long) kk * plane;
-        double* d0 = sm + (kk & (RT_SLOTS - 1)) * RT_PLANE + tid;
+        double* d0 = sm + T::slot(kk) * T::PLANE + tid;
 #pragma unroll
-        for (int m = 0; m < RT_LOADS; m++) {
-            if (tid + m * RT_THREADS < RT_PLANE) {
+        for (int m = 0; m < T::LOADS; m++) {
+            if (tid + m * RT_THREADS < T::PLANE) {
                 double* d = d0 + m * RT_THREADS;
                 const long long o = base + goff[m];
                 cp_async8(d, A.u + o);
-                cp_async8(d + RT_FIELD, A.v + o);
-                cp_async8(d + 2 * RT_FIELD, A.w + o);
-                cp_async8(d + 3 * RT_FIELD, A.c + o);
+                cp_async8(d + T::FIELD, A.v + o);
+                cp_async8(d + 2 * T::FIELD, A.w + o);
+                cp_async8(d + 3 * T::FIELD, A.c + o);
             }
         }
         cp_async_commit();
     };
     // g values (per thread) and fused coefficient rows (per block) of row kk,
     // staged one row ahead so the sweeps never wait on global memory
-    double* gst = sm + 4 * RT_FIELD;              // [2][4][RT_THREADS]
+    double* gst = sm + 4 * T::FIELD;              // [2][4][RT_THREADS]
     double* cst = gst + 2 * 4 * RT_THREADS;       // [2][4][RT_FWMAX]
     constexpr int FWR = (ORDER == 2 ? 3 : 7) + 6; // fused row width (host_band.h fused_rows)
     const long long gij = (i0 + ty < nx && j0 + tx < ny) ? (long long) (i0 + ty) * ny + (j0 + tx) : 0;
@@ -226,7 +243,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
         }
     };
     load_extras(kb);
-    for (int kk = kb - 3; kk <= kb + 3; kk++) load_plane(kk);
+    for (int kk = kb - T::ZH; kk <= kb + T::ZH; kk++) load_plane(kk);
     cp_async_wait_all();
     __syncthreads();
 
@@ -241,7 +258,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 
     int k = kb;
     auto at = [&](int f, int di, int dj, int dk) -> double {
-        return sm[f * RT_FIELD + ((k + dk) & (RT_SLOTS - 1)) * RT_PLANE + (ty + RT_H + di) * RT_PJ + (tx + RT_H + dj)];
+        return sm[f * T::FIELD + T::slot(k + dk) * T::PLANE + (ty + T::H + di) * T::PJ + (tx + T::H + dj)];
     };
     auto U = [&](int di, int dj, int dk) { return at(0, di, dj, dk); };
     auto V = [&](int di, int dj, int dk) { return at(1, di, dj, dk); };
@@ -548,7 +565,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 
     for (; k < ke; k++) {
         if (k + 1 < ke) load_extras(k + 1);
-        if (k + 4 <= ke + 2) load_plane(k + 4);
+        if (k + T::ZH + 1 <= ke + T::ZH - 1) load_plane(k + T::ZH + 1);   // the last row reads ke - 1 + ZH
         else cp_async_commit();
         if (k <= GZ + 1 || k >= n2 - GZ - 3) row(std::true_type{});
         else row(std::false_type{});
@@ -558,13 +575,13 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 }
 
 template <int ORDER, bool IMPL3D>
-__global__ void __launch_bounds__(RT_THREADS, 1) k_rhs(Geo G, RhsArgs A)
+__global__ void __launch_bounds__(RT_THREADS, RhsTile<ORDER>::BLOCKS) k_rhs(Geo G, RhsArgs A)
 {
     rhs_body<ORDER, IMPL3D>(G, A, blockIdx);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(RT_THREADS, 1) k_rhs_batch(const BatchRec<RhsArgs>* r, int n)
+__global__ void __launch_bounds__(RT_THREADS, RhsTile<ORDER>::BLOCKS) k_rhs_batch(const BatchRec<RhsArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<RhsArgs>& R = batch_locate(r, n, b);
@@ -603,33 +620,32 @@ void launch_rhs_batch(const BatchLaunch& L, int order, cudaStream_t st)
 {
     auto r = static_cast<const BatchRec<RhsArgs>*>(L.recs);
     dim3 blk(RT_J, RT_I, 1);
-    if (order == 2) k_rhs_batch<2><<<L.blocks, blk, rhs_smem_bytes(), st>>>(r, L.n);
-    else k_rhs_batch<4><<<L.blocks, blk, rhs_smem_bytes(), st>>>(r, L.n);
+    if (order == 2) k_rhs_batch<2><<<L.blocks, blk, rhs_smem_bytes<2>(), st>>>(r, L.n);
+    else k_rhs_batch<4><<<L.blocks, blk, rhs_smem_bytes<4>(), st>>>(r, L.n);
 }
 
 void launch_rhs(const Geo& G, const RhsArgs& A, bool implicit3d, cudaStream_t st)
 {
     dim3 blk(RT_J, RT_I, 1);
     dim3 grd = grid_rhs(G);
-    size_t sm = rhs_smem_bytes();
     if (implicit3d) {
-        if (G.order == 2) k_rhs<2, true><<<grd, blk, sm, st>>>(G, A);
-        else k_rhs<4, true><<<grd, blk, sm, st>>>(G, A);
+        if (G.order == 2) k_rhs<2, true><<<grd, blk, rhs_smem_bytes<2>(), st>>>(G, A);
+        else k_rhs<4, true><<<grd, blk, rhs_smem_bytes<4>(), st>>>(G, A);
     } else {
-        if (G.order == 2) k_rhs<2, false><<<grd, blk, sm, st>>>(G, A);
-        else k_rhs<4, false><<<grd, blk, sm, st>>>(G, A);
+        if (G.order == 2) k_rhs<2, false><<<grd, blk, rhs_smem_bytes<2>(), st>>>(G, A);
+        else k_rhs<4, false><<<grd, blk, rhs_smem_bytes<4>(), st>>>(G, A);
     }
 }
 
 cudaError_t rhs_set_smem_limits()
 {
-    int v = (int) rhs_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_rhs<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    const int v2 = (int) rhs_smem_bytes<2>(), v4 = (int) rhs_smem_bytes<4>();
+    cudaError_t e = cudaFuncSetAttribute(k_rhs<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v2);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v4);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v2);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v4);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v2);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rhs_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v4);
     return e;
 }
 
