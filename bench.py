@@ -473,7 +473,7 @@ def run_serve(args):
 
     def measure(max_active):
         t0 = time.perf_counter()
-        res = cf.serve(reqs, hbm_budget_bytes=150e9, max_active=max_active, quantum=1)
+        res = cf.serve(reqs, hbm_budget_bytes=150e9, max_active=max_active, quantum=args.serve_quantum)
         wall = time.perf_counter() - t0
         lat = np.array([x["finish_s"] - r["arrival_s"] for x, r in zip(res, reqs)])
         ok = sum(1 for x in res if x["status"] == 0)
@@ -493,7 +493,7 @@ def run_serve(args):
                                      + ", Re_b log-U[2800, 20000], order 2 or 4",
                          "steps": f"U[200, 2000] x {args.serve_step_scale} RK3 steps per request",
                          "admission": "150 GB budget by cf_instance_bytes, at most 64 resident",
-                         "rounds": "one RK3 step of every resident solve per batched call"},
+                         "rounds": f"{args.serve_quantum} RK3 step(s) of every resident solve per batched call"},
               "clocks": clk.summary()}
     if args.serve_baseline:
         result["one_at_a_time"] = measure(1)
@@ -543,6 +543,7 @@ def main():
     ap.add_argument("--serve-step-scale", type=float, default=0.1,
                     help="scale of the U[200, 2000] step counts (1.0 = the full trace)")
     ap.add_argument("--serve-baseline", action="store_true", help="also serve the trace one solve at a time")
+    ap.add_argument("--serve-quantum", type=int, default=1, help="RK3 steps per serving round")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 (default) is the benchmark; the others serve profiling and checks")
     args = ap.parse_args()

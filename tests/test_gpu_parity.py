@@ -54,10 +54,13 @@ def params(order, nx, ny, nz, **kw):
     return cn.Params(order=order, nx=nx, ny=ny, nz=nz, **base)
 
 
-# the last four cover every fixed-size non-power-of-two transform (48, 96, 160,
-# 192, 320, 384) in x and in y
+# (2, 96, 96, 16) .. (4, 48, 320, 8) cover every fixed-size non-power-of-two
+# transform (48, 96, 160, 192, 320, 384) in x and in y; the last two have odd
+# nx and ny (no Nyquist column; the ky / ny - ky pairs of the band solves
+# then have no self-paired column but ky = 0)
 CASES = [(2, 16, 12, 10), (2, 32, 32, 32), (4, 18, 24, 12), (4, 64, 48, 40),
-         (2, 96, 96, 16), (4, 192, 160, 12), (2, 384, 48, 8), (4, 48, 320, 8)]
+         (2, 96, 96, 16), (4, 192, 160, 12), (2, 384, 48, 8), (4, 48, 320, 8),
+         (2, 15, 9, 10), (4, 25, 27, 12)]
 
 
 @pytest.mark.parametrize("order,nx,ny,nz", CASES)
