@@ -942,7 +942,7 @@ __host__ __device__ constexpr int p2_stride_x(int n) { return p2_pad(n) + (p2_li
 // L2 once; w is carried up the column in a register window, and at the walls
 // that window supplies the extrapolated w of pressure.c:80-95.  The x
 // transform then reads the result as a real field.
-constexpr int DV_I = 8, DV_J = 32, DV_KC = 8;
+constexpr int DV_I = 8, DV_J = 32, DV_KC = 16;
 
 __device__ __forceinline__ void dv_cp8(double* dst, const double* src)
 {
@@ -963,18 +963,28 @@ __device__ __forceinline__ void k_div_body(const Geo& G, const DivArgs& A, uint3
     const int k1 = min(k0 + DV_KC, n2 - GZ);
     const int i = i0 + ty, j = j0 + tx;
     const bool valid = i < nx && j < ny;
+    // this thread's halo elements (at most two of u, two of v): their
+    // offsets within a plane, the same for every plane, computed once
+    constexpr int NU = (DV_I + 3) * DV_J, NV = DV_I * (DV_J + 3), NT = DV_I * DV_J;
+    int uoff[2], voff[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int e = tid + q * NT;
+        const int r = e / DV_J, c = e - r * DV_J;
+        int ii = (i0 - 2 + r) % nx; if (ii < 0) ii += nx;
+        uoff[q] = e < NU ? ii * ny + min(j0 + c, ny - 1) : 0;
+        const int rv = e / (DV_J + 3), cv = e - rv * (DV_J + 3);
+        int jj = (j0 - 2 + cv) % ny; if (jj < 0) jj += ny;
+        voff[q] = e < NV ? min(i0 + rv, nx - 1) * ny + jj : 0;
+    }
     auto load = [&](int kk, int buf) {
         const double* uk = A.u + kk * plane;
         const double* vk = A.v + kk * plane;
-        for (int e = tid; e < (DV_I + 3) * DV_J; e += DV_I * DV_J) {
-            const int r = e / DV_J, c = e - r * DV_J;
-            int ii = (i0 - 2 + r) % nx; if (ii < 0) ii += nx;
-            dv_cp8(&su[buf][r][c], uk + ii * ny + min(j0 + c, ny - 1));
-        }
-        for (int e = tid; e < DV_I * (DV_J + 3); e += DV_I * DV_J) {
-            const int r = e / (DV_J + 3), c = e - r * (DV_J + 3);
-            int jj = (j0 - 2 + c) % ny; if (jj < 0) jj += ny;
-            dv_cp8(&sv[buf][r][c], vk + min(i0 + r, nx - 1) * ny + jj);
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int e = tid + q * NT;
+            if (e < NU) dv_cp8(&su[buf][0][0] + e, uk + uoff[q]);
+            if (e < NV) dv_cp8(&sv[buf][0][0] + e, vk + voff[q]);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
