@@ -75,3 +75,49 @@ def test_config_mirrors_reference_arguments(cf):
     p = cn.Params(order=4, nx=8, ny=8, nz=8, lx=1, ly=1, lz=2, dt=1e-3, nu=1e-3)
     c = cf.Config.from_params(p)
     assert (c.order, c.nx, c.ngz) == (4, 8, 3)
+
+
+def test_instance_bytes_and_batch_serve_argument_checks(cf):
+    """Host-side parts of batching and serving, no device needed: the memory
+    estimate used for admission, and argument checks that return before any
+    device work."""
+    L = cf.lib()
+    big = cf.Config.make(order=4, nx=512, ny=512, nz=384, lx=6.28, ly=3.14, lz=2.0, dt=2.5e-4, nu=5e-5)
+    small = cf.Config.make(order=2, nx=64, ny=64, nz=64, lx=6.28, ly=3.14, lz=2.0, dt=1e-3, nu=1e-3)
+    chan = cf.Config.make(order=4, nx=512, ny=512, nz=384, lx=6.28, ly=3.14, lz=2.0, dt=2.5e-4, nu=5e-5,
+                          scheme="channel")
+    assert 13e9 < cf.instance_bytes(big) < 15e9          # 13 fields of 818 MB + spectrum + scratch
+    assert 30e6 < cf.instance_bytes(small) < 50e6
+    assert cf.instance_bytes(chan) > cf.instance_bytes(big)   # four spectra
+    bad = cf.Config.make(order=3, nx=64, ny=64, nz=64, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, nu=1e-3)
+    assert cf.instance_bytes(bad) == 0
+    res = (cf.Result * 2)()
+    reqs = (cf.Request * 2)()
+    for q in range(2):
+        reqs[q].cfg = small
+        reqs[q].nsteps = 1
+    reqs[0].arrival_s, reqs[1].arrival_s = 1.0, 0.5          # not in arrival order
+    cb = cf.DONE_FN(lambda i, h, u: None)
+    assert L.cf_serve(reqs, 2, 1e9, 4, 1, None, cb, None, res) == cf.CF_EINVAL
+    reqs[1].arrival_s = 2.0
+    assert L.cf_serve(reqs, 2, 1e9, 0, 1, None, cb, None, res) == cf.CF_EINVAL    # no slots
+    assert L.cf_serve(reqs, 2, 1e9, 4, 0, None, cb, None, res) == cf.CF_EINVAL    # empty rounds
+    reqs[1].cfg = chan                                          # the fully implicit scheme is not served
+    assert L.cf_serve(reqs, 2, 1e9, 4, 1, None, cb, None, res) == cf.CF_EINVAL
+    assert L.cf_batch_step(None, 0, 3, None) == cf.CF_EINVAL
+
+
+def test_ensemble_and_serving_traces_are_deterministic():
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    a, b = bench.ensemble_members(), bench.ensemble_members()
+    assert a == b and len(a) == 64
+    assert {(m["nx"], m["ny"], m["nz"]) for m in a} == set(bench.ENSEMBLE_GRIDS)
+    assert all(2800.0 <= m["re"] <= 10000.0 for m in a)
+    t = bench.serve_trace(2000, 4.0, 1.0)
+    assert t == bench.serve_trace(2000, 4.0, 1.0)
+    rate = len(t) / t[-1]["arrival_s"]
+    assert 3.6 < rate < 4.4                                     # Poisson arrivals at 4 per second
+    assert all(200 <= r["nsteps"] <= 2000 and r["order"] in (2, 4) for r in t)
+    assert all(2800.0 <= r["re"] <= 20000.0 for r in t)
