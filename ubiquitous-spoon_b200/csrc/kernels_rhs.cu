@@ -127,7 +127,9 @@ struct RhsTile {
     static constexpr int FIELD = SLOTS * PLANE;                  // one field's ring
     static constexpr int LOADS = (PLANE + RT_THREADS - 1) / RT_THREADS;   // plane points per thread
     static constexpr int BLOCKS = 1;                             // launch bound: blocks per SM
-    __host__ __device__ static constexpr int slot(int kk) { return kk % SLOTS; }
+    // plane kk >= 0 (every plane a row reads lies in 0 .. n2-1): an unsigned
+    // remainder, a single AND for the 8-slot ring
+    __host__ __device__ static constexpr int slot(int kk) { return (int) ((unsigned) kk % (unsigned) SLOTS); }
 };
 constexpr double B1h = 0.5 * B1, B2h = 0.5 * B2;   // halved interpolation weights (exact)
 // 7-point form of the fourth-order staggered second difference:
@@ -136,12 +138,13 @@ constexpr double B1h = 0.5 * B1, B2h = 0.5 * B2;   // halved interpolation weigh
 constexpr double L1 = A1 * A1 - 2.0 * A1 * A2, L2 = 2.0 * A1 * A2, L3 = A2 * A2;
 
 constexpr int RT_FWMAX = 14;   // widest fused forward row (order 4: 13), padded to 16-byte pairs
+constexpr int RT_MROW = 12;   // per-row grid metrics: dydz[k-1..k+2], dxdz[k-1..k+2], ivol[k], ivolw[k] (+2 pad)
 // ring of haloed planes + two rows of each thread's g values + two rows of
-// the four fused coefficient rows
+// the four fused coefficient rows + two rows of grid metrics
 template <int ORDER>
 constexpr size_t rhs_smem_bytes()
 {
-    return (size_t) (4 * RhsTile<ORDER>::FIELD + 2 * 4 * RT_THREADS + 2 * 4 * RT_FWMAX) * sizeof(double);
+    return (size_t) (4 * RhsTile<ORDER>::FIELD + 2 * 4 * RT_THREADS + 2 * 4 * RT_FWMAX + 2 * RT_MROW) * sizeof(double);
 }
 
 // z fluxes of one advected field (order 4), carried up the column.  With
@@ -210,17 +213,21 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
         goff[m] = gi * ny + gj;
     }
     auto load_plane = [&](int kk) {
-        const long long base = (long long) kk * plane;
+        const long long base = (long long) kk * plane;   // same for the whole block
+        const double* bu = A.u + base;
+        const double* bv = A.v + base;
+        const double* bw = A.w + base;
+        const double* bc = A.c + base;
         double* d0 = sm + T::slot(kk) * T::PLANE + tid;
 #pragma unroll
         for (int m = 0; m < T::LOADS; m++) {
             if (tid + m * RT_THREADS < T::PLANE) {
                 double* d = d0 + m * RT_THREADS;
-                const long long o = base + goff[m];
-                cp_async8(d, A.u + o);
-                cp_async8(d + T::FIELD, A.v + o);
-                cp_async8(d + 2 * T::FIELD, A.w + o);
-                cp_async8(d + 3 * T::FIELD, A.c + o);
+                const int o = goff[m];
+                cp_async8(d, bu + o);
+                cp_async8(d + T::FIELD, bv + o);
+                cp_async8(d + 2 * T::FIELD, bw + o);
+                cp_async8(d + 3 * T::FIELD, bc + o);
             }
         }
         cp_async_commit();
@@ -229,6 +236,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     // staged one row ahead so the sweeps never wait on global memory
     double* gst = sm + 4 * T::FIELD;              // [2][4][RT_THREADS]
     double* cst = gst + 2 * 4 * RT_THREADS;       // [2][4][RT_FWMAX]
+    double* mst = cst + 2 * 4 * RT_FWMAX;         // [2][RT_MROW]
     constexpr int FWR = (ORDER == 2 ? 3 : 7) + 6; // fused row width (host_band.h fused_rows)
     const long long gij = (i0 + ty < nx && j0 + tx < ny) ? (long long) (i0 + ty) * ny + (j0 + tx) : 0;
     auto load_extras = [&](int kk) {
@@ -241,6 +249,11 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
             if (!(f == 2 && kk - GZ >= G.nz - 1))   // the w solve has nz - 1 rows
                 cp_async8(cst + ((kk & 1) * 4 + f) * RT_FWMAX + e, A.sw[f].rows + (kk - GZ) * FWR + e);
         }
+        const int e = tid - 4 * FWR;   // grid metrics of row kk (rows kk-1 .. kk+2 lie within 0 .. n2-1)
+        if (e >= 0 && e < 10) {
+            const double* src = e < 4 ? G.dydz + kk - 1 + e : e < 8 ? G.dxdz + kk - 5 + e : e == 8 ? G.ivol + kk : G.ivolw + kk;
+            cp_async8(mst + (kk & 1) * RT_MROW + e, src);
+        }
     };
     load_extras(kb);
     for (int kk = kb - T::ZH; kk <= kb + T::ZH; kk++) load_plane(kk);
@@ -252,8 +265,6 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     const double dxdy = G.dxdy, idx = G.idx, idy = G.idy;
     const double idx2 = idx * idx, idy2 = idy * idy;
     const double lapc = -2.0 * (L1 + L2 + L3) * (idx2 + idy2);   // centre weight of the sum-form Laplacian
-    const double* __restrict__ dydz = G.dydz;
-    const double* __restrict__ dxdz = G.dxdz;
     const int kb_w = GZ - 1, kt_u = n2 - GZ;   // wall ghost rows of cell-centred fields
 
     int k = kb;
@@ -265,46 +276,42 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     auto W = [&](int di, int dj, int dk) { return at(2, di, dj, dk); };
     auto C = [&](int di, int dj, int dk) { return at(3, di, dj, dk); };
 
-    // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation
-    auto mx_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
-        return B1 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)) + B2 * (d * U(di - 1, dj, dk) + d * U(di + 2, dj, dk)); };
-    auto mx_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
-        return B1 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)) + B2 * (d * V(di - 1, dj, dk) + d * V(di + 2, dj, dk)); };
+    // grid metrics of the current row, staged one row ahead: dydz[k+dk],
+    // dxdz[k+dk] for dk = -1 .. 2, 1 / cell volume, 1 / w-face volume
+    auto DYDZ = [&](int dk) { return mst[(k & 1) * RT_MROW + 1 + dk]; };
+    auto DXDZ = [&](int dk) { return mst[(k & 1) * RT_MROW + 5 + dk]; };
+    // massflux{x,y,z}4 (advect.c:88-283): fourth-order interpolation of the
+    // w mass fluxes (the u and v ones are formed per face below)
     auto mx_w = [&](int di, int dj, int dk) {
         return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
-    auto my_u = [&](int di, int dj, int dk) { double d = dydz[k + dk];
+    auto my_u = [&](int di, int dj, int dk) { double d = DYDZ(dk);
         return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
-    auto my_v = [&](int di, int dj, int dk) { double d = dxdz[k + dk];
+    auto my_v = [&](int di, int dj, int dk) { double d = DXDZ(dk);
         return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
     auto my_w = [&](int di, int dj, int dk) {
         return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
-    auto mz_u = [&](int di, int dj, int dk) {
-        return B1 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1))
-             + B2 * (dydz[k + dk - 1] * U(di, dj, dk - 1) + dydz[k + dk + 2] * U(di, dj, dk + 2)); };
-    auto mz_v = [&](int di, int dj, int dk) {
-        return B1 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1))
-             + B2 * (dxdz[k + dk - 1] * V(di, dj, dk - 1) + dxdz[k + dk + 2] * V(di, dj, dk + 2)); };
     auto mz_w = [&](int di, int dj, int dk) {
         return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)) + B2 * (dxdy * W(di, dj, dk - 1) + dxdy * W(di, dj, dk + 2)); };
     // massflux{x,y,z}2 (advect.c:6-85)
-    auto mx_u2 = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
-    auto mx_v2 = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
+    auto mx_u2 = [&](int di, int dj, int dk) { double d = DYDZ(dk); return 0.5 * (d * U(di, dj, dk) + d * U(di + 1, dj, dk)); };
+    auto mx_v2 = [&](int di, int dj, int dk) { double d = DXDZ(dk); return 0.5 * (d * V(di, dj, dk) + d * V(di + 1, dj, dk)); };
     auto mx_w2 = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)); };
-    auto my_u2 = [&](int di, int dj, int dk) { double d = dydz[k + dk]; return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
-    auto my_v2 = [&](int di, int dj, int dk) { double d = dxdz[k + dk]; return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
+    auto my_u2 = [&](int di, int dj, int dk) { double d = DYDZ(dk); return 0.5 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)); };
+    auto my_v2 = [&](int di, int dj, int dk) { double d = DXDZ(dk); return 0.5 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)); };
     auto my_w2 = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)); };
-    auto mz_u2 = [&](int di, int dj, int dk) { return 0.5 * (dydz[k + dk] * U(di, dj, dk) + dydz[k + dk + 1] * U(di, dj, dk + 1)); };
-    auto mz_v2 = [&](int di, int dj, int dk) { return 0.5 * (dxdz[k + dk] * V(di, dj, dk) + dxdz[k + dk + 1] * V(di, dj, dk + 1)); };
+    auto mz_u2 = [&](int di, int dj, int dk) { return 0.5 * (DYDZ(dk) * U(di, dj, dk) + DYDZ(dk + 1) * U(di, dj, dk + 1)); };
+    auto mz_v2 = [&](int di, int dj, int dk) { return 0.5 * (DXDZ(dk) * V(di, dj, dk) + DXDZ(dk + 1) * V(di, dj, dk + 1)); };
     auto mz_w2 = [&](int di, int dj, int dk) { return 0.5 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj, dk + 1)); };
 
     const double qk = -0.125;   // QUICK coefficient (scalar.c:79-162)
-    auto quick = [&](double m, double cm1, double c0, double c1, double c2) {
-        // the upwind curvature x - 2y + z: (c1, c0, cm1) for m > 0, else
-        // (c2, c1, c0); the operands are chosen first, then one evaluation
-        const bool up = m > 0.0;
-        const double x = up ? c1 : c2, y = up ? c0 : c1, z = up ? cm1 : c0;
+    // The face value between cells c0 and c1 takes the upwind curvature
+    // x - 2y + z of (c1, c0, c-1) for m > 0, else of (c2, c1, c0): the
+    // curvature centred on the upwind cell.  Each point forms the curvatures
+    // of cells i-1, i, i+1 once per direction and both faces pick theirs.
+    auto curv = [](double x, double y, double z) { return x - 2.0 * y + z; };
+    auto quick = [&](double m, double c0, double c1, double kup, double kdn) {
         double cph = 0.5 * (c0 + c1);
-        cph += qk * (x - 2.0 * y + z);
+        cph += qk * (m > 0.0 ? kup : kdn);
         return m * cph;
     };
     // add_buoyancy is skipped when every betg is zero (adding exact zeros)
@@ -318,7 +325,10 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
         zq_v.prime(V, my_w);
         zq_w.prime(W, mz_w);
     }
-    double fzp_prev = quick(dxdy * W(0, 0, -1), C(0, 0, -2), C(0, 0, -1), C(0, 0, 0), C(0, 0, 1));
+    // z curvature of cell k (carried from row to row) and the scalar flux
+    // through the bottom face of the first row
+    double kz = curv(C(0, 0, 1), C(0, 0, 0), C(0, 0, -1));
+    double fzp_prev = quick(dxdy * W(0, 0, -1), C(0, 0, -1), C(0, 0, 0), curv(C(0, 0, 0), C(0, 0, -1), C(0, 0, -2)), kz);
 
     // Forward-sweep state: s of rows k-1, k-2, k-3 per field, the lazily
     // applied shifts of g (u: mdpdx, c: dcdt of the previous control step),
@@ -358,7 +368,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     // window reaches above the top face; other rows take a branch-free path.
     auto row = [&](auto wall_tag) {
         constexpr bool WALL = decltype(wall_tag)::value;
-        const double ivol = G.ivol[k];
+        const double ivol = mst[(k & 1) * RT_MROW + 8], ivolw = mst[(k & 1) * RT_MROW + 9];
         const bool do_w = !WALL || k < n2 - GZ - 1;
         const long long ijk = (long long) k * plane + gij;
         const double* gk = gst + (k & 1) * 4 * RT_THREADS + tid;   // g of this row (staged)
@@ -392,7 +402,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
                 double xmh = mz_u2(-1, 0, 0) * 0.5 * (q0 + W(-1, 0, 0));
                 double ymh = mz_v2(0, -1, 0) * 0.5 * (q0 + W(0, -1, 0));
                 double zmh = mz_w2(0, 0, -1) * 0.5 * (q0 + W(0, 0, -1));
-                fw = -((xph - xmh) + (yph - ymh) + (zph - zmh)) * G.ivolw[k];
+                fw = -((xph - xmh) + (yph - ymh) + (zph - zmh)) * ivolw;
             }
             // add_laplacexy_operator_{u,w}2 (diffuseu.c:286-313, diffusew.c:290-317)
             auto lap2 = [&](auto F, double nu) {
@@ -448,7 +458,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
                 }
                 return A1 * (zph - zmh) + A2 * (zp3 - zm3);
             };
-            const double mdy = dydz[k], mdx = dxdz[k];
+            const double mdy = DYDZ(0), mdx = DXDZ(0);
             zq_u.advance(U, mx_w);
             zq_v.advance(V, my_w);
             {
@@ -469,8 +479,8 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
                 zq_w.advance(W, mz_w);
                 // z interpolation of the u / v mass fluxes to the w face: the
                 // metric differs per plane, folded into four row constants
-                const double cu0 = B1h * dydz[k], cu1 = B1h * dydz[k + 1], cum = B2h * dydz[k - 1], cu2 = B2h * dydz[k + 2];
-                const double cv0 = B1h * dxdz[k], cv1 = B1h * dxdz[k + 1], cvm = B2h * dxdz[k - 1], cv2 = B2h * dxdz[k + 2];
+                const double cu0 = B1h * DYDZ(0), cu1 = B1h * DYDZ(1), cum = B2h * DYDZ(-1), cu2 = B2h * DYDZ(2);
+                const double cv0 = B1h * DXDZ(0), cv1 = B1h * DXDZ(1), cvm = B2h * DXDZ(-1), cv2 = B2h * DXDZ(2);
                 auto mu = [&](int di, int dj) {
                     return (cu0 * U(di, dj, 0) + cu1 * U(di, dj, 1)) + (cum * U(di, dj, -1) + cu2 * U(di, dj, 2));
                 };
@@ -479,7 +489,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
                 };
                 const double q0 = W(0, 0, 0);
                 fw = -((xflux(W, mu, q0) + yflux(W, mv, q0))
-                       + (A1 * (zq_w.f1 - zq_w.f1m) + A2 * (zq_w.f3 - zq_w.f3m[0]))) * G.ivolw[k];
+                       + (A1 * (zq_w.f1 - zq_w.f1m) + A2 * (zq_w.f3 - zq_w.f3m[0]))) * ivolw;
             }
             // add_laplacexy_operator_{u,w}4 (diffuseu.c:316-359, diffusew.c:320-363):
             // A1 (d+1/2 - d-1/2) + A2 (d+3/2 - d-3/2) of the staggered first
@@ -508,12 +518,17 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
         fc = IMPL3D ? 0.0 : lc;
 
         {   // flux_quick + advect_scalar (scalar.c:79-162), order independent
-            double c0 = C(0, 0, 0);
-            double fxp = quick(dydz[k] * U(0, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0), C(2, 0, 0));
-            double fxm = quick(dydz[k] * U(-1, 0, 0), C(-2, 0, 0), C(-1, 0, 0), c0, C(1, 0, 0));
-            double fyp = quick(dxdz[k] * V(0, 0, 0), C(0, -1, 0), c0, C(0, 1, 0), C(0, 2, 0));
-            double fym = quick(dxdz[k] * V(0, -1, 0), C(0, -2, 0), C(0, -1, 0), c0, C(0, 1, 0));
-            double fzp = quick(dxdy * W(0, 0, 0), C(0, 0, -1), c0, C(0, 0, 1), C(0, 0, 2));
+            const double c0 = C(0, 0, 0);
+            const double kx0 = curv(C(1, 0, 0), c0, C(-1, 0, 0)), ky0 = curv(C(0, 1, 0), c0, C(0, -1, 0));
+            const double kxm = curv(c0, C(-1, 0, 0), C(-2, 0, 0)), kxp = curv(C(2, 0, 0), C(1, 0, 0), c0);
+            const double kym = curv(c0, C(0, -1, 0), C(0, -2, 0)), kyp = curv(C(0, 2, 0), C(0, 1, 0), c0);
+            const double kzp = curv(C(0, 0, 2), C(0, 0, 1), c0);
+            double fxp = quick(DYDZ(0) * U(0, 0, 0), c0, C(1, 0, 0), kx0, kxp);
+            double fxm = quick(DYDZ(0) * U(-1, 0, 0), C(-1, 0, 0), c0, kxm, kx0);
+            double fyp = quick(DXDZ(0) * V(0, 0, 0), c0, C(0, 1, 0), ky0, kyp);
+            double fym = quick(DXDZ(0) * V(0, -1, 0), C(0, -1, 0), c0, kym, ky0);
+            double fzp = quick(dxdy * W(0, 0, 0), c0, C(0, 0, 1), kz, kzp);
+            kz = kzp;
             double fzm = fzp_prev;   // the top-face flux of row k-1
             fzp_prev = fzp;
             fc = -((fxp - fxm) + (fyp - fym) + (fzp - fzm)) * ivol + fc;
