@@ -241,6 +241,9 @@ def run_ours(args):
     b_alg = w.get("b_alg", B_ALG)
     stream = torch.cuda.Stream()
     inst = cf.Instance(cfg, stream=ctypes_stream(stream))
+    if args.launch_shape:
+        inst.set_launch_shape(tuple(int(x) for x in args.launch_shape.split(",")))
+    shape = list(inst.launch_shape())
     inst.init_fields(w["seed"] + rank, w["amp"], w["c_amp"])
     inst.step_graph(args.warmup)
     inst.sync()
@@ -334,7 +337,9 @@ def run_ours(args):
                    "step": "one RK3 time step = 3 substeps",
                    "l2": f"inputs larger than L2 ({pts * (w['nz'] + 6) // w['nz'] * 8 / 1e6:.0f} MB per field, "
                          "4 fields read per kernel vs 126 MB L2); no flush",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single instance"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single instance",
+                   "launch_shape": {"solve_threads": shape[0], "poisson_threads": shape[1],
+                                    "project_block": shape[2:]}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "max_divergence": div,
     }
@@ -387,7 +392,10 @@ def run_ensemble(args):
     pts = sum(m["nx"] * m["ny"] * m["nz"] for m in members)
     # batched
     insts = create()
-    B = cf.Batch(insts)
+    t0 = time.perf_counter()
+    B = cf.Batch(insts)   # records the cycle and tunes the batched launch shapes
+    t_create = time.perf_counter() - t0
+    batch_shape = list(B.launch_shape())
     B.run(args.warmup)
     B.sync()
     with ClockSampler(0) as clk:
@@ -418,6 +426,9 @@ def run_ensemble(args):
         "metric": "ensemble solves/h", "value": round(per_h(t_batch), 1), "unit": "solves/h",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "sequential_plain_path": round(per_h(t_seq), 1), "speedup_vs_sequential": round(t_seq / t_batch, 2),
+        "batch_launch_shape": {"solve_threads": batch_shape[0], "poisson_threads": batch_shape[1],
+                               "project_block": batch_shape[2:]},
+        "batch_create_s": round(t_create, 3),
         "mpt_substeps_per_s": round(pts * 3 * args.steps / t_batch / 1e6, 1),
         "ms_per_step_all_members": round(t_batch / args.steps * 1e3, 3),
         "batched_launches_per_substep": launches, "dtype": "f64", "data": "synthetic",
@@ -544,6 +555,8 @@ def main():
                     help="scale of the U[200, 2000] step counts (1.0 = the full trace)")
     ap.add_argument("--serve-baseline", action="store_true", help="also serve the trace one solve at a time")
     ap.add_argument("--serve-quantum", type=int, default=1, help="RK3 steps per serving round")
+    ap.add_argument("--launch-shape", default="",
+                    help="force the tuned kernels' launch shape: solve,poisson,proj_bx,proj_by")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 (default) is the benchmark; the others serve profiling and checks")
     args = ap.parse_args()

@@ -209,6 +209,30 @@ int cf_batch_launches_per_substep(const cf_batch *batch);
 int cf_batch_destroy(cf_batch *batch);
 
 /* ------------------------------------------------------------------------
+ * Launch-shape autotuning.  Three kernels run with any of a few block shapes
+ * and give the same results bit for bit: the back substitution (columns per
+ * block: 64, 128), the Poisson / spectral Helmholtz band solve (column
+ * pairs per block: 64, 128) and the projection (block of j by i: 32x2, 32x4,
+ * 32x8, 64x2).  cf_create times the candidates on the new instance (before
+ * it holds state) and keeps the fastest; cf_batch_create does the same on
+ * the batch's own launches with their outputs in scratch memory.  Results
+ * are cached per configuration (per member set for a batch) for the process
+ * and, when the environment variable CF_TUNE_CACHE names a file, across
+ * processes (one line per key: "key solve pois proj_bx proj_by").
+ * cf_batch_step uses the cached shape of its member set, else the defaults.
+ *
+ * cf_set_tuning(0) (or CF_TUNE=0 in the environment) turns tuning off: new
+ * instances and batches use the default shapes 128, 128, 32x4.
+ * A shape is four ints: solve threads, Poisson threads, projection block x,
+ * projection block y.  cf_set_launch_shape rejects shapes outside the
+ * candidates with CF_EINVAL.
+ * ---------------------------------------------------------------------- */
+int cf_set_tuning(int on);
+int cf_get_launch_shape(const cf_instance *inst, int shape[4]);
+int cf_set_launch_shape(cf_instance *inst, const int shape[4]);
+int cf_batch_get_launch_shape(const cf_batch *batch, int shape[4]);
+
+/* ------------------------------------------------------------------------
  * Serving: a request loop over the instance and batch calls.
  *
  * cf_instance_bytes: device memory an instance of this configuration holds

@@ -137,6 +137,11 @@ def _bind(L):
     L.cf_batch_sync.argtypes = [vp]
     L.cf_batch_launches_per_substep.argtypes = [vp]
     L.cf_batch_destroy.argtypes = [vp]
+    i4 = ctypes.c_int * 4
+    L.cf_set_tuning.argtypes = [ip]
+    L.cf_get_launch_shape.argtypes = [vp, i4]
+    L.cf_set_launch_shape.argtypes = [vp, i4]
+    L.cf_batch_get_launch_shape.argtypes = [vp, i4]
     return L
 
 
@@ -297,6 +302,21 @@ class Instance:
     def launches_per_substep(self):
         return int(self.L.cf_launches_per_substep(self.h))
 
+    def launch_shape(self):
+        """Tuned launch shape: (back-substitution threads, Poisson threads,
+        projection block x, projection block y)."""
+        out = (ctypes.c_int * 4)()
+        _check(self.L.cf_get_launch_shape(self.h, out), "cf_get_launch_shape")
+        return tuple(out)
+
+    def set_launch_shape(self, shape):
+        _check(self.L.cf_set_launch_shape(self.h, (ctypes.c_int * 4)(*shape)), "cf_set_launch_shape")
+
+
+def set_tuning(on):
+    """Launch-shape tuning of new instances and batches on (default) or off."""
+    _check(lib().cf_set_tuning(1 if on else 0), "cf_set_tuning")
+
 
 def instance_bytes(cfg):
     """Device bytes an instance of this configuration holds (cf_instance_bytes)."""
@@ -374,6 +394,11 @@ class Batch:
 
     def launches_per_substep(self):
         return int(self.L.cf_batch_launches_per_substep(self.h))
+
+    def launch_shape(self):
+        out = (ctypes.c_int * 4)()
+        _check(self.L.cf_batch_get_launch_shape(self.h, out), "cf_batch_get_launch_shape")
+        return tuple(out)
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

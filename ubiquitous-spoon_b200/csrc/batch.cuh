@@ -45,12 +45,14 @@ __device__ __forceinline__ const Rec& batch_locate(const Rec* __restrict__ r, in
 
 // One batched launch: `recs` points at n device records whose grids add up
 // to `blocks` flat blocks; `smem` is the dynamic shared memory of the
-// largest instance.
+// largest instance; `block` the block shape of the kernels with a tuned
+// shape (every record's grid was formed with it).
 struct BatchLaunch {
     const void* recs;
     int n;
     unsigned blocks;
     size_t smem;
+    dim3 block;
 };
 
 }  // namespace cf

@@ -26,8 +26,26 @@ struct WallRowsD {
     double row[3][7];
 };
 
+// Launch shapes of the kernels whose block shape is free: the tuner
+// (instance.cu, cf_tune) times the candidates and keeps the fastest; the
+// defaults are the hand-picked shapes.  Results do not depend on the choice:
+// these kernels index their work from blockDim, one column (pair, point) per
+// thread, and the per-warp row sums of k_back4 cover the same 32 columns
+// whatever the block size.
+struct LaunchShape {
+    int solve_threads = 128;           // k_back4: columns per block (64, 128)
+    int pois_threads = 128;            // k_poisson / k_helmholtz_spectral: column pairs per block (64, 128)
+    int proj_bx = 32, proj_by = 4;     // k_project block: j by i (32x2, 32x4, 32x8, 64x2)
+};
+// k_back4 is bound to 128 threads: a 256-thread bound costs it 4 registers
+// and one resident block per SM (measured 40 % slower)
+constexpr int SOLVE_THREADS_MAX = 128;
+constexpr int POIS_THREADS_MAX = 128;
+constexpr int PROJ_THREADS_MAX = 256;
+
 // Geometry / metric tables shared by all kernels of an instance.
 struct Geo {
+    LaunchShape shape;    // tuned launch shapes (host side; kernels read blockDim)
     int order, nx, ny, nz, n2, nkx;
     long long plane;      // nx*ny (points per k-plane)
     long long splane;     // nkx*ny (spectral columns per k-plane)
@@ -183,10 +201,10 @@ struct PoissonArgs {
     double abc_bot, abc_top;  // and its wall values
 };
 
-constexpr int POIS_THREADS = 128;  // k_poisson block: one thread per (kx, +-ky) column pair
+// k_poisson block: one thread per (kx, +-ky) column pair, LaunchShape::pois_threads per block
 constexpr int POIS_PF = 8;         // forward rows in flight per thread (both columns)
 constexpr int POIS_PB = 2;         // back-substitution rows loaded ahead (registers)
-inline size_t pois_smem_bytes() { return (size_t) POIS_PF * 2 * POIS_THREADS * 16; }
+inline size_t pois_smem_bytes(int threads) { return (size_t) POIS_PF * 2 * threads * 16; }
 
 struct ProjArgs {
     double *u, *v, *w, *c;
@@ -202,7 +220,7 @@ struct ProjArgs {
 // otherwise as apply_bc_w leaves them (after the spectral solves)
 void launch_ghosts(const Geo& G, const GhostArgs& A, cudaStream_t st, bool extrap = true);
 void launch_rhs(const Geo& G, const RhsArgs& A, bool implicit3d, cudaStream_t st);
-constexpr int SOLVE_THREADS = 128;   // k_back4 block: one thread per column
+// k_back4 block: one thread per column, LaunchShape::solve_threads per block
 struct SolveBatch {
     SolveArgs a[4];   // u, v, c, w
 };

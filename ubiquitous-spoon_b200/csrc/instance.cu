@@ -8,8 +8,10 @@
 //   scalar-mean control c -> solve w -> divergence+x FFT -> y FFT ->
 //   Poisson -> inverse y FFT -> inverse x FFT -> projection
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -993,7 +995,8 @@ struct BatchProgram {
 // Append one group per key of `recs` to P: records laid out contiguously
 // with their first flat blocks, one batched launch each.
 template <class Args, class KeyFn, class SmemFn>
-void add_groups(BatchProgram& P, int kernel, const std::vector<BatchRec<Args>>& recs, KeyFn key, SmemFn smem)
+void add_groups(BatchProgram& P, int kernel, const std::vector<BatchRec<Args>>& recs, KeyFn key, SmemFn smem,
+                dim3 block = dim3(1, 1, 1))
 {
     std::map<int, std::vector<BatchRec<Args>>> groups;
     for (const auto& r : recs) groups[key(r)].push_back(r);
@@ -1016,8 +1019,24 @@ void add_groups(BatchProgram& P, int kernel, const std::vector<BatchRec<Args>>& 
         op.L.n = (int) g.size();
         op.L.blocks = begin;
         op.L.smem = sm;
+        op.L.block = block;
         P.ops.push_back(op);
     }
+}
+
+// Block shape of a batched launch of a tuned kernel: every record of a batch
+// is recorded with the batch's one launch shape (record()).
+dim3 back4_block(const std::vector<BatchRec<SolveBatch>>& r)
+{
+    return dim3(r.empty() ? 128 : r[0].G.shape.solve_threads);
+}
+dim3 poisson_block(const std::vector<BatchRec<PoissonArgs>>& r)
+{
+    return dim3(r.empty() ? 128 : r[0].G.shape.pois_threads);
+}
+dim3 project_block(const std::vector<BatchRec<ProjArgs>>& r)
+{
+    return r.empty() ? dim3(32, 4) : dim3(r[0].G.shape.proj_bx, r[0].G.shape.proj_by);
 }
 
 void compile(const BatchSink& K, BatchProgram& P)
@@ -1033,7 +1052,7 @@ void compile(const BatchSink& K, BatchProgram& P)
         switch (S.kind) {
         case ST_GHOSTS: add_groups(P, BK_GHOSTS, S.ghosts, order, none); break;
         case ST_RHS: add_groups(P, BK_RHS, S.rhs, order, none); break;
-        case ST_BACK4: add_groups(P, BK_BACK4, S.back4, order, none); break;
+        case ST_BACK4: add_groups(P, BK_BACK4, S.back4, order, none, back4_block(S.back4)); break;
         case ST_MASS:
             add_groups(P, BK_ROWAVG, S.rowavg, none, none);
             add_groups(P, BK_CONTROL, S.control, none, none);
@@ -1045,9 +1064,9 @@ void compile(const BatchSink& K, BatchProgram& P)
                        smem_nx);
             break;
         case ST_FFTY: add_groups(P, BK_FFTY, S.ffty, keyny, smem_ny); break;
-        case ST_POISSON: add_groups(P, BK_POISSON, S.poisson, order, none); break;
+        case ST_POISSON: add_groups(P, BK_POISSON, S.poisson, order, none, poisson_block(S.poisson)); break;
         case ST_C2R: add_groups(P, BK_C2R, S.c2r, keynx, smem_nx); break;
-        default: add_groups(P, BK_PROJECT, S.project, order, none); break;
+        default: add_groups(P, BK_PROJECT, S.project, order, none, project_block(S.project)); break;
         }
     }
 }
@@ -1082,12 +1101,19 @@ void run_program(const BatchProgram& P, cudaStream_t st)
     }
 }
 
-// Record `nsub` substeps of every member into P (this advances each member's
-// host-side substep counter and f/g roles, as stepping would).
-int record(const std::vector<cf_instance*>& v, int nsub, BatchProgram& P)
+// Record `nsub` substeps of every member into K (this advances each member's
+// host-side substep counter and f/g roles, as stepping would), every member
+// with the launch shape `shape` (a batched launch has one block shape; the
+// members' own shapes are put back afterwards).
+int record_sink(const std::vector<cf_instance*>& v, int nsub, const LaunchShape& shape, BatchSink& K)
 {
-    BatchSink K;
-    for (int q = 0; q < nsub; q++) {
+    std::vector<LaunchShape> own;
+    for (cf_instance* I : v) {
+        own.push_back(I->geo.shape);
+        I->geo.shape = shape;
+    }
+    int rc = CF_OK;
+    for (int q = 0; q < nsub && rc == CF_OK; q++) {
         const size_t base = K.stages.size();
         size_t per = 0;
         for (size_t m = 0; m < v.size(); m++) {
@@ -1097,10 +1123,20 @@ int record(const std::vector<cf_instance*>& v, int nsub, BatchProgram& P)
             if (m == 0) per = n;
             if (n != per || K.mismatch) {
                 g_last_error = "batch members emit different stage sequences";
-                return CF_EINVAL;
+                rc = CF_EINVAL;
+                break;
             }
         }
     }
+    for (size_t m = 0; m < v.size(); m++) v[m]->geo.shape = own[m];
+    return rc;
+}
+
+int record(const std::vector<cf_instance*>& v, int nsub, BatchProgram& P, const LaunchShape& shape)
+{
+    BatchSink K;
+    const int rc = record_sink(v, nsub, shape, K);
+    if (rc) return rc;
     compile(K, P);
     P.substeps = nsub;
     return CF_OK;
@@ -1153,7 +1189,354 @@ struct cf_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaEvent_t ev = nullptr;
+    LaunchShape shape;              // launch shape of the tuned kernels (tune_batch)
 };
+
+// ====================================================================== tuner
+//
+// Launch-shape autotuner.  Three kernels run with any of a few block shapes
+// and give the same results (LaunchShape, engine.cuh): k_back4 (columns per
+// block), k_poisson / k_helmholtz_spectral (column pairs per block) and
+// k_project (2-D block).  The tuner captures one substep's arguments of those
+// stages, times every candidate shape of each kernel with CUDA events on the
+// instance's stream (one warm-up launch, then TUNE_REPS launches), and keeps
+// the fastest.  Choices are cached per configuration for the process, and in
+// the text file named by CF_TUNE_CACHE when that is set (one line per key:
+// key solve pois proj_bx proj_by), so every size is timed once.
+//
+// * A single instance is tuned when it is created, before it holds any state:
+//   the timed launches write its fields (zeroed again afterwards), its
+//   spectrum and its scratch.
+// * A batch is tuned when it is created (cf_batch_create), on its own batched
+//   launches with every output those launches write redirected to scratch
+//   device memory, so the members' state is untouched.  It is skipped (the
+//   default shapes are used) when that scratch would not fit in free memory.
+//   cf_batch_step uses the cached shape of its member set, else the defaults.
+//
+// CF_TUNE=0 in the environment, or cf_set_tuning(0), turns tuning off.
+
+namespace {
+
+const int TUNE_SOLVE[] = {64, 128};
+const int TUNE_POIS[] = {64, 128};
+const int TUNE_PROJ[][2] = {{32, 2}, {32, 4}, {32, 8}, {64, 2}};
+constexpr int TUNE_REPS = 3;
+
+std::mutex g_tune_mu;
+std::map<std::string, LaunchShape> g_tune_cache;
+bool g_tune_file_read = false;
+int g_tune_mode = -1;   // -1: not decided yet (CF_TUNE), 0 off, 1 on
+
+bool tune_enabled()
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune_mode < 0) {
+        const char* e = std::getenv("CF_TUNE");
+        g_tune_mode = (e && e[0] == '0') ? 0 : 1;
+    }
+    return g_tune_mode == 1;
+}
+
+bool shape_valid(const LaunchShape& S)
+{
+    bool a = false, b = false, c = false;
+    for (int t : TUNE_SOLVE) a |= S.solve_threads == t;
+    for (int t : TUNE_POIS) b |= S.pois_threads == t;
+    for (const auto& t : TUNE_PROJ) c |= S.proj_bx == t[0] && S.proj_by == t[1];
+    return a && b && c;
+}
+
+// Cache file: "key solve pois proj_bx proj_by" per line; unreadable or
+// malformed lines are ignored.
+void tune_read_file_locked()
+{
+    if (g_tune_file_read) return;
+    g_tune_file_read = true;
+    const char* path = std::getenv("CF_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[512];
+    LaunchShape S;
+    while (std::fscanf(f, "%511s %d %d %d %d", key, &S.solve_threads, &S.pois_threads, &S.proj_bx, &S.proj_by) == 5)
+        if (shape_valid(S)) g_tune_cache[key] = S;
+    std::fclose(f);
+}
+
+bool tune_lookup(const std::string& key, LaunchShape& out)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_read_file_locked();
+    auto it = g_tune_cache.find(key);
+    if (it == g_tune_cache.end()) return false;
+    out = it->second;
+    return true;
+}
+
+void tune_store(const std::string& key, const LaunchShape& S)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = S;
+    const char* path = std::getenv("CF_TUNE_CACHE");
+    if (!path || !*path) return;
+    if (FILE* f = std::fopen(path, "a")) {
+        std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), S.solve_threads, S.pois_threads, S.proj_bx, S.proj_by);
+        std::fclose(f);
+    }
+}
+
+std::string device_tag(int device)
+{
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return "sm" + std::to_string(sms);
+}
+
+std::string config_key(const cf_instance* I)
+{
+    const cf_config& C = I->cfg;
+    return "o" + std::to_string(C.order) + "s" + std::to_string(C.scheme) + "-" + std::to_string(C.nx) + "x"
+         + std::to_string(C.ny) + "x" + std::to_string(C.nz);
+}
+
+// Key of a member set: its configurations with their counts, sorted.
+std::string batch_key(const std::vector<cf_instance*>& v)
+{
+    std::map<std::string, int> n;
+    for (const cf_instance* I : v) n[config_key(I)]++;
+    std::string k = device_tag(v[0]->device) + ":batch";
+    for (const auto& kv : n) k += ":" + kv.first + "*" + std::to_string(kv.second);
+    return k;
+}
+
+// Mean device time of `launch` over TUNE_REPS launches after one warm-up.
+template <class F>
+int time_launch(cudaStream_t st, F launch, float& ms)
+{
+    cudaEvent_t a, b;
+    CF_CUDA(cudaEventCreate(&a));
+    CF_CUDA(cudaEventCreate(&b));
+    launch();
+    cudaEventRecord(a, st);
+    for (int r = 0; r < TUNE_REPS; r++) launch();
+    cudaEventRecord(b, st);
+    cudaError_t e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    float t = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("tuning: ") + cudaGetErrorString(e);
+        return CF_ECUDA;
+    }
+    ms = t / TUNE_REPS;
+    return CF_OK;
+}
+
+// Arguments of the tuned stages of one substep.
+struct CaptureSink : Sink {
+    Geo G{};
+    bool has_back4 = false, has_pois = false, has_proj = false;
+    SolveBatch back4_args{};
+    PoissonArgs pois_args{};
+    ProjArgs proj_args{};
+    void mark() override {}
+    void ghosts(const Geo&, const GhostArgs&) override {}
+    void rhs(const Geo&, const RhsArgs&) override {}
+    void back4(const Geo& g, const SolveBatch& B) override { G = g; back4_args = B; has_back4 = true; }
+    void mass(const Geo&, const double*, double*, const MassArgs&) override {}
+    void div_fftx(const Geo&, const DivArgs&) override {}
+    void ffty(const Geo&, const FftyArgs&, int) override {}
+    void poisson(const Geo& g, const PoissonArgs& A) override { G = g; pois_args = A; has_pois = true; }
+    void c2r(const Geo&, const C2rArgs&, int) override {}
+    void project(const Geo& g, const ProjArgs& A) override { G = g; proj_args = A; has_proj = true; }
+};
+
+// Fastest candidate of each tuned kernel; `run(kind, shape)` launches that
+// kernel once with the shape (kind 0 back4, 1 Poisson, 2 projection).
+template <class Run>
+int tune_shapes(cudaStream_t st, bool with_back4, Run run, LaunchShape& best)
+{
+    best = LaunchShape{};
+    float bt = 1e30f, t = 0.0f;
+    if (with_back4) {
+        for (int c : TUNE_SOLVE) {
+            LaunchShape S = best;
+            S.solve_threads = c;
+            int rc = time_launch(st, [&] { run(0, S); }, t);
+            if (rc) return rc;
+            if (t < bt) { bt = t; best.solve_threads = c; }
+        }
+    }
+    bt = 1e30f;
+    for (int c : TUNE_POIS) {
+        LaunchShape S = best;
+        S.pois_threads = c;
+        int rc = time_launch(st, [&] { run(1, S); }, t);
+        if (rc) return rc;
+        if (t < bt) { bt = t; best.pois_threads = c; }
+    }
+    bt = 1e30f;
+    for (const auto& c : TUNE_PROJ) {
+        LaunchShape S = best;
+        S.proj_bx = c[0];
+        S.proj_by = c[1];
+        int rc = time_launch(st, [&] { run(2, S); }, t);
+        if (rc) return rc;
+        if (t < bt) { bt = t; best.proj_bx = c[0]; best.proj_by = c[1]; }
+    }
+    return CF_OK;
+}
+
+}  // namespace
+
+// Tune a newly created instance (no state yet); cached per configuration.
+int tune_instance(cf_instance* I)
+{
+    if (!tune_enabled()) return CF_OK;
+    const std::string key = device_tag(I->device) + ":" + config_key(I);
+    LaunchShape S;
+    if (tune_lookup(key, S)) {
+        I->geo.shape = S;
+        return CF_OK;
+    }
+    CaptureSink K;
+    double* fb[4];
+    double* gb[4];
+    for (int q = 0; q < 4; q++) { fb[q] = I->fbuf[q]; gb[q] = I->gbuf[q]; }
+    const long sub = I->substep;
+    if (I->cfg.scheme == CF_SCHEME_CHANNEL) pressure_sequence(I, I->pois[0], I->cfg.dt, 0, true, K);
+    else enqueue_substep(I, K);
+    for (int q = 0; q < 4; q++) { I->fbuf[q] = fb[q]; I->gbuf[q] = gb[q]; }
+    I->substep = sub;
+    if (!K.has_pois || !K.has_proj) return CF_OK;
+    auto run = [&](int kind, const LaunchShape& sh) {
+        Geo G = K.G;
+        G.shape = sh;
+        if (kind == 0) launch_back4(G, K.back4_args, I->stream);
+        else if (kind == 1) launch_poisson(G, K.pois_args, I->stream);
+        else launch_project(G, K.proj_args, I->stream);
+    };
+    int rc = tune_shapes(I->stream, K.has_back4, run, S);
+    if (rc) return rc;
+    // the timed launches wrote the fields: zero them as creation leaves them
+    const size_t fbytes = (size_t) I->geo.plane * I->geo.n2 * sizeof(double);
+    for (double* f : {I->u, I->v, I->w, I->c}) CF_CUDA(cudaMemsetAsync(f, 0, fbytes, I->stream));
+    CF_CUDA(cudaStreamSynchronize(I->stream));
+    I->geo.shape = S;
+    tune_store(key, S);
+    return CF_OK;
+}
+
+// Launch shape of a member set for cf_batch_step: cached, else the defaults.
+LaunchShape batch_cached_shape(const std::vector<cf_instance*>& v)
+{
+    LaunchShape S;
+    if (tune_enabled()) tune_lookup(batch_key(v), S);
+    return S;
+}
+
+// Tune the batched launches of a member set (cf_batch_create); outputs
+// redirected to scratch.  The members' host state is restored.
+int tune_batch(const std::vector<cf_instance*>& v, cudaStream_t st, LaunchShape& out)
+{
+    out = LaunchShape{};
+    if (!tune_enabled()) return CF_OK;
+    const std::string key = batch_key(v);
+    if (tune_lookup(key, out)) return CF_OK;
+    // one substep of every member, recorded and put back
+    std::vector<std::array<double*, 8>> fg(v.size());
+    std::vector<long> sub(v.size());
+    for (size_t m = 0; m < v.size(); m++) {
+        for (int q = 0; q < 4; q++) { fg[m][q] = v[m]->fbuf[q]; fg[m][4 + q] = v[m]->gbuf[q]; }
+        sub[m] = v[m]->substep;
+    }
+    BatchSink K;
+    int rc = record_sink(v, 1, LaunchShape{}, K);
+    for (size_t m = 0; m < v.size(); m++) {
+        for (int q = 0; q < 4; q++) { v[m]->fbuf[q] = fg[m][q]; v[m]->gbuf[q] = fg[m][4 + q]; }
+        v[m]->substep = sub[m];
+    }
+    if (rc) return rc;
+    std::vector<BatchRec<SolveBatch>> back4;
+    std::vector<BatchRec<PoissonArgs>> pois;
+    std::vector<BatchRec<ProjArgs>> proj;
+    for (const BatchStage& S : K.stages) {
+        if (S.kind == ST_BACK4) back4 = S.back4;
+        if (S.kind == ST_POISSON) pois = S.poisson;
+        if (S.kind == ST_PROJECT) proj = S.project;
+    }
+    if (back4.size() != v.size() || pois.size() != v.size() || proj.size() != v.size()) return CF_OK;
+    // scratch: four fields and two row-sum blocks per member
+    size_t need = 0;
+    std::vector<size_t> off(v.size());
+    for (size_t m = 0; m < v.size(); m++) {
+        const Geo& G = v[m]->geo;
+        const size_t nw = (size_t) ((G.plane + SOLVE_THREADS_MAX - 1) / SOLVE_THREADS_MAX) * (SOLVE_THREADS_MAX / 32);
+        off[m] = need;
+        need += 4 * (size_t) G.plane * G.n2 + 2 * nw * G.n2;
+    }
+    size_t free_b = 0, total_b = 0;
+    CF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (need * sizeof(double) > free_b / 2) return CF_OK;   // no room: defaults
+    double* scr = nullptr;
+    CF_CUDA(cudaMalloc(&scr, need * sizeof(double)));
+    for (size_t m = 0; m < v.size(); m++) {
+        const Geo& G = v[m]->geo;
+        const size_t fsz = (size_t) G.plane * G.n2;
+        double* base = scr + off[m];
+        const size_t nw = (size_t) ((G.plane + SOLVE_THREADS_MAX - 1) / SOLVE_THREADS_MAX) * (SOLVE_THREADS_MAX / 32);
+        for (int q = 0; q < 4; q++) back4[m].A.a[q].x = base + q * fsz;
+        back4[m].A.a[0].partial = back4[m].A.a[0].partial ? base + 4 * fsz : nullptr;
+        back4[m].A.a[2].partial = back4[m].A.a[2].partial ? base + 4 * fsz + nw * G.n2 : nullptr;
+        proj[m].A.u = base;
+        proj[m].A.v = base + fsz;
+        proj[m].A.w = base + 2 * fsz;
+        proj[m].A.c = base + 3 * fsz;
+    }
+    // one program per candidate (records regridded with the candidate
+    // shape), built and uploaded at its first (warm-up) launch
+    std::map<std::array<int, 5>, BatchProgram> progs;
+    auto run = [&](int kind, const LaunchShape& sh) {
+        const std::array<int, 5> code{kind, sh.solve_threads, sh.pois_threads, sh.proj_bx, sh.proj_by};
+        auto it = progs.find(code);
+        if (it != progs.end()) {
+            run_program(it->second, st);
+            return;
+        }
+        BatchProgram P;
+        auto order = [](const auto& r) { return r.G.order; };
+        auto none = [](const auto&) { return 0; };
+        if (kind == 0) {
+            auto recs = back4;
+            for (auto& r : recs) { r.G.shape = sh; dim3 g = grid_back4(r.G); r.gx = g.x; r.gy = g.y; r.gz = g.z; }
+            add_groups(P, BK_BACK4, recs, order, none, back4_block(recs));
+        } else if (kind == 1) {
+            auto recs = pois;
+            for (auto& r : recs) { r.G.shape = sh; dim3 g = grid_poisson(r.G); r.gx = g.x; r.gy = g.y; r.gz = g.z; }
+            add_groups(P, BK_POISSON, recs, order, none, poisson_block(recs));
+        } else {
+            auto recs = proj;
+            for (auto& r : recs) { r.G.shape = sh; dim3 g = grid_project(r.G); r.gx = g.x; r.gy = g.y; r.gz = g.z; }
+            add_groups(P, BK_PROJECT, recs, order, none, project_block(recs));
+        }
+        if (upload(P, st) != CF_OK) return;
+        run_program(P, st);
+        progs.emplace(code, P);
+    };
+    rc = tune_shapes(st, true, run, out);
+    cudaStreamSynchronize(st);
+    for (auto& kv : progs)
+        if (kv.second.dblob) cudaFree(kv.second.dblob);
+    cudaFree(scr);
+    if (rc) {
+        out = LaunchShape{};
+        return rc;
+    }
+    tune_store(key, out);
+    return CF_OK;
+}
 
 // ======================================================================= C ABI
 
@@ -1239,7 +1622,8 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     CF_CUDA(cudaMemsetAsync(I->spec, 0, nspec * sizeof(double2), I->stream));
     const int nscr = C.order == 4 ? 3 : 1;
     CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
-    const long long nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);   // per-warp partial sums of k_back4
+    // per-warp partial sums of k_back4, for its largest block size
+    const long long nwarps = ((G.plane + SOLVE_THREADS_MAX - 1) / SOLVE_THREADS_MAX) * (SOLVE_THREADS_MAX / 32);
     CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->partial_c, (size_t) nwarps * G.n2 * sizeof(double)));
     CF_CUDA(cudaMalloc(&I->avg, (size_t) G.n2 * sizeof(double)));
@@ -1281,7 +1665,7 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     rc = build_tables(I, C.dt);
     if (rc) return rc;
     CF_CUDA(cudaStreamSynchronize(I->stream));
-    return CF_OK;
+    return tune_instance(I);
 }
 
 int cf_create(const cf_config* cfg, void* stream, cf_instance** out)
@@ -1583,7 +1967,7 @@ int cf_batch_step(cf_instance** members, int n, int nsub, void* stream)
     std::vector<cf_instance*> v(members, members + n);
     cudaStream_t st = stream ? (cudaStream_t) stream : v[0]->stream;
     BatchProgram P;
-    rc = record(v, nsub, P);
+    rc = record(v, nsub, P, batch_cached_shape(v));
     if (rc) return rc;
     cudaEvent_t ev;
     CF_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -1601,6 +1985,51 @@ int cf_batch_step(cf_instance** members, int n, int nsub, void* stream)
     if (rc == CF_OK) rc = join_streams(v, st, ev, false);
     cudaEventDestroy(ev);
     return rc;
+}
+
+int cf_set_tuning(int on)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_mode = on ? 1 : 0;
+    return CF_OK;
+}
+
+static void shape_out(const LaunchShape& S, int* out)
+{
+    out[0] = S.solve_threads;
+    out[1] = S.pois_threads;
+    out[2] = S.proj_bx;
+    out[3] = S.proj_by;
+}
+
+int cf_get_launch_shape(const cf_instance* I, int shape[4])
+{
+    if (!I || !shape) return CF_EINVAL;
+    shape_out(I->geo.shape, shape);
+    return CF_OK;
+}
+
+int cf_set_launch_shape(cf_instance* I, const int shape[4])
+{
+    if (!I || !shape) return CF_EINVAL;
+    LaunchShape S;
+    S.solve_threads = shape[0];
+    S.pois_threads = shape[1];
+    S.proj_bx = shape[2];
+    S.proj_by = shape[3];
+    if (!shape_valid(S)) return CF_EINVAL;
+    I->geo.shape = S;
+    // the captured graph holds the old launches
+    if (I->gexec) { cudaGraphExecDestroy(I->gexec); I->gexec = nullptr; }
+    if (I->graph) { cudaGraphDestroy(I->graph); I->graph = nullptr; }
+    return CF_OK;
+}
+
+int cf_batch_get_launch_shape(const cf_batch* B, int shape[4])
+{
+    if (!B || !shape) return CF_EINVAL;
+    shape_out(B->shape, shape);
+    return CF_OK;
 }
 
 int cf_batch_destroy(cf_batch* B)
@@ -1632,10 +2061,13 @@ static int batch_create_impl(cf_batch* B, cf_instance** members, int n, void* st
         B->own_stream = true;
     }
     CF_CUDA(cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming));
+    int trc = join_streams(B->v, B->stream, B->ev, true);   // members' pending work first
+    if (trc == CF_OK) trc = tune_batch(B->v, B->stream, B->shape);
+    if (trc) return trc;
     std::vector<long> start;
     for (cf_instance* I : B->v) start.push_back(I->substep);
     for (int h = 0; h < 2; h++) {
-        int rc = record(B->v, 3, B->half[h]);
+        int rc = record(B->v, 3, B->half[h], B->shape);
         if (rc) {
             for (size_t m = 0; m < B->v.size(); m++) B->v[m]->substep = start[m];
             return rc;
@@ -1839,7 +2271,7 @@ unsigned long long cf_instance_bytes(const cf_config* c)
     unsigned long long b = 5 * fb + 8 * fb;                                     // u v w c p, f and g blocks
     b += (c->scheme == CF_SCHEME_CHANNEL ? 4 : 1) * splane * n2 * 16;          // spectra
     b += (c->order == 4 ? 3 : 1) * splane * n2 * 8;                            // band-solve scratch
-    const unsigned long long nwarps = (plane + SOLVE_THREADS - 1) / SOLVE_THREADS * (SOLVE_THREADS / 32);
+    const unsigned long long nwarps = (plane + SOLVE_THREADS_MAX - 1) / SOLVE_THREADS_MAX * (SOLVE_THREADS_MAX / 32);
     b += 2 * nwarps * n2 * 8 + 2 * n2 * 8 + 64 + 8;                            // row sums, averages, scalars
     b += 3ull * 4096 * LOG_COLS * 8;                                           // log ring
     b += (unsigned long long) (c->nx + c->ny) * 16;                            // twiddles

@@ -644,7 +644,8 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
     double* Rp = A.scratch + 2 * (long long) n2 * npair;
     extern __shared__ double2 pring[];
     const int t = threadIdx.x;
-    auto fslot = [&](int i, int c) { return pring + ((i % POIS_PF) * 2 + c) * POIS_THREADS + t; };
+    const int nt = blockDim.x;
+    auto fslot = [&](int i, int c) { return pring + ((i % POIS_PF) * 2 + c) * nt + t; };
     auto ffetch = [&](int i) {
         if (i < n) {
             cp_async16_ordered(fslot(i, 0), &SA(GZ + i));
@@ -756,13 +757,13 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 4) k_poisson(Geo G, PoissonArgs A)
+__global__ void __launch_bounds__(POIS_THREADS_MAX, 4) k_poisson(Geo G, PoissonArgs A)
 {
     band_column<ORDER, true>(G, A, blockIdx);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 4) k_poisson_batch(const BatchRec<PoissonArgs>* r, int n)
+__global__ void __launch_bounds__(POIS_THREADS_MAX, 4) k_poisson_batch(const BatchRec<PoissonArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<PoissonArgs>& R = batch_locate(r, n, b);
@@ -770,7 +771,7 @@ __global__ void __launch_bounds__(POIS_THREADS, 4) k_poisson_batch(const BatchRe
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(POIS_THREADS, 4) k_helmholtz_spectral(Geo G, PoissonArgs A)
+__global__ void __launch_bounds__(POIS_THREADS_MAX, 4) k_helmholtz_spectral(Geo G, PoissonArgs A)
 {
     band_column<ORDER, false>(G, A, blockIdx);
 }
@@ -816,13 +817,13 @@ __device__ __forceinline__ void k_project_body(const Geo& G, const ProjArgs& A, 
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_project(Geo G, ProjArgs A)
+__global__ void __launch_bounds__(PROJ_THREADS_MAX) k_project(Geo G, ProjArgs A)
 {
     k_project_body<ORDER>(G, A, blockIdx);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_project_batch(const BatchRec<ProjArgs>* r, int n)
+__global__ void __launch_bounds__(PROJ_THREADS_MAX) k_project_batch(const BatchRec<ProjArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<ProjArgs>& R = batch_locate(r, n, b);
@@ -1366,21 +1367,23 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st,
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
 {
     unsigned nb = grid_poisson(G).x;
-    if (G.order == 2) k_poisson<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
-    else k_poisson<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
+    const int nt = G.shape.pois_threads;
+    if (G.order == 2) k_poisson<2><<<nb, nt, 0, st>>>(G, A);
+    else k_poisson<4><<<nb, nt, pois_smem_bytes(nt), st>>>(G, A);
 }
 
 void launch_helmholtz_spectral(const Geo& G, const PoissonArgs& A, cudaStream_t st)
 {
     unsigned nb = grid_poisson(G).x;
-    if (G.order == 2) k_helmholtz_spectral<2><<<nb, POIS_THREADS, 0, st>>>(G, A);
-    else k_helmholtz_spectral<4><<<nb, POIS_THREADS, pois_smem_bytes(), st>>>(G, A);
+    const int nt = G.shape.pois_threads;
+    if (G.order == 2) k_helmholtz_spectral<2><<<nb, nt, 0, st>>>(G, A);
+    else k_helmholtz_spectral<4><<<nb, nt, pois_smem_bytes(nt), st>>>(G, A);
 }
 
 void launch_project(const Geo& G, const ProjArgs& A, cudaStream_t st)
 {
-    dim3 blk(32, 4, 1);
-    dim3 grd((G.ny + 31) / 32, (G.nx + 3) / 4, G.n2);
+    dim3 blk(G.shape.proj_bx, G.shape.proj_by, 1);
+    dim3 grd = grid_project(G);
     if (G.order == 2) k_project<2><<<grd, blk, 0, st>>>(G, A);
     else k_project<4><<<grd, blk, 0, st>>>(G, A);
 }
@@ -1422,10 +1425,15 @@ dim3 grid_c2r(const Geo& G, int nrows, int nfields)
 dim3 grid_poisson(const Geo& G)
 {
     const long long npair = (long long) G.nkx * (G.ny / 2 + 1);
-    return dim3((unsigned) ((npair + POIS_THREADS - 1) / POIS_THREADS));
+    const int nt = G.shape.pois_threads;
+    return dim3((unsigned) ((npair + nt - 1) / nt));
 }
 
-dim3 grid_project(const Geo& G) { return dim3((G.ny + 31) / 32, (G.nx + 3) / 4, G.n2); }
+dim3 grid_project(const Geo& G)
+{
+    const int bx = G.shape.proj_bx, by = G.shape.proj_by;
+    return dim3((G.ny + bx - 1) / bx, (G.nx + by - 1) / by, G.n2);
+}
 
 template <class Args>
 static const BatchRec<Args>* recs_of(const BatchLaunch& L) { return static_cast<const BatchRec<Args>*>(L.recs); }
@@ -1481,8 +1489,8 @@ void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st)
 
 void launch_poisson_batch(const BatchLaunch& L, int order, cudaStream_t st)
 {
-    if (order == 2) k_poisson_batch<2><<<L.blocks, POIS_THREADS, 0, st>>>(recs_of<PoissonArgs>(L), L.n);
-    else k_poisson_batch<4><<<L.blocks, POIS_THREADS, pois_smem_bytes(), st>>>(recs_of<PoissonArgs>(L), L.n);
+    if (order == 2) k_poisson_batch<2><<<L.blocks, L.block, 0, st>>>(recs_of<PoissonArgs>(L), L.n);
+    else k_poisson_batch<4><<<L.blocks, L.block, pois_smem_bytes(L.block.x), st>>>(recs_of<PoissonArgs>(L), L.n);
 }
 
 void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st)
@@ -1502,9 +1510,8 @@ void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st)
 
 void launch_project_batch(const BatchLaunch& L, int order, cudaStream_t st)
 {
-    dim3 blk(32, 4, 1);
-    if (order == 2) k_project_batch<2><<<L.blocks, blk, 0, st>>>(recs_of<ProjArgs>(L), L.n);
-    else k_project_batch<4><<<L.blocks, blk, 0, st>>>(recs_of<ProjArgs>(L), L.n);
+    if (order == 2) k_project_batch<2><<<L.blocks, L.block, 0, st>>>(recs_of<ProjArgs>(L), L.n);
+    else k_project_batch<4><<<L.blocks, L.block, 0, st>>>(recs_of<ProjArgs>(L), L.n);
 }
 
 bool batch_pow2(int n) { return pow2_kernel_size(n); }

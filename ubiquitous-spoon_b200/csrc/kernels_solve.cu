@@ -212,33 +212,39 @@ __device__ __forceinline__ void back4_body(const Geo& G, const SolveBatch& B, ui
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(SOLVE_THREADS) k_back4(Geo G, SolveBatch B)
+__global__ void __launch_bounds__(SOLVE_THREADS_MAX) k_back4(Geo G, SolveBatch B)
 {
     back4_body<ORDER>(G, B, blockIdx);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(SOLVE_THREADS) k_back4_batch(const BatchRec<SolveBatch>* r, int n)
+__global__ void __launch_bounds__(SOLVE_THREADS_MAX) k_back4_batch(const BatchRec<SolveBatch>* r, int n)
 {
     uint3 b;
     const BatchRec<SolveBatch>& R = batch_locate(r, n, b);
     back4_body<ORDER>(R.G, R.A, b);
 }
 
-dim3 grid_back4(const Geo& G) { return dim3((unsigned) ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS), 4); }
+dim3 grid_back4(const Geo& G)
+{
+    const int nt = G.shape.solve_threads;
+    return dim3((unsigned) ((G.plane + nt - 1) / nt), 4);
+}
 
 void launch_back4(const Geo& G, const SolveBatch& B, cudaStream_t st)
 {
     dim3 grd = grid_back4(G);
-    if (G.order == 2) k_back4<2><<<grd, SOLVE_THREADS, 0, st>>>(G, B);
-    else k_back4<4><<<grd, SOLVE_THREADS, 0, st>>>(G, B);
+    const int nt = G.shape.solve_threads;
+    if (G.order == 2) k_back4<2><<<grd, nt, 0, st>>>(G, B);
+    else k_back4<4><<<grd, nt, 0, st>>>(G, B);
 }
 
 RowAvgArgs row_average_args(const Geo& G, const double* partial, double* avg)
 {
     RowAvgArgs R;
     R.partial = partial;
-    R.nwarps = ((G.plane + SOLVE_THREADS - 1) / SOLVE_THREADS) * (SOLVE_THREADS / 32);
+    const int nt = G.shape.solve_threads;
+    R.nwarps = ((G.plane + nt - 1) / nt) * (nt / 32);
     R.n2 = G.n2;
     R.scale = 1.0 / ((double) G.nx * (double) G.ny);
     R.avg = avg;
@@ -259,8 +265,8 @@ void launch_mass_control(const MassArgs& M, cudaStream_t st)
 void launch_back4_batch(const BatchLaunch& L, int order, cudaStream_t st)
 {
     auto r = static_cast<const BatchRec<SolveBatch>*>(L.recs);
-    if (order == 2) k_back4_batch<2><<<L.blocks, SOLVE_THREADS, 0, st>>>(r, L.n);
-    else k_back4_batch<4><<<L.blocks, SOLVE_THREADS, 0, st>>>(r, L.n);
+    if (order == 2) k_back4_batch<2><<<L.blocks, L.block, 0, st>>>(r, L.n);
+    else k_back4_batch<4><<<L.blocks, L.block, 0, st>>>(r, L.n);
 }
 
 void launch_row_average_batch(const BatchLaunch& L, cudaStream_t st)
