@@ -88,9 +88,10 @@ __global__ void k_ghosts_batch(const BatchRec<GhostArgs>* r, int n)
 // --------------------------------------------------------------------- RHS
 //
 // One block owns an 8 (x) by 32 (y) column tile and marches up all interior
-// rows.  The 7 k-planes a row needs (k-3..k+3) of u, v, w, c, with a 3-cell
-// periodic halo in x and y, sit in a ring of 8 shared-memory slots; the next
-// plane streams in with cp.async while the current row is computed.  Every
+// rows.  The 7 k-planes a row needs (k-3..k+3) of u, v, w, c, with a
+// periodic halo of 3 rows in x and 4 columns in y, sit in a ring of 8
+// shared-memory slots; the next plane streams in with cp.async while the
+// current row is computed.  Every
 // stencil value is read from shared memory.  Divisions by the grid metrics
 // are multiplications by their reciprocals (host tables), so results agree
 // with the reference to rounding, not bit for bit.
@@ -117,15 +118,21 @@ constexpr int RT_THREADS = RT_I * RT_J;
 // (8 and 6 slots).  Order 2 thus needs 83 KB of ring instead of 136 KB.
 // One block per SM for both: capping order 2 at 128 registers for two blocks
 // per SM measured 5-9 % slower (less instruction-level parallelism).
+// The y halo is rounded up to an even width (XL) so that, for even ny, every
+// haloed row segment starts on a 16-byte boundary in global and shared
+// memory: planes stream in as 16-byte copies that bypass L1.
 template <int ORDER>
 struct RhsTile {
     static constexpr int H = ORDER == 2 ? 2 : 3;
     static constexpr int ZH = H;
+    static constexpr int XL = (H + 1) & ~1;                      // y halo columns: 4 / 2
     static constexpr int SLOTS = 2 * ZH + 2;
-    static constexpr int PI = RT_I + 2 * H, PJ = RT_J + 2 * H;   // 14 x 38 / 12 x 36
+    static constexpr int PI = RT_I + 2 * H, PJ = RT_J + 2 * XL;  // 14 x 40 / 12 x 36
     static constexpr int PLANE = PI * PJ;
     static constexpr int FIELD = SLOTS * PLANE;                  // one field's ring
-    static constexpr int LOADS = (PLANE + RT_THREADS - 1) / RT_THREADS;   // plane points per thread
+    static constexpr int LOADS = (PLANE + RT_THREADS - 1) / RT_THREADS;       // 8-byte copies per thread (odd ny)
+    static constexpr int PAIRS = PLANE / 2;
+    static constexpr int LOADS2 = (PAIRS + RT_THREADS - 1) / RT_THREADS;      // 16-byte copies per thread (even ny)
     static constexpr int BLOCKS = 1;                             // launch bound: blocks per SM
     // plane kk >= 0 (every plane a row reads lies in 0 .. n2-1): an unsigned
     // remainder, a single AND for the 8-slot ring
@@ -187,6 +194,11 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src)
     unsigned d = (unsigned) __cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
 }
+__device__ __forceinline__ void cp_async16(double* dst, const double* src)   // L2 only
+{
+    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -201,15 +213,21 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     const long long plane = (long long) nx * ny;
     const int kb = GZ, ke = GZ + G.nz;   // all interior rows: the forward sweeps run in order
 
-    // This thread's points of a haloed plane (same in every plane): their
-    // offsets within a field plane, computed once.
+    // This thread's points (even ny: pairs of points) of a haloed plane,
+    // the same in every plane: their offsets within a field plane, computed
+    // once.  For even ny a pair starts at an even y index (j0 and XL are
+    // even), so it never straddles the periodic wrap and its global and
+    // shared addresses are 16-byte aligned.
+    const bool pairs = (ny & 1) == 0;
     int goff[T::LOADS];
 #pragma unroll
     for (int m = 0; m < T::LOADS; m++) {
         const int r = tid + m * RT_THREADS;
-        const int ii = r / T::PJ, jj = r - ii * T::PJ;
+        int ii, jj;
+        if (pairs) { ii = r / (T::PJ / 2); jj = 2 * (r - ii * (T::PJ / 2)); }
+        else { ii = r / T::PJ; jj = r - ii * T::PJ; }
         int gi = (i0 + ii - T::H) % nx; if (gi < 0) gi += nx;
-        int gj = (j0 + jj - T::H) % ny; if (gj < 0) gj += ny;
+        int gj = (j0 + jj - T::XL) % ny; if (gj < 0) gj += ny;
         goff[m] = gi * ny + gj;
     }
     auto load_plane = [&](int kk) {
@@ -218,16 +236,30 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
         const double* bv = A.v + base;
         const double* bw = A.w + base;
         const double* bc = A.c + base;
-        double* d0 = sm + T::slot(kk) * T::PLANE + tid;
+        double* ps = sm + T::slot(kk) * T::PLANE;
+        if (pairs) {
 #pragma unroll
-        for (int m = 0; m < T::LOADS; m++) {
-            if (tid + m * RT_THREADS < T::PLANE) {
-                double* d = d0 + m * RT_THREADS;
-                const int o = goff[m];
-                cp_async8(d, bu + o);
-                cp_async8(d + T::FIELD, bv + o);
-                cp_async8(d + 2 * T::FIELD, bw + o);
-                cp_async8(d + 3 * T::FIELD, bc + o);
+            for (int m = 0; m < T::LOADS2; m++) {
+                if (tid + m * RT_THREADS < T::PAIRS) {
+                    double* d = ps + 2 * (tid + m * RT_THREADS);
+                    const int o = goff[m];
+                    cp_async16(d, bu + o);
+                    cp_async16(d + T::FIELD, bv + o);
+                    cp_async16(d + 2 * T::FIELD, bw + o);
+                    cp_async16(d + 3 * T::FIELD, bc + o);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < T::LOADS; m++) {
+                if (tid + m * RT_THREADS < T::PLANE) {
+                    double* d = ps + tid + m * RT_THREADS;
+                    const int o = goff[m];
+                    cp_async8(d, bu + o);
+                    cp_async8(d + T::FIELD, bv + o);
+                    cp_async8(d + 2 * T::FIELD, bw + o);
+                    cp_async8(d + 3 * T::FIELD, bc + o);
+                }
             }
         }
         cp_async_commit();
@@ -269,7 +301,7 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
 
     int k = kb;
     auto at = [&](int f, int di, int dj, int dk) -> double {
-        return sm[f * T::FIELD + T::slot(k + dk) * T::PLANE + (ty + T::H + di) * T::PJ + (tx + T::H + dj)];
+        return sm[f * T::FIELD + T::slot(k + dk) * T::PLANE + (ty + T::H + di) * T::PJ + (tx + T::XL + dj)];
     };
     auto U = [&](int di, int dj, int dk) { return at(0, di, dj, dk); };
     auto V = [&](int di, int dj, int dk) { return at(1, di, dj, dk); };
