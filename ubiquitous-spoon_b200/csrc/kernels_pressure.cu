@@ -938,11 +938,13 @@ __host__ __device__ constexpr int p2_stride_x(int n) { return p2_pad(n) + (p2_li
 // Divergence of the power-of-two path as its own streaming kernel
 // (divergence{2,4}, pressure.c:40-117).  A block owns an 8 (i) x 32 (j)
 // tile and climbs DV_KC planes.  Per plane, u with its x halo (rows i-2 ..
-// i+8) and v with its y halo (columns j-2 .. j+32) are staged in shared
-// memory by cp.async, double-buffered one plane ahead, so each value crosses
-// L2 once; w is carried up the column in a register window, and at the walls
-// that window supplies the extrapolated w of pressure.c:80-95.  The x
-// transform then reads the result as a real field.
+// i+8) and v with its y halo (columns j-2 .. j+33, an even width) are staged
+// in shared memory by cp.async, double-buffered one plane ahead, so each
+// value crosses L2 once; for even ny the copies are 16-byte pairs that
+// bypass L1.  w is carried up the column in a register window (the next
+// row loaded one plane ahead), and at the walls that window supplies the
+// extrapolated w of pressure.c:80-95.  The x transform then reads the
+// result as a real field.
 constexpr int DV_I = 8, DV_J = 32, DV_KC = 16;
 
 __device__ __forceinline__ void dv_cp8(double* dst, const double* src)
@@ -950,12 +952,17 @@ __device__ __forceinline__ void dv_cp8(double* dst, const double* src)
     unsigned d = (unsigned) __cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void dv_cp16(double* dst, const double* src)   // L2 only
+{
+    unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 
 template <int ORDER>
 __device__ __forceinline__ void k_div_body(const Geo& G, const DivArgs& A, uint3 bid)
 {
-    __shared__ double su[2][DV_I + 3][DV_J];   // u, rows i0-2 .. i0+8
-    __shared__ double sv[2][DV_I][DV_J + 3];   // v, columns j0-2 .. j0+32
+    __shared__ __align__(16) double su[2][DV_I + 3][DV_J];   // u, rows i0-2 .. i0+8
+    __shared__ __align__(16) double sv[2][DV_I][DV_J + 4];   // v, columns j0-2 .. j0+33
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DV_J + tx;
     const int j0 = bid.x * DV_J, i0 = bid.y * DV_I;
     const int nx = G.nx, ny = G.ny, n2 = G.n2;
@@ -964,28 +971,46 @@ __device__ __forceinline__ void k_div_body(const Geo& G, const DivArgs& A, uint3
     const int k1 = min(k0 + DV_KC, n2 - GZ);
     const int i = i0 + ty, j = j0 + tx;
     const bool valid = i < nx && j < ny;
-    // this thread's halo elements (at most two of u, two of v): their
-    // offsets within a plane, the same for every plane, computed once
-    constexpr int NU = (DV_I + 3) * DV_J, NV = DV_I * (DV_J + 3), NT = DV_I * DV_J;
+    // this thread's halo elements (even ny: one pair of u, one pair of v;
+    // odd ny: at most two of u, two of v): their offsets within a plane,
+    // the same for every plane, computed once.  For even ny a pair starts
+    // at an even y index (j0 is even, the v halo starts 2 before), so it
+    // never straddles the periodic wrap and its addresses are 16-byte aligned.
+    constexpr int NU = (DV_I + 3) * DV_J, NV = DV_I * (DV_J + 4), NT = DV_I * DV_J;
+    const bool pairs = (ny & 1) == 0;
     int uoff[2], voff[2];
 #pragma unroll
     for (int q = 0; q < 2; q++) {
         const int e = tid + q * NT;
-        const int r = e / DV_J, c = e - r * DV_J;
-        int ii = (i0 - 2 + r) % nx; if (ii < 0) ii += nx;
-        uoff[q] = e < NU ? ii * ny + min(j0 + c, ny - 1) : 0;
-        const int rv = e / (DV_J + 3), cv = e - rv * (DV_J + 3);
-        int jj = (j0 - 2 + cv) % ny; if (jj < 0) jj += ny;
-        voff[q] = e < NV ? min(i0 + rv, nx - 1) * ny + jj : 0;
+        if (pairs) {   // pair e of u (e < NU/2) and of v (e < NV/2)
+            const int r = e / (DV_J / 2), c = 2 * (e - r * (DV_J / 2));
+            int ii = (i0 - 2 + r) % nx; if (ii < 0) ii += nx;
+            uoff[q] = 2 * e < NU ? ii * ny + min(j0 + c, ny - 2) : 0;
+            const int rv = e / ((DV_J + 4) / 2), cv = 2 * (e - rv * ((DV_J + 4) / 2));
+            int jj = (j0 - 2 + cv) % ny; if (jj < 0) jj += ny;
+            voff[q] = 2 * e < NV ? min(i0 + rv, nx - 1) * ny + jj : 0;
+        } else {
+            const int r = e / DV_J, c = e - r * DV_J;
+            int ii = (i0 - 2 + r) % nx; if (ii < 0) ii += nx;
+            uoff[q] = e < NU ? ii * ny + min(j0 + c, ny - 1) : 0;
+            const int rv = e / (DV_J + 4), cv = e - rv * (DV_J + 4);
+            int jj = (j0 - 2 + cv) % ny; if (jj < 0) jj += ny;
+            voff[q] = e < NV ? min(i0 + rv, nx - 1) * ny + jj : 0;
+        }
     }
     auto load = [&](int kk, int buf) {
         const double* uk = A.u + kk * plane;
         const double* vk = A.v + kk * plane;
+        if (pairs) {
+            if (2 * tid < NU) dv_cp16(&su[buf][0][0] + 2 * tid, uk + uoff[0]);
+            if (2 * tid < NV) dv_cp16(&sv[buf][0][0] + 2 * tid, vk + voff[0]);
+        } else {
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
-            const int e = tid + q * NT;
-            if (e < NU) dv_cp8(&su[buf][0][0] + e, uk + uoff[q]);
-            if (e < NV) dv_cp8(&sv[buf][0][0] + e, vk + voff[q]);
+            for (int q = 0; q < 2; q++) {
+                const int e = tid + q * NT;
+                if (e < NU) dv_cp8(&su[buf][0][0] + e, uk + uoff[q]);
+                if (e < NV) dv_cp8(&sv[buf][0][0] + e, vk + voff[q]);
+            }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
@@ -999,11 +1024,13 @@ __device__ __forceinline__ void k_div_body(const Geo& G, const DivArgs& A, uint3
     double w0 = ORDER == 4 ? __ldg(wp + (k0 - 2) * plane) : 0.0;
     double w1 = __ldg(wp + (k0 - 1) * plane);
     double w2 = __ldg(wp + k0 * plane);
+    double w3n = __ldg(wp + (k0 + 1) * plane);   // row k+1, loaded one plane ahead
     for (int k = k0; k < k1; k++) {
         const int buf = (k - k0) & 1;
         if (k + 1 < k1) load(k + 1, buf ^ 1);
         else asm volatile("cp.async.commit_group;\n" ::: "memory");
-        const double w3 = __ldg(wp + (k + 1) * plane);   // row k+1 (a ghost row at the top: unused there)
+        const double w3 = w3n;   // row k+1 (a ghost row at the top: unused there)
+        if (k + 1 < k1) w3n = __ldg(wp + (k + 2) * plane);   // rows up to k1 <= n2 - GZ, as before
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
         const double uc = corr ? A.gu[k] * mu : 0.0;   // chanfast.c:516-519
@@ -1130,13 +1157,13 @@ __device__ __forceinline__ void k_ffty_p2_body(const Geo& G, const FftyArgs& A, 
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_ffty_p2(Geo G, FftyArgs A)
+__global__ void __launch_bounds__(256, 4) k_ffty_p2(Geo G, FftyArgs A)
 {
     k_ffty_p2_body<N>(G, A, blockIdx);
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_ffty_p2_batch(const BatchRec<FftyArgs>* r, int n)
+__global__ void __launch_bounds__(256, 4) k_ffty_p2_batch(const BatchRec<FftyArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<FftyArgs>& R = batch_locate(r, n, b);
