@@ -147,13 +147,26 @@ __global__ void k_row_average_batch(const BatchRec<RowAvgArgs>* r, int n)
     row_average_body(R.A, b);
 }
 
-// Bulk-mean control of chanfast.c:485-529 (u) / 572-616 (c).
+// Bulk-mean control of chanfast.c:485-529 (u) / 572-616 (c).  The warp
+// stages the profile and the cell heights in shared memory (rows up to
+// MASS_MAX_N2, else read in place); one thread then sums them in the
+// reference's order.
+constexpr int MASS_MAX_N2 = 2048;   // 32 KB of static shared memory
 __device__ __forceinline__ void mass_control_body(const MassArgs& A)
 {
-    if (threadIdx.x != 0) return;
-    const double* avg = A.avg;
-    const double* dz = A.dz;
+    __shared__ double s_avg[MASS_MAX_N2], s_dz[MASS_MAX_N2];
     const int g = GZ, n2 = A.n2, nz = A.nz;
+    const bool staged = n2 <= MASS_MAX_N2;
+    if (staged) {
+        for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+            s_avg[k] = A.avg[k];
+            s_dz[k] = A.dz[k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const double* avg = staged ? s_avg : A.avg;
+    const double* dz = staged ? s_dz : A.dz;
     double a = 0.0, l = 0.0;  // get_z_avg (get.c:490-502)
     for (int k = g; k < nz + g; k++) {
         a += avg[k] * dz[k];
