@@ -243,7 +243,7 @@ def run_ours(args):
     inst = cf.Instance(cfg, stream=ctypes_stream(stream))
     if args.launch_shape:
         inst.set_launch_shape(tuple(int(x) for x in args.launch_shape.split(",")))
-    shape = list(inst.launch_shape())
+    lshape = list(inst.launch_shape())
     inst.init_fields(w["seed"] + rank, w["amp"], w["c_amp"])
     inst.step_graph(args.warmup)
     inst.sync()
@@ -338,8 +338,8 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 ({pts * (w['nz'] + 6) // w['nz'] * 8 / 1e6:.0f} MB per field, "
                          "4 fields read per kernel vs 126 MB L2); no flush",
                    "parallelism": f"replicas x{world}" if world > 1 else "single instance",
-                   "launch_shape": {"solve_threads": shape[0], "poisson_threads": shape[1],
-                                    "project_block": shape[2:]}},
+                   "launch_shape": {"solve_threads": lshape[0], "poisson_threads": lshape[1],
+                                    "project_block": lshape[2:]}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "max_divergence": div,
     }
