@@ -121,3 +121,14 @@ def test_ensemble_and_serving_traces_are_deterministic():
     assert 3.6 < rate < 4.4                                     # Poisson arrivals at 4 per second
     assert all(200 <= r["nsteps"] <= 2000 and r["order"] in (2, 4) for r in t)
     assert all(2800.0 <= r["re"] <= 20000.0 for r in t)
+
+
+def test_tuning_calls_check_arguments(cf):
+    """Launch-shape calls: argument checks that return before any device work."""
+    import ctypes
+    L = cf.lib()
+    shape = (ctypes.c_int * 4)(128, 128, 32, 4)
+    assert L.cf_get_launch_shape(None, shape) == cf.CF_EINVAL
+    assert L.cf_set_launch_shape(None, shape) == cf.CF_EINVAL
+    assert L.cf_batch_get_launch_shape(None, shape) == cf.CF_EINVAL
+    assert L.cf_set_tuning(1) == cf.CF_OK
