@@ -316,10 +316,6 @@ __device__ __forceinline__ void rhs_body(const Geo& G, const RhsArgs& A, uint3 b
     // w mass fluxes (the u and v ones are formed per face below)
     auto mx_w = [&](int di, int dj, int dk) {
         return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di + 1, dj, dk)) + B2 * (dxdy * W(di - 1, dj, dk) + dxdy * W(di + 2, dj, dk)); };
-    auto my_u = [&](int di, int dj, int dk) { double d = DYDZ(dk);
-        return B1 * (d * U(di, dj, dk) + d * U(di, dj + 1, dk)) + B2 * (d * U(di, dj - 1, dk) + d * U(di, dj + 2, dk)); };
-    auto my_v = [&](int di, int dj, int dk) { double d = DXDZ(dk);
-        return B1 * (d * V(di, dj, dk) + d * V(di, dj + 1, dk)) + B2 * (d * V(di, dj - 1, dk) + d * V(di, dj + 2, dk)); };
     auto my_w = [&](int di, int dj, int dk) {
         return B1 * (dxdy * W(di, dj, dk) + dxdy * W(di, dj + 1, dk)) + B2 * (dxdy * W(di, dj - 1, dk) + dxdy * W(di, dj + 2, dk)); };
     auto mz_w = [&](int di, int dj, int dk) {
