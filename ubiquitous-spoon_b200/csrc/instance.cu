@@ -1299,14 +1299,25 @@ std::string config_key(const cf_instance* I)
          + std::to_string(C.ny) + "x" + std::to_string(C.nz);
 }
 
-// Key of a member set: its configurations with their counts, sorted.
+// Key of a member set: its configurations with their counts, sorted.  A
+// set of many distinct configurations is keyed by the 64-bit FNV-1a hash of
+// that list instead, so that every key fits one cache-file field.
 std::string batch_key(const std::vector<cf_instance*>& v)
 {
     std::map<std::string, int> n;
     for (const cf_instance* I : v) n[config_key(I)]++;
-    std::string k = device_tag(v[0]->device) + ":batch";
-    for (const auto& kv : n) k += ":" + kv.first + "*" + std::to_string(kv.second);
-    return k;
+    std::string list;
+    for (const auto& kv : n) list += ":" + kv.first + "*" + std::to_string(kv.second);
+    const std::string head = device_tag(v[0]->device) + ":batch";
+    if (list.size() <= 400) return head + list;
+    unsigned long long h = 1469598103934665603ull;
+    for (unsigned char ch : list) {
+        h ^= ch;
+        h *= 1099511628211ull;
+    }
+    char hex[24];
+    std::snprintf(hex, sizeof hex, "%016llx", h);
+    return head + ":h" + hex;
 }
 
 // Mean device time of `launch` over TUNE_REPS launches after one warm-up.
