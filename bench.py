@@ -70,8 +70,53 @@ METRIC = "FP64 Mpt-substeps/s"
 KERNEL_BYTES = {"rhs": 128.0, "solve": 64.0,
                 "div_fftx": 32.0, "ffty_fwd": 16.0, "poisson": 16.0, "ffty_bwd": 16.0,
                 "fftx_c2r": 16.0, "project": 72.0}
-# CPU-baseline sample: same order / nz / dt / viscosity, fewer x-y points per process
-CPU_SAMPLE = dict(nx=128, ny=128, substeps=2)
+# CPU-baseline sample: same order / nz / dt / viscosity, fewer x-y points per
+# process; REPEATS timed repeats of `substeps` substeps after one warm-up
+CPU_SAMPLE = dict(nx=128, ny=128, substeps=1, repeats=5)
+# the oracle's build of the reference sources (oracle/Makefile)
+REF_CFLAGS = "-O3 -funroll-loops -ffp-contract=off"
+
+
+def host_info():
+    """CPU model, physical and logical cores, compiler, and whether an MPI
+    compiler and FFTW 3 exist on this host (they decide how the reference
+    can be built here: with neither, the oracle's single-rank shims)."""
+    info = {"cpu_model": None, "physical_cores": None, "logical_cpus": os.cpu_count()}
+    try:
+        cores, model = set(), None
+        phys = core = None
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None:
+            cores.add((phys, core))
+        info["cpu_model"] = model
+        info["physical_cores"] = len(cores) or None
+    except OSError:
+        pass
+    import shutil
+
+    def first_line(cmd):
+        try:
+            r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=20)
+            return r.stdout.strip().splitlines()[0] if r.returncode == 0 and r.stdout.strip() else None
+        except (OSError, subprocess.SubprocessError):
+            return None
+    info["compiler"] = first_line([os.environ.get("CC", "gcc"), "--version"])
+    info["cflags"] = REF_CFLAGS
+    info["mpicc"] = first_line(["mpicc", "--version"]) if shutil.which("mpicc") else "not found"
+    info["fftw3"] = first_line(["pkg-config", "--modversion", "fftw3"]) or "not found (pkg-config)"
+    return info
 
 
 def measured_peaks():
@@ -137,8 +182,9 @@ class ClockSampler:
 # ------------------------------------------------------------ CPU reference
 
 def _ref_worker(args):
-    """One single-rank reference instance (oracle/_ref) on a sample grid."""
-    wname, nx, ny, nsub, warm, seed = args
+    """One single-rank reference instance (oracle/_ref) on a sample grid:
+    `warm` untimed substeps, then `reps` timed runs of `nsub` substeps."""
+    wname, nx, ny, nsub, warm, reps, seed = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import chanfast_np as cn
     import ic
@@ -155,16 +201,21 @@ def _ref_worker(args):
     scheme = w.get("scheme", "chanfast")
     if warm:
         R.substeps(warm, scheme)
-    t0 = time.perf_counter()
-    R.substeps(nsub, scheme)
-    dt = time.perf_counter() - t0
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        R.substeps(nsub, scheme)
+        times.append(time.perf_counter() - t0)
     R.close()
-    return dt
+    return times
 
 
-def cpu_reference(nsub, warm, nproc=None):
+def cpu_reference(nsub, warm, reps, nproc=None):
     """Aggregate reference throughput on `nproc` independent single-rank
-    processes (one per core) -- Mpt-substeps/s."""
+    processes (one per core), Mpt-substeps/s: the median over `reps` timed
+    repeats (each the sum over processes of that repeat's rate), with the
+    spread.  Returns (median, nproc, sample, per-repeat slowest time,
+    [min, max])."""
     if nproc is None:
         ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
         try:
@@ -176,14 +227,15 @@ def cpu_reference(nsub, warm, nproc=None):
     ctx = mp.get_context("spawn")
     with ctx.Pool(nproc) as pool:
         wname = next(k for k, v in WORKLOADS.items() if v is WORKLOAD)
-        times = pool.map(_ref_worker, [(wname, nx, ny, nsub, warm, 100 + r) for r in range(nproc)])
+        times = pool.map(_ref_worker, [(wname, nx, ny, nsub, warm, reps, 100 + r) for r in range(nproc)])
     pts = nx * ny * WORKLOAD["nz"]
-    value = sum(pts * nsub / t for t in times) / 1e6
+    per_rep = [sum(pts * nsub / t[r] for t in times) / 1e6 for r in range(reps)]
+    slowest = statistics.median(max(t[r] for t in times) for r in range(reps))
     sample = (f"unmodified reference {WORKLOAD.get('scheme', 'chanfast')}{WORKLOAD['order']} substep "
               f"(oracle/_ref, single-rank MPI/FFTW shims, "
-              f"gcc -O3 -funroll-loops) on {nproc} independent {nx}x{ny}x{WORKLOAD['nz']} instances, "
-              f"{nsub} timed substeps each after {warm} warm-up")
-    return value, nproc, sample, max(times)
+              f"gcc {REF_CFLAGS}) on {nproc} independent {nx}x{ny}x{WORKLOAD['nz']} instances, one per core; "
+              f"median of {reps} timed repeats of {nsub} substep(s) each after {warm} warm-up")
+    return statistics.median(per_rep), nproc, sample, slowest, [min(per_rep), max(per_rep)]
 
 
 def ensure_reference():
@@ -322,8 +374,9 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and ensure_reference():
-        v, nproc, sample, _ = cpu_reference(CPU_SAMPLE["substeps"], 1)
-        cpu = {"value": round(v, 3), "unit": METRIC, "cores": nproc, "kind": "reference", "sample": sample}
+        v, nproc, sample, _, spread = cpu_reference(CPU_SAMPLE["substeps"], 1, CPU_SAMPLE["repeats"])
+        cpu = {"value": round(v, 3), "unit": METRIC, "cores": nproc, "kind": "reference", "sample": sample,
+               "spread": [round(x, 3) for x in spread], "host": host_info()}
 
     div = inst.max_divergence()
     launches = inst.launches_per_substep() * substeps
@@ -523,9 +576,10 @@ def run_reference(args):
     if not ensure_reference():
         print(json.dumps({"impl": "reference", "unavailable": "reference sources absent and oracle/_ref not built"}))
         return
-    v, nproc, sample, tmax = cpu_reference(args.steps, args.warmup)
+    # a step: one substep on every process; the median over the K steps
+    v, nproc, sample, tstep, spread = cpu_reference(1, args.warmup, args.steps)
     nx, ny = CPU_SAMPLE["nx"], CPU_SAMPLE["ny"]
-    ms_per_step = tmax / args.steps * 1e3
+    ms_per_step = tstep * 1e3
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": METRIC, "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1),
@@ -534,7 +588,7 @@ def run_reference(args):
                    "nz": WORKLOAD["nz"], "step": f"one substep on each of {nproc} {nx}x{ny}x{WORKLOAD['nz']} "
                    "sample instances in parallel"},
         "cpu_baseline": {"value": round(v, 3), "unit": METRIC, "cores": nproc, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample, "spread": [round(x, 3) for x in spread], "host": host_info()},
         "e2e": {"value": round(v, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 

@@ -35,7 +35,7 @@ enum {
     CF_ENOMEM = -2,      /* device or host allocation failed */
     CF_ECUDA = -3,       /* a CUDA runtime call failed */
     CF_EPIVOT = -4,      /* zero pivot in a band factorisation */
-    CF_ENONFINITE = -5,  /* a field contains NaN or Inf */
+    CF_ENONFINITE = -5,  /* the state went NaN or Inf (see cf_sync) */
     CF_EIO = -6          /* restart / log file error (drivers) */
 };
 
@@ -103,14 +103,21 @@ int cf_step(cf_instance *inst, int nsub);
  * any substeps needed to reach the start of a time step run as cf_step. */
 int cf_step_graph(cf_instance *inst, int nsteps);
 
-/* Wait for all work of the instance. */
+/* Wait for all work of the instance.  Returns CF_ENONFINITE once a substep
+ * has found the bulk mean of u or c (a sum over every interior point) NaN or
+ * Inf: a blown-up or NaN-seeded state is detected within one substep, and
+ * within two for v, w and p, which feed u in the next substep.  The
+ * reference has no such check (its check(), check.h:8-12, aborts only on
+ * allocation, order and pivot failures).  The flag stays set until
+ * cf_set_field or cf_init_fields loads new fields. */
 int cf_sync(cf_instance *inst);
 
 /* Per-substep log rows (10 doubles each): mdpdx, nu du/dz bottom, top, bulk
  * velocity, centreline velocity, then dcdt and the same four scalar
  * statistics -- the values chanfast appends to pstat.dat / cstat.dat
  * (chanfast.c:525-528, 612-615).  Returns the number of rows written into
- * `out` (at most max_rows, most recent last) or a negative status. */
+ * `out` (at most max_rows, most recent last) or a negative status
+ * (CF_ENONFINITE as for cf_sync). */
 long cf_get_log(cf_instance *inst, double *out, long max_rows);
 
 /* Number of substeps done so far. */
@@ -248,7 +255,9 @@ int cf_batch_get_launch_shape(const cf_batch *batch, int shape[4]);
  * cf_batch_step (new arrivals join at the next round); a solve that has run
  * its steps is retired at once: on_done(index, inst, user) may read its
  * fields, then its memory is released (inst is NULL for a request that
- * failed; its status says why).  Requests use CF_SCHEME_CHANFAST.  Each
+ * failed; its status says why).  A solve whose state goes NaN or Inf
+ * (cf_sync) is retired at the end of that round with status CF_ENONFINITE
+ * while the others run on.  Requests use CF_SCHEME_CHANFAST.  Each
  * solve's result is the same, bit for bit, as stepping it alone with
  * cf_batch_step.  Times in results are seconds after the call.
  * ------------------------------------------------------------------------ */
@@ -277,8 +286,16 @@ int cf_serve(const cf_request *reqs, int n, double hbm_budget_bytes, int max_act
  * reference (chanfast.h:1-21, called at main.c:56-60); they read
  * outputdir/{u,v,w,c}_it<it>.dat, run nt - it time steps on the current
  * CUDA device, append outputdir/cfl.dat, pstat.dat and cstat.dat, and write
- * outputdir/{u,v,w,c}_it<N>.dat every istat steps.  p_row * p_col must be
- * 1.  The reference returns nothing and aborts on error; these print the
+ * outputdir/{u,v,w,c}_it<N>.dat every istat steps.  One GPU holds the whole
+ * grid: a single process accepts any p_row x p_col (main.c passes 2 x 2,
+ * main.c:9-10) with a note on stderr; under an MPI launcher with N > 1
+ * ranks (read from the launcher's environment: Open MPI, MPICH / Hydra,
+ * PMIx, Slurm), p_row * p_col must be N as in the reference
+ * (chanfast.c:87), rank 0 runs the whole grid and writes every file, and
+ * the other ranks return at once.  The reference main.c therefore builds
+ * and runs unchanged against this library.  A NaN / Inf state stops the run
+ * with CF_ENONFINITE (see cf_sync).
+ * The reference returns nothing and aborts on error; these print the
  * failing status to stderr and return.  chanfast2_status / chanfast4_status
  * return it instead.  channel2 / channel4 (channel.h:1-21) are the same with
  * the fully implicit scheme (CF_SCHEME_CHANNEL and its size limits).

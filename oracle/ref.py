@@ -16,7 +16,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libchanref.so")
-REFERENCE_SRC = os.environ.get("CHANFAST_REFERENCE_SRC", "/root/reference")
+# the reference sources: CHANFAST_REFERENCE_SRC, else a checkout named
+# `reference` beside this repository
+REFERENCE_SRC = os.environ.get("CHANFAST_REFERENCE_SRC") or os.path.abspath(
+    os.path.join(HERE, "..", "..", "reference"))
 
 _lock = threading.Lock()
 _lib = None
@@ -70,8 +73,16 @@ def lib():
                                        + [ctypes.c_int] + [ctypes.c_double] * 4 + [ctypes.c_int]
                                        + [ctypes.c_double, ctypes.c_int] + [ctypes.c_double] * 5)
             L.ref_channel.argtypes = L.ref_chanfast.argtypes
+            L.shim_set_exact_dft.argtypes = [ctypes.c_int]
             _lib = L
         return _lib
+
+
+def set_exact_dft(on: bool):
+    """Switch the oracle's FFTW stand-in between its recursive mixed-radix
+    FFT (default) and a direct DFT summed in long double (see
+    oracle/shim/fftw_shim.c); applies to every later transform."""
+    lib().shim_set_exact_dft(1 if on else 0)
 
 
 def _dp(a):

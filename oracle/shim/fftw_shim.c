@@ -3,6 +3,12 @@
  * See fftw3.h for scope.  Transforms are computed by a recursive mixed-radix
  * decimation-in-time DFT (any length; radices are the prime factors of n)
  * with twiddles exp(-2 pi i j / n) taken from a per-length cos/sin table.
+ *
+ * shim_set_exact_dft(1) switches every later fftw_execute to a direct DFT
+ * summed in long double (x87 80-bit, 64-bit mantissa) and rounded to double
+ * once: a second, differently rounded and more accurate DFT, used to measure
+ * how much the reference's results depend on which correct FFT it links
+ * (FFTW's own output bits are unpinned).
  */
 #include "fftw3.h"
 
@@ -77,6 +83,38 @@ static void dft_rec(const cplx *x, size_t stride, int n, int N, int sign,
         }
     }
     free(sub);
+}
+
+static int exact_dft = 0;
+void shim_set_exact_dft(int on) { exact_dft = on; }
+
+/* out[k] = sum_t x[t] exp(sign 2 pi i t k / n), summed in long double. */
+static void dft_exact(const cplx *x, int n, int sign, cplx *out)
+{
+    long double *c = (long double *) malloc(sizeof(long double) * 2 * (size_t) n);
+    long double *s = c + n;
+    for (int j = 0; j < n; j++) {
+        long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double) j / (long double) n;
+        c[j] = cosl(a);
+        s[j] = (long double) sign * sinl(a);
+    }
+    for (int k = 0; k < n; k++) {
+        long double sr = 0.0L, si = 0.0L;
+        for (int t = 0; t < n; t++) {
+            const int j = (int) (((long) t * k) % n);
+            sr += c[j] * (long double) x[t].re - s[j] * (long double) x[t].im;
+            si += c[j] * (long double) x[t].im + s[j] * (long double) x[t].re;
+        }
+        out[k].re = (double) sr;
+        out[k].im = (double) si;
+    }
+    free(c);
+}
+
+static void dft(const cplx *x, int n, int sign, const cplx *tw, cplx *out)
+{
+    if (exact_dft) dft_exact(x, n, sign, out);
+    else dft_rec(x, 1, n, n, sign, tw, out);
 }
 
 void shim_fft_c2c(int n, int sign, const fftw_complex *in, fftw_complex *out)
@@ -156,7 +194,7 @@ static void run_one(const struct shim_fftw_plan *p, size_t ioff, size_t ooff, cp
     if (p->kind == K_R2C) {
         const double *in = (const double *) p->in + ioff;
         for (int j = 0; j < n; j++) { x[j].re = in[(size_t) j * p->is]; x[j].im = 0.0; }
-        dft_rec(x, 1, n, n, -1, p->tw, y);
+        dft(x, n, -1, p->tw, y);
         cplx *out = (cplx *) p->out + ooff;
         for (int k = 0; k <= n / 2; k++) out[(size_t) k * p->os] = y[k];
     } else if (p->kind == K_C2R) {
@@ -165,13 +203,13 @@ static void run_one(const struct shim_fftw_plan *p, size_t ioff, size_t ooff, cp
         x[0].im = 0.0;
         if (n % 2 == 0) x[n / 2].im = 0.0;
         for (int k = n / 2 + 1; k < n; k++) { x[k].re = x[n - k].re; x[k].im = -x[n - k].im; }
-        dft_rec(x, 1, n, n, +1, p->tw, y);
+        dft(x, n, +1, p->tw, y);
         double *out = (double *) p->out + ooff;
         for (int j = 0; j < n; j++) out[(size_t) j * p->os] = y[j].re;
     } else {
         const cplx *in = (const cplx *) p->in + ioff;
         for (int j = 0; j < n; j++) x[j] = in[(size_t) j * p->is];
-        dft_rec(x, 1, n, n, p->sign, p->tw, y);
+        dft(x, n, p->sign, p->tw, y);
         cplx *out = (cplx *) p->out + ooff;
         for (int k = 0; k < n; k++) out[(size_t) k * p->os] = y[k];
     }

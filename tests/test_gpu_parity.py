@@ -221,22 +221,3 @@ def test_config0_100_steps(cf, ref, gpu):
         assert inst.max_divergence() <= 1e-12
         assert logs_close(inst.log(), R.log())
     R.close()
-
-
-@pytest.mark.slow
-def test_config1_size_substeps(cf, ref, gpu):
-    """Full config-1 grid (256 x 256 x 192, order 4, Re_b 1e4, dt 5e-4, scalar
-    Pr 0.71): three substeps against the reference."""
-    prm = cn.Params(order=4, nx=256, ny=256, nz=192, lx=2 * np.pi, ly=np.pi, lz=2.0, dt=5e-4,
-                    nu=1e-4, prandtl=0.71)
-    R, F = projected_state(ref, prm, 1, 0.1, 0.01)
-    with cf.Instance(cf.Config.from_params(prm)) as inst:
-        for nm in "uvwc":
-            inst.set_field(nm, F[nm])
-        inst.step(3)
-        R.substeps(3)
-        for nm in "uvwc":
-            assert rel(interior(inst.get_field(nm), prm), interior(R.get(nm), prm)) < 1e-13, nm
-        assert rel(interior(inst.get_field("p"), prm), interior(R.get("p"), prm)) < 1e-10
-        assert inst.max_divergence() < 1e-12
-    R.close()

@@ -1,0 +1,121 @@
+"""GPU parity on production grids and over 100 RK3 steps of the benchmarked
+scheme (order 4 with the scalar), against the compiled reference
+(oracle/_ref) on the same reference-projected initial state.
+
+The reference runs take minutes on one core, so they run in child processes
+started at collection time (tests/ref_jobs.py); this file is collected late
+so that they overlap the rest of the suite.
+
+Bars (relative L2 over the interior):
+* after 100 RK3 steps: <= 1e-10 on u, v, w, c, p -- the end-to-end parity
+  bar;
+* after 3 and 30 substeps: <= 1e-13 on u, v, w, c and <= 1e-10 on p, the
+  bars of the small-grid cases.
+Max discrete divergence: <= 1e-12, or twice the reference's own divergence
+of its own state at the same point (its divergence{2,4} over the interior)
+where the reference does not reach 1e-12 itself: on the 512 x 512 x 384 grid
+it leaves 6.8e-12 after one substep (the projection's residual on the
+stretched fourth-order grid, whose first cell is 3.3e-5 high).
+"""
+import numpy as np
+import pytest
+
+import ref_jobs
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def interior(a, p):
+    return a[p.ngx:p.ngx + p.nx, p.ngy:p.ngy + p.ny, p.ngz:p.ngz + p.nz]
+
+
+def log_mismatch(a, b):
+    """Worst |a - b| / (1e-9 x column scale) over the per-substep log rows
+    (the bar of test_gpu_parity.logs_close), with its row and column."""
+    assert a.shape == b.shape, (a.shape, b.shape)
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-3)
+    r = np.abs(a - b) / (1e-9 * scale)
+    i, j = np.unravel_index(np.argmax(r), r.shape)
+    return float(r[i, j]), (int(i), int(j), float(a[i, j]), float(b[i, j]))
+
+
+def check_divergence(inst, refjobs, name, n):
+    ours = inst.max_divergence()
+    theirs = float(refjobs.wait(name, f"s{n}_div")[0])
+    print(name, n, "max div", ours, "reference", theirs)
+    assert ours <= max(1e-12, 2.0 * theirs), (ours, theirs)
+
+
+def load_initial(cf, refjobs, name, prm):
+    inst = cf.Instance(cf.Config.from_params(prm))
+    for nm in "uvwc":
+        inst.set_field(nm, refjobs.wait(name, "init_" + nm))
+    return inst
+
+
+def compare(inst, refjobs, name, prm, n):
+    out = {}
+    for nm in "uvwcp":
+        b = interior(refjobs.wait(name, f"s{n}_{nm}"), prm)
+        out[nm] = rel(interior(inst.get_field(nm), prm), b)
+        del b
+    return out
+
+
+@pytest.mark.refjob("o4_64x64x48_100steps")
+def test_order4_scalar_100_steps(cf, refjobs, gpu):
+    """chanfast4 with the scalar (Pr 0.71), Re_b 1e4, dt 5e-4 on 64 x 64 x 48:
+    100 RK3 steps through the CUDA-graph path."""
+    name = "o4_64x64x48_100steps"
+    prm = ref_jobs.params(name)
+    with load_initial(cf, refjobs, name, prm) as inst:
+        inst.step_graph(100)
+        err = compare(inst, refjobs, name, prm, 300)
+        print(name, 300, {k: "%.2e" % v for k, v in err.items()})
+        assert all(err[nm] <= 1e-10 for nm in "uvwcp"), err
+        check_divergence(inst, refjobs, name, 300)
+        worst, where = log_mismatch(inst.log(), refjobs.wait(name, "s300_log"))
+        assert worst <= 1.0, where
+
+
+@pytest.mark.refjob("cfg1_256x256x192")
+def test_config1_grid_30_substeps(cf, refjobs, gpu):
+    """The 256 x 256 x 192 grid (order 4, Re_b 1e4, dt 5e-4, scalar), 3 and
+    30 substeps."""
+    name = "cfg1_256x256x192"
+    prm = ref_jobs.params(name)
+    with load_initial(cf, refjobs, name, prm) as inst:
+        done = 0
+        for n in (3, 30):
+            inst.step(n - done)
+            done = n
+            err = compare(inst, refjobs, name, prm, n)
+            print(name, n, {k: "%.2e" % v for k, v in err.items()})
+            assert all(err[nm] <= 1e-13 for nm in "uvwc"), (n, err)
+            assert err["p"] <= 1e-10, (n, err)
+            worst, where = log_mismatch(inst.log(), refjobs.wait(name, f"s{n}_log"))
+            print(name, n, "log", worst, where)
+            assert worst <= 1.0, where
+            check_divergence(inst, refjobs, name, n)
+
+
+@pytest.mark.refjob("cfg2_512x512x384")
+def test_config2_grid_substep(cf, refjobs, gpu):
+    """The benchmarked grid, 512 x 512 x 384 (order 4, Re_b 2e4, dt 2.5e-4,
+    perturbation 0.05, scalar): one substep."""
+    name = "cfg2_512x512x384"
+    prm = ref_jobs.params(name)
+    with load_initial(cf, refjobs, name, prm) as inst:
+        inst.step(1)
+        err = compare(inst, refjobs, name, prm, 1)
+        print(name, 1, {k: "%.2e" % v for k, v in err.items()})
+        assert all(err[nm] <= 1e-13 for nm in "uvwc"), err
+        assert err["p"] <= 1e-10, err
+        worst, where = log_mismatch(inst.log(), refjobs.wait(name, "s1_log"))
+        print(name, 1, "log", worst, where)
+        assert worst <= 1.0, where
+        check_divergence(inst, refjobs, name, 1)

@@ -4,8 +4,19 @@
  *
  * Same arguments and file protocol as the reference drivers (chanfast.h:1-21,
  * chanfast.c:71-992 / 995-1916; channel.h:1-21, channel.c:71-1018 /
- * 1021-1968, the same loop with the fully implicit substep) at
- * p_row = p_col = 1:
+ * 1021-1968, the same loop with the fully implicit substep).  One GPU holds
+ * the whole grid, so the pencil decomposition p_row x p_col has nothing to
+ * split:
+ *   - a single process (no MPI launcher, or one rank) runs whatever p_row x
+ *     p_col it is given, with a one-line note on stderr when that is not
+ *     1 x 1 -- the reference's main.c passes 2 x 2 (main.c:9-10);
+ *   - under an MPI launcher with N > 1 ranks, p_row x p_col must equal N as
+ *     in the reference (chanfast.c:87; CF_EINVAL otherwise); rank 0 then
+ *     runs the whole grid on its GPU and writes every file, and the other
+ *     ranks return at once without touching a GPU or a file.  The rank and
+ *     size come from the launcher's environment (Open MPI, MPICH / Hydra,
+ *     PMIx, Slurm), so the library needs no MPI itself.
+ * The run itself:
  *   - read outputdir/{u,v,w,c}_it<it>.dat (raw FP64, C order [nx][ny][nz],
  *     io.c:259-297)
  *   - for it in [it, nt): CFL of the current field (get.c:390-416), adapt dt
@@ -127,6 +138,24 @@ static int append_ascii(const double *u, int n, const char *filename)
     return fclose(fp) == 0 ? CF_OK : CF_EIO;
 }
 
+/* World size and rank of this process as its MPI launcher exported them;
+ * 1 and 0 when no launcher did. */
+static void launcher_rank(int *size, int *rank)
+{
+    static const char *const sizes[] = {"OMPI_COMM_WORLD_SIZE", "PMI_SIZE", "PMIX_SIZE", "SLURM_NTASKS"};
+    static const char *const ranks[] = {"OMPI_COMM_WORLD_RANK", "PMI_RANK", "PMIX_RANK", "SLURM_PROCID"};
+    *size = 1;
+    *rank = 0;
+    for (int q = 0; q < 4; q++) {
+        const char *s = getenv(sizes[q]), *r = getenv(ranks[q]);
+        if (s && r && atoi(s) > 0) {
+            *size = atoi(s);
+            *rank = atoi(r);
+            return;
+        }
+    }
+}
+
 static int run(int order, int scheme, int p_row, int p_col, int nx, int ny, int nz, int it, int nt, int istat,
                int nghost_x, int nghost_y, int nghost_z, double lx, double ly, double lz,
                double dt, double want_cfl, int cflmode, double nu, double prandtl,
@@ -134,7 +163,16 @@ static int run(int order, int scheme, int p_row, int p_col, int nx, int ny, int 
                double want_cvolavg, int cvolavgmode, double setuframe, double setvframe,
                double betg_x, double betg_y, double betg_z)
 {
-    if (p_row * p_col != 1 || istat <= 0) return CF_EINVAL;
+    if (p_row < 1 || p_col < 1 || istat <= 0) return CF_EINVAL;
+    int nproc, rank;
+    launcher_rank(&nproc, &rank);
+    if (nproc > 1) {
+        if (p_row * p_col != nproc) return CF_EINVAL;
+        if (rank != 0) return CF_OK;
+    } else if (p_row * p_col != 1) {
+        fprintf(stderr, "%s%d: p_row x p_col = %d x %d: one GPU holds the whole %d x %d x %d grid\n",
+                scheme == CF_SCHEME_CHANNEL ? "channel" : "chanfast", order, p_row, p_col, nx, ny, nz);
+    }
     cf_config cfg;
     memset(&cfg, 0, sizeof cfg);
     cfg.order = order;

@@ -130,6 +130,7 @@ struct MassArgs {
     int log_cap;
     int col;              // first column written: m, bottom gradient, top gradient, bulk, centreline
     int advance;          // 1: increment the counter afterwards (last statistics of a substep)
+    double* nonfinite;    // device flag: set to 1 when the bulk mean or the control is NaN / Inf
 };
 
 struct RowAvgArgs {

@@ -425,7 +425,7 @@ struct cf_instance {
     double* partial_c = nullptr;   // and of the c solve
     double* avg = nullptr;
     double* avg_c = nullptr;        // channel scheme: xy-average of c (avg holds u's)
-    double* dscal = nullptr;        // [0] mdpdx, [1] dcdt
+    double* dscal = nullptr;        // [0] mdpdx, [1] dcdt, [2] non-finite flag
     long long* dcount = nullptr;    // device substep counter (log row)
     double* dlog = nullptr;
     int log_cap = 0;
@@ -731,6 +731,7 @@ MassArgs mass_args(cf_instance* I, int s, int q, const double* avg)
     M.log_cap = I->log_cap;
     M.col = q == 0 ? 0 : 5;
     M.advance = q == 2 ? 1 : 0;
+    M.nonfinite = I->dscal + 2;
     return M;
 }
 
@@ -1746,6 +1747,7 @@ int cf_set_field(cf_instance* I, int field, const double* host, int layout)
     dim3 blk(32, 8), grd((K + 31) / 32, (I->geo.ny + 31) / 32, I->geo.nx);
     k_host2dev<<<grd, blk, 0, I->stream>>>(I->geo, I->staging, field_ptr(I, field), B, K, ox, oy, oz);
     CF_CUDA(cudaGetLastError());
+    CF_CUDA(cudaMemsetAsync(I->dscal + 2, 0, sizeof(double), I->stream));
     CF_CUDA(cudaStreamSynchronize(I->stream));
     return CF_OK;
 }
@@ -1773,6 +1775,7 @@ int cf_init_fields(cf_instance* I, unsigned long long seed, double amp, double c
     dim3 blk(128), grd((G.ny + 127) / 128, G.nx, G.n2);
     k_init_raw<<<grd, blk, 0, I->stream>>>(G, I->u, I->v, I->w, I->c, I->zp, seed, amp, c_amp);
     CF_CUDA(cudaGetLastError());
+    CF_CUDA(cudaMemsetAsync(I->dscal + 2, 0, sizeof(double), I->stream));
     pressure_sequence(I, I->pois_init, 1.0, 0, false);
     CF_CUDA(cudaGetLastError());
     CF_CUDA(cudaStreamSynchronize(I->stream));
@@ -1817,11 +1820,21 @@ int cf_step_graph(cf_instance* I, int nsteps)
     return CF_OK;
 }
 
+// CF_ENONFINITE once a mass-control kernel has found a NaN / Inf bulk mean
+// of u or c (the caller has synchronised the instance's stream).  The flag
+// is cleared when fields are set again.
+static int finite_status(cf_instance* I)
+{
+    double flag = 0.0;
+    CF_CUDA(cudaMemcpy(&flag, I->dscal + 2, sizeof(double), cudaMemcpyDeviceToHost));
+    return flag != 0.0 ? CF_ENONFINITE : CF_OK;
+}
+
 int cf_sync(cf_instance* I)
 {
     if (!I) return CF_EINVAL;
     CF_CUDA(cudaStreamSynchronize(I->stream));
-    return CF_OK;
+    return finite_status(I);
 }
 
 long cf_substeps_done(const cf_instance* I) { return I ? I->substep : CF_EINVAL; }
@@ -1830,6 +1843,7 @@ long cf_get_log(cf_instance* I, double* out, long max_rows)
 {
     if (!I || max_rows < 0) return CF_EINVAL;
     CF_CUDA(cudaStreamSynchronize(I->stream));
+    if (int rc = finite_status(I)) return rc;
     long long count = 0;
     CF_CUDA(cudaMemcpy(&count, I->dcount, sizeof(count), cudaMemcpyDeviceToHost));
     long long avail = count < I->log_cap ? count : I->log_cap;

@@ -184,6 +184,10 @@ __device__ __forceinline__ void mass_control_body(const MassArgs& A)
     }
     s[3] = nz % 2 == 0 ? 0.5 * (avg[g + nz / 2 - 1] + avg[g + nz / 2]) : avg[g + nz / 2];
     double m = A.mode == 1 ? (A.target - s[0]) / A.green[0] : A.fixed;
+    // The bulk mean sums every interior point of the field, so a NaN or Inf
+    // anywhere in it (or in the control) shows here; the flag stays set
+    // until the host resets it with new fields.
+    if (A.nonfinite && !isfinite(s[0] + m)) *A.nonfinite = 1.0;
     for (int t = 0; t < 4; t++) s[t] += A.green[t] * m;
     *A.m_out = m;
     if (A.log_base) {

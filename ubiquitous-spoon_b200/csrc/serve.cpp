@@ -139,7 +139,13 @@ extern "C" int cf_serve(const cf_request* reqs, int n, double hbm_budget_bytes, 
             break;
         }
         for (size_t a = 0; a < active.size();) {
-            if (active[a].remaining <= 0) retire(a, CF_OK);
+            // a solve whose state went NaN / Inf retires at once with that status
+            const int s = cf_sync(active[a].inst);
+            if (s == CF_ENONFINITE) retire(a, CF_ENONFINITE);
+            else if (s != CF_OK) {
+                rc = s;
+                break;
+            } else if (active[a].remaining <= 0) retire(a, CF_OK);
             else a++;
         }
     }
