@@ -77,6 +77,12 @@ CPU_SAMPLE = dict(nx=128, ny=128, substeps=1, repeats=5)
 REF_CFLAGS = "-O3 -funroll-loops -ffp-contract=off"
 
 
+def cpu_sample_grid():
+    """x-y size of one CPU-sample instance: the workload's own grid when it
+    is no larger than the sample, else the sample (same nz)."""
+    return min(WORKLOAD["nx"], CPU_SAMPLE["nx"]), min(WORKLOAD["ny"], CPU_SAMPLE["ny"])
+
+
 def host_info():
     """CPU model, physical and logical cores, compiler, and whether an MPI
     compiler and FFTW 3 exist on this host (they decide how the reference
@@ -223,7 +229,7 @@ def cpu_reference(nsub, warm, reps, nproc=None):
         except (ValueError, OSError):
             mem_gb = 16.0
         nproc = max(1, min(ncpu, int(mem_gb // 3), 64))
-    nx, ny = CPU_SAMPLE["nx"], CPU_SAMPLE["ny"]
+    nx, ny = cpu_sample_grid()
     ctx = mp.get_context("spawn")
     with ctx.Pool(nproc) as pool:
         wname = next(k for k, v in WORKLOADS.items() if v is WORKLOAD)
@@ -578,7 +584,7 @@ def run_reference(args):
         return
     # a step: one substep on every process; the median over the K steps
     v, nproc, sample, tstep, spread = cpu_reference(1, args.warmup, args.steps)
-    nx, ny = CPU_SAMPLE["nx"], CPU_SAMPLE["ny"]
+    nx, ny = cpu_sample_grid()
     ms_per_step = tstep * 1e3
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": METRIC, "n_gpus": 0,

@@ -104,13 +104,16 @@ def test_channel_drop_in_driver_matches_reference_driver(cf, ref, gpu, tmp_path,
 @pytest.mark.parametrize("order", [2, 4])
 def test_channel_100_steps(cf, ref, gpu, order):
     """100 RK3 steps of channel2 / channel4 at 64 x 64 x 32 (Re_b 2800,
-    dt 1e-3): u, v, w, c within 1e-12 relative L2 (measured 2e-13, growing
-    linearly by ~4e-16 per step), max divergence <= 1e-12.  The pressure sits
-    at a constant 0.9-1.2e-10 from the first steps on, without growth: this
-    scheme passes every velocity field through 2-D transforms each substep,
-    whose rounding (a different FFT from the oracle's) enters u* at O(eps),
-    and p is the inverse Laplacian of div(u*) / dt, which amplifies that by
-    ~1/dt.  The bar for p here is therefore 2e-10."""
+    dt 1e-3): u, v, w, c within 1e-12 relative L2 (measured 2e-13), max
+    divergence <= 1e-12.  This scheme passes every velocity field through 2-D
+    transforms each substep, and p, the inverse Laplacian of div(u*) / dt,
+    amplifies their rounding by ~1/dt.  The reference itself moves by the
+    same amount when only its FFT is replaced by another correct one
+    (tests/test_oracle_fft_sensitivity.py): after these 100 steps its own p
+    moves by 1.17e-10 (order 2) and 1.07e-10 (order 4), its u, v, w, c by
+    3.6e-14 .. 2.0e-13 -- what the engine measures against it.  The bar for
+    p is therefore twice that spread, 2.4e-10 (order 2) and 2.2e-10
+    (order 4), in place of 1e-10."""
     prm = params(order, 64, 64, 32, lx=4 * np.pi, ly=4 * np.pi / 3, nu=1 / 2800.0, prandtl=1.0)
     R, F = projected_state(ref, prm, 0, 0.1, 0.01)
     with cf.Instance(cf.Config.from_params(prm, scheme="channel")) as inst:
@@ -122,7 +125,8 @@ def test_channel_100_steps(cf, ref, gpu, order):
         for nm in "uvwcp":
             worst[nm] = rel(interior(inst.get_field(nm), prm), interior(R.get(nm), prm))
         assert all(worst[nm] <= 1e-12 for nm in "uvwc"), worst
-        assert worst["p"] <= 2e-10, worst
+        fft_spread = {2: 1.17e-10, 4: 1.07e-10}[order]   # the reference's own, above
+        assert worst["p"] <= 2.0 * fft_spread, worst
         assert inst.max_divergence() <= 1e-12
         assert logs_close(inst.log(), R.log())
     R.close()

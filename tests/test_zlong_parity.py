@@ -33,12 +33,20 @@ def interior(a, p):
     return a[p.ngx:p.ngx + p.nx, p.ngy:p.ngy + p.ny, p.ngz:p.ngz + p.nz]
 
 
-def log_mismatch(a, b):
-    """Worst |a - b| / (1e-9 x column scale) over the per-substep log rows
-    (the bar of test_gpu_parity.logs_close), with its row and column."""
+def log_mismatch(a, b, dt):
+    """Worst |a - b| / bar over the per-substep log rows, with its row and
+    column.  The bar is 1e-9 x the column's scale (test_gpu_parity.logs_close),
+    and for the two control values -- mdpdx (column 0) and dcdt (column 5),
+    (target - bulk mean) / Green's-function mean, where the bulk mean sums
+    every point in another order than the reference's loop -- at least
+    1e-14 / dt: a control that differs by m shifts that substep's bulk mean
+    by at most m gamma dt < m dt, so this keeps the shift below 1e-14 of
+    the O(1) field (the fields themselves are compared at 1e-13)."""
     assert a.shape == b.shape, (a.shape, b.shape)
     scale = np.maximum(np.abs(b).max(axis=0), 1e-3)
-    r = np.abs(a - b) / (1e-9 * scale)
+    bar = 1e-9 * scale
+    bar[[0, 5]] = np.maximum(bar[[0, 5]], 1e-14 / dt)
+    r = np.abs(a - b) / bar
     i, j = np.unravel_index(np.argmax(r), r.shape)
     return float(r[i, j]), (int(i), int(j), float(a[i, j]), float(b[i, j]))
 
@@ -78,7 +86,7 @@ def test_order4_scalar_100_steps(cf, refjobs, gpu):
         print(name, 300, {k: "%.2e" % v for k, v in err.items()})
         assert all(err[nm] <= 1e-10 for nm in "uvwcp"), err
         check_divergence(inst, refjobs, name, 300)
-        worst, where = log_mismatch(inst.log(), refjobs.wait(name, "s300_log"))
+        worst, where = log_mismatch(inst.log(), refjobs.wait(name, "s300_log"), prm.dt)
         assert worst <= 1.0, where
 
 
@@ -97,7 +105,7 @@ def test_config1_grid_30_substeps(cf, refjobs, gpu):
             print(name, n, {k: "%.2e" % v for k, v in err.items()})
             assert all(err[nm] <= 1e-13 for nm in "uvwc"), (n, err)
             assert err["p"] <= 1e-10, (n, err)
-            worst, where = log_mismatch(inst.log(), refjobs.wait(name, f"s{n}_log"))
+            worst, where = log_mismatch(inst.log(), refjobs.wait(name, f"s{n}_log"), prm.dt)
             print(name, n, "log", worst, where)
             assert worst <= 1.0, where
             check_divergence(inst, refjobs, name, n)
@@ -115,7 +123,7 @@ def test_config2_grid_substep(cf, refjobs, gpu):
         print(name, 1, {k: "%.2e" % v for k, v in err.items()})
         assert all(err[nm] <= 1e-13 for nm in "uvwc"), err
         assert err["p"] <= 1e-10, err
-        worst, where = log_mismatch(inst.log(), refjobs.wait(name, "s1_log"))
+        worst, where = log_mismatch(inst.log(), refjobs.wait(name, "s1_log"), prm.dt)
         print(name, 1, "log", worst, where)
         assert worst <= 1.0, where
         check_divergence(inst, refjobs, name, 1)
