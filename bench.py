@@ -430,7 +430,12 @@ def run_ensemble(args):
     """Solves/hour of the ensemble batched (cf_batch: one launch per stage
     for all 64 instances, replayed as a CUDA graph) against the same
     instances one after another through the plain path (cf_step_graph), both
-    on device time; a solve is 500 RK3 steps, timed over args.steps."""
+    on device time; a solve is 500 RK3 steps, timed over args.steps.  Both
+    arms start from the same seeded states and run the same steps, so every
+    member is then compared with its plain-path run (relative L2 of u, v, w,
+    c; the batched kernels are other instantiations of the same bodies and
+    may contract multiply-adds differently)."""
+    import numpy as np
     import torch
     cf = importlib.import_module("ubiquitous-spoon_b200")
     torch.cuda.set_device(0)
@@ -465,19 +470,24 @@ def run_ensemble(args):
         t_batch = time.perf_counter() - t0
     launches = B.launches_per_substep()
     div = max(inst.max_divergence() for inst in insts)
+    batched = [{nm: inst.get_field(nm, layout=cf.LAYOUT_INTERIOR) for nm in "uvwc"} for inst in insts]
     B.close()
     for inst in insts:
         inst.close()
     # one after another, plain path
     insts = create()
     t_seq = 0.0
-    for inst in insts:
+    worst = {nm: 0.0 for nm in "uvwc"}
+    for m, inst in enumerate(insts):
         inst.step_graph(args.warmup)
         inst.sync()
         t0 = time.perf_counter()
         inst.step_graph(args.steps)
         inst.sync()
         t_seq += time.perf_counter() - t0
+        for nm in "uvwc":
+            a, b = batched[m][nm], inst.get_field(nm, layout=cf.LAYOUT_INTERIOR)
+            worst[nm] = max(worst[nm], float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
         inst.close()
     solve_steps = 500
     per_h = lambda t: len(members) / (t * solve_steps / args.steps) * 3600.0
@@ -497,6 +507,8 @@ def run_ensemble(args):
                    "solve": f"{solve_steps} RK3 steps (timed over {args.steps}, scaled)",
                    "points": pts, "timing": "wall clock around stream-synchronised runs"},
         "max_divergence": div, "clocks": clk.summary(),
+        "members_vs_plain_path": {"members": len(members), "max_rel_l2": {k: float(f"{v:.3e}") for k, v in worst.items()},
+                                  "within_1e-13": all(v <= 1e-13 for v in worst.values())},
     }
     print(json.dumps(result), flush=True)
 
@@ -536,8 +548,9 @@ def run_serve(args):
     trace = serve_trace(args.serve_requests, 4.0, args.serve_step_scale)
     reqs = []
     for r in trace:
-        cfg = cf.Config.make(order=r["order"], nx=r["nx"], ny=r["ny"], nz=r["nz"], lx=2 * math.pi, ly=math.pi,
-                             lz=2.0, dt=2.5e-4 if r["nx"] >= 256 else 1e-3, nu=1.0 / r["re"], prandtl=0.71)
+        # the ensemble's box and time step (4pi x 4pi/3 x 2, dt 1e-3)
+        cfg = cf.Config.make(order=r["order"], nx=r["nx"], ny=r["ny"], nz=r["nz"], lx=4 * math.pi,
+                             ly=4 * math.pi / 3, lz=2.0, dt=1e-3, nu=1.0 / r["re"], prandtl=0.71)
         reqs.append(dict(cfg=cfg, seed=r["seed"], amp=0.05, c_amp=0.01, nsteps=r["nsteps"],
                          arrival_s=r["arrival_s"]))
 
@@ -562,6 +575,7 @@ def run_serve(args):
                                      + ", ".join("x".join(map(str, g)) for g in SERVE_GRIDS)
                                      + ", Re_b log-U[2800, 20000], order 2 or 4",
                          "steps": f"U[200, 2000] x {args.serve_step_scale} RK3 steps per request",
+                         "box": "4pi x 4pi/3 x 2, dt 1e-3",
                          "admission": "150 GB budget by cf_instance_bytes, at most 64 resident",
                          "rounds": f"{args.serve_quantum} RK3 step(s) of every resident solve per batched call"},
               "clocks": clk.summary()}

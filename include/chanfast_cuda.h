@@ -209,6 +209,12 @@ int cf_z_coords(const cf_instance *inst, double *zp, double *zw);         /* get
 typedef struct cf_batch cf_batch;
 int cf_batch_step(cf_instance **members, int n, int nsub, void *stream);
 int cf_batch_create(cf_instance **members, int n, void *stream, cf_batch **out);
+/* cf_batch_create with options: CF_BATCH_NO_TUNE skips the launch-shape
+ * trials (a member set tuned before keeps its cached shape, others take the
+ * defaults) -- for a caller that forms a new batch whenever its member set
+ * changes, as the serving loop does. */
+#define CF_BATCH_NO_TUNE 1
+int cf_batch_create_opts(cf_instance **members, int n, void *stream, int flags, cf_batch **out);
 int cf_batch_run(cf_batch *batch, int nsteps);
 int cf_batch_sync(cf_batch *batch);
 /* Batched launches per substep of the whole batch (all members together). */

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cctype>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -1286,11 +1287,18 @@ void tune_store(const std::string& key, const LaunchShape& S)
     }
 }
 
+// Device model, compute capability and SM count: launch shapes tuned on one
+// model are not reused on another (a cache file may be shared).  One
+// whitespace-free token, as the cache file's first field.
 std::string device_tag(int device)
 {
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    return "sm" + std::to_string(sms);
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return "unknown";
+    std::string name = p.name;
+    for (char& ch : name)
+        if (!std::isalnum((unsigned char) ch)) ch = '_';
+    return name + "-cc" + std::to_string(p.major) + std::to_string(p.minor) + "-sm"
+         + std::to_string(p.multiProcessorCount);
 }
 
 std::string config_key(const cf_instance* I)
@@ -2075,7 +2083,7 @@ int cf_batch_destroy(cf_batch* B)
     return CF_OK;
 }
 
-static int batch_create_impl(cf_batch* B, cf_instance** members, int n, void* stream)
+static int batch_create_impl(cf_batch* B, cf_instance** members, int n, void* stream, bool tune)
 {
     B->v.assign(members, members + n);
     B->device = members[0]->device;
@@ -2087,7 +2095,10 @@ static int batch_create_impl(cf_batch* B, cf_instance** members, int n, void* st
     }
     CF_CUDA(cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming));
     int trc = join_streams(B->v, B->stream, B->ev, true);   // members' pending work first
-    if (trc == CF_OK) trc = tune_batch(B->v, B->stream, B->shape);
+    if (trc == CF_OK) {
+        if (tune) trc = tune_batch(B->v, B->stream, B->shape);
+        else B->shape = batch_cached_shape(B->v);
+    }
     if (trc) return trc;
     std::vector<long> start;
     for (cf_instance* I : B->v) start.push_back(I->substep);
@@ -2115,7 +2126,12 @@ static int batch_create_impl(cf_batch* B, cf_instance** members, int n, void* st
 
 int cf_batch_create(cf_instance** members, int n, void* stream, cf_batch** out)
 {
-    if (!out) return CF_EINVAL;
+    return cf_batch_create_opts(members, n, stream, 0, out);
+}
+
+int cf_batch_create_opts(cf_instance** members, int n, void* stream, int flags, cf_batch** out)
+{
+    if (!out || (flags & ~CF_BATCH_NO_TUNE)) return CF_EINVAL;
     *out = nullptr;
     int rc = check_members(members, n);
     if (rc) return rc;
@@ -2124,7 +2140,7 @@ int cf_batch_create(cf_instance** members, int n, void* stream, cf_batch** out)
     int prev = 0;
     CF_CUDA(cudaGetDevice(&prev));
     CF_CUDA(cudaSetDevice(members[0]->device));
-    rc = batch_create_impl(B, members, n, stream);
+    rc = batch_create_impl(B, members, n, stream, !(flags & CF_BATCH_NO_TUNE));
     cudaSetDevice(prev);
     if (rc) {
         cf_batch_destroy(B);

@@ -4,7 +4,11 @@
 // slot limit allow, stays resident on the device, is advanced together with
 // every other resident solve by one batched launch per substep stage, and is
 // retired on its own as soon as it has run its steps.  Requests that arrive
-// while others run join the next round: continuous batching.
+// while others run join the next round: continuous batching.  While the set
+// of solves advancing by a full quantum stays the same from round to round,
+// its recorded batch (per-instance records uploaded once, two steps replayed
+// as one CUDA graph) is replayed; it is formed again, without launch-shape
+// trials, only when that set changes.
 #include <algorithm>
 #include <chrono>
 #include <thread>
@@ -49,12 +53,20 @@ extern "C" int cf_serve(const cf_request* reqs, int n, double hbm_budget_bytes, 
     }
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<Active> active;
+    cf_batch* batch = nullptr;              // recorded batch of the full-quantum set
+    std::vector<cf_instance*> batch_set;
+    auto drop_batch = [&]() {
+        if (batch) cf_batch_destroy(batch);
+        batch = nullptr;
+        batch_set.clear();
+    };
     std::vector<double> bytes(n, 0.0);
     double used = 0.0;
     int next = 0, done = 0, rc = CF_OK;
 
     auto retire = [&](size_t a, int status) {
         Active& A = active[a];
+        if (std::find(batch_set.begin(), batch_set.end(), A.inst) != batch_set.end()) drop_batch();
         cf_result& R = results[A.index];
         R.status = status;
         R.finish_s = seconds_since(t0);
@@ -122,7 +134,21 @@ extern "C" int cf_serve(const cf_request* reqs, int n, double hbm_budget_bytes, 
                 if ((pass == 0 && A.remaining >= q_full) || (pass == 1 && A.remaining < q_full))
                     group.push_back(A.inst);
             if (group.empty()) continue;
-            int s = cf_batch_step(group.data(), (int) group.size(), 3 * steps, st);
+            int s;
+            if (pass == 0) {   // the full-quantum set: its recorded batch
+                if (group != batch_set) {
+                    drop_batch();
+                    s = cf_batch_create_opts(group.data(), (int) group.size(), st, CF_BATCH_NO_TUNE, &batch);
+                    if (s != CF_OK) {
+                        rc = s;
+                        break;
+                    }
+                    batch_set = group;
+                }
+                s = cf_batch_run(batch, steps);
+            } else {
+                s = cf_batch_step(group.data(), (int) group.size(), 3 * steps, st);
+            }
             if (s != CF_OK) {
                 rc = s;
                 break;
@@ -149,6 +175,7 @@ extern "C" int cf_serve(const cf_request* reqs, int n, double hbm_budget_bytes, 
             else a++;
         }
     }
+    drop_batch();
     for (size_t a = active.size(); a-- > 0;) retire(a, rc == CF_OK ? CF_OK : rc);
     if (own) cudaStreamDestroy(st);
     return rc;
