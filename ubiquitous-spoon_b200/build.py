@@ -76,7 +76,7 @@ def build(verbose=False, ptxas_info=False):
         _run([NVCC, *ARCH, "-shared", "-o", LIB_CUDA, *objs, "-lcudart"])
     steps_src = os.path.join(CSRC, STEPS_SOURCE)
     steps_hdr = os.path.join(INCLUDE, "chanfast_steps.h")
-    if os.path.exists(steps_src) and _stale(LIB_STEPS, [steps_src, steps_hdr]):
+    if os.path.exists(steps_src) and _stale(LIB_STEPS, [steps_src, steps_hdr] + headers):
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--extended-lambda", "-Xcompiler",
                "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", INCLUDE, "-shared", steps_src, "-o", LIB_STEPS,
                "-Xlinker", "-Bsymbolic", "-lcudart"]

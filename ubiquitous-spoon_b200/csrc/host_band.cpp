@@ -2,6 +2,7 @@
 // restates the reference closure or band row named beside it, keeping its
 // evaluation order (x86-64 builds without FMA contraction).
 #include "host_band.h"
+#include "closures.h"
 
 #include <algorithm>
 #include <cmath>
@@ -39,296 +40,65 @@ Metrics make_metrics(int order, int nx, int ny, int nz, int gz, double lx, doubl
 }
 
 // ---------------------------------------------------------------- closures
-// Cell-centred fields and pressure (diffuseu.c:617-940, pressure.c:446-770).
+// Cell-centred fields and pressure (diffuseu.c:617-940, pressure.c:446-770),
+// face fields (diffusew.c:617-884): closures.h, shared with the device step
+// functions, over a view of the Band.
+
+struct BandRef {
+    Band& B;
+    double& a(int k) const { return B.a[k]; }
+    double& b(int k) const { return B.b[k]; }
+    double& c(int k) const { return B.c[k]; }
+    double& d(int k) const { return B.d[k]; }
+    double& e(int k) const { return B.e[k]; }
+    double& f(int k) const { return B.f[k]; }
+    double& g(int k) const { return B.g[k]; }
+    double& r(int k) const { return B.r[k]; }
+    double& x(int k) const { return B.x[k]; }
+};
 
 static void u_stencil_bot2(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
 {
-    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-    if (t == BC_NEUMANN) { B.a[k] = 0.0; B.b[k] = -1.0 / dzp1h; B.c[k] = +1.0 / dzp1h; }
-    else { B.a[k] = 0.0; B.b[k] = 0.5; B.c[k] = 0.5; }
-    B.r[k] = bc;
+    closure::cell_stencil_bot2(BandRef{B}, dz.data(), k, bc, t == BC_NEUMANN);
 }
-
 static void u_stencil_top2(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
 {
-    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-    if (t == BC_NEUMANN) { B.a[k] = -1.0 / dzm1h; B.b[k] = +1.0 / dzm1h; B.c[k] = 0.0; }
-    else { B.a[k] = 0.5; B.b[k] = 0.5; B.c[k] = 0.0; }
-    B.r[k] = bc;
+    closure::cell_stencil_top2(BandRef{B}, dz.data(), k, bc, t == BC_NEUMANN);
 }
-
-static void u_reduce_bot2(Band& B, int k)
-{
-    int kp1 = k + 1;
-    double fac = B.a[kp1] / B.b[k];
-    B.a[kp1] -= B.b[k] * fac;
-    B.b[kp1] -= B.c[k] * fac;
-    B.r[kp1] -= B.r[k] * fac;
-}
-
-static void u_reduce_top2(Band& B, int k)
-{
-    int km1 = k - 1;
-    double fac = B.c[km1] / B.b[k];
-    B.c[km1] -= B.b[k] * fac;
-    B.b[km1] -= B.a[k] * fac;
-    B.r[km1] -= B.r[k] * fac;
-}
-
-static void u_fill_bot2(Band& B, int k) { B.x[k] = (B.c[k] * B.x[k + 1] - B.r[k]) / -B.b[k]; }
-static void u_fill_top2(Band& B, int k) { B.x[k] = (B.a[k] * B.x[k - 1] - B.r[k]) / -B.b[k]; }
-
+static void u_reduce_bot2(Band& B, int k) { closure::cell_reduce_bot2(BandRef{B}, k); }
+static void u_reduce_top2(Band& B, int k) { closure::cell_reduce_top2(BandRef{B}, k); }
+static void u_fill_bot2(Band& B, int k) { closure::cell_fill_bot2(BandRef{B}, k); }
+static void u_fill_top2(Band& B, int k) { closure::cell_fill_top2(BandRef{B}, k); }
 static void u_stencil_bot4(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
 {
-    int km2 = k - 2, km1 = k - 1;
-    double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
-    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-    B.a[k] = 0.0;
-    B.b[k] = -A2 / dzm1h;
-    B.c[k] = -A1 / dzm1h - 2.0 * -A2 / dzp1h;
-    B.d[k] = +A1 / dzm1h - 2.0 * -A1 / dzp1h - A2 / dzp3h;
-    B.e[k] = +A2 / dzm1h - 2.0 * +A1 / dzp1h - A1 / dzp3h;
-    B.f[k] = -2.0 * +A2 / dzp1h + A1 / dzp3h;
-    B.g[k] = +A2 / dzp3h;
-    B.r[k] = 0.0;
-    B.a[km1] = 0.0; B.b[km1] = 0.0; B.c[km1] = 0.0;
-    if (t == BC_NEUMANN) {
-        B.d[km1] = -A2 / dzp1h; B.e[km1] = -A1 / dzp1h; B.f[km1] = +A1 / dzp1h; B.g[km1] = +A2 / dzp1h;
-    } else {
-        B.d[km1] = 0.5 * A2; B.e[km1] = 0.5 * (A1 + 2.0 * A2);
-        B.f[km1] = 0.5 * (A1 + 2.0 * A2); B.g[km1] = 0.5 * A2;
-    }
-    B.r[km1] = bc;
-    B.a[km2] = 0.0; B.b[km2] = 0.0; B.c[km2] = 0.0; B.d[km2] = 0.0; B.e[km2] = 0.0;
-    B.f[km2] = -1.0; B.g[km2] = +1.0; B.r[km2] = 0.0;
+    closure::cell_stencil_bot4(BandRef{B}, dz.data(), k, bc, t == BC_NEUMANN, A1, A2);
 }
-
 static void u_stencil_top4(Band& B, const std::vector<double>& dz, int k, double bc, BcKind t)
 {
-    int kp2 = k + 2, kp1 = k + 1;
-    double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-    double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-    double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
-    B.a[k] = -A2 / dzm3h;
-    B.b[k] = -A1 / dzm3h - 2.0 * -A2 / dzm1h;
-    B.c[k] = +A1 / dzm3h - 2.0 * -A1 / dzm1h - A2 / dzp1h;
-    B.d[k] = +A2 / dzm3h - 2.0 * +A1 / dzm1h - A1 / dzp1h;
-    B.e[k] = -2.0 * +A2 / dzm1h + A1 / dzp1h;
-    B.f[k] = +A2 / dzp1h;
-    B.g[k] = 0.0;
-    B.r[k] = 0.0;
-    if (t == BC_NEUMANN) {
-        B.a[kp1] = -A2 / dzm1h; B.b[kp1] = -A1 / dzm1h; B.c[kp1] = +A1 / dzm1h; B.d[kp1] = +A2 / dzm1h;
-    } else {
-        B.a[kp1] = 0.5 * A2; B.b[kp1] = 0.5 * (A1 + 2.0 * A2);
-        B.c[kp1] = 0.5 * (A1 + 2.0 * A2); B.d[kp1] = 0.5 * A2;
-    }
-    B.e[kp1] = 0.0; B.f[kp1] = 0.0; B.g[kp1] = 0.0; B.r[kp1] = bc;
-    B.a[kp2] = -1.0; B.b[kp2] = +1.0; B.c[kp2] = 0.0; B.d[kp2] = 0.0;
-    B.e[kp2] = 0.0; B.f[kp2] = 0.0; B.g[kp2] = 0.0; B.r[kp2] = 0.0;
+    closure::cell_stencil_top4(BandRef{B}, dz.data(), k, bc, t == BC_NEUMANN, A1, A2);
 }
+// `dsub` (optional) receives the diagonal subtractions (closures.h)
+static void u_reduce_bot4(Band& B, int k, double dsub[3][3]) { closure::cell_reduce_bot4(BandRef{B}, k, dsub); }
+static void u_reduce_top4(Band& B, int k, double dsub[3][3]) { closure::cell_reduce_top4(BandRef{B}, k, dsub); }
+static void u_fill_bot4(Band& B, int k) { closure::cell_fill_bot4(BandRef{B}, k); }
+static void u_fill_top4(Band& B, int k) { closure::cell_fill_top4(BandRef{B}, k); }
 
-// Bottom elimination of the ghost rows of a 7-band system (diffuseu.c:807-850).
-// `dsub` (optional) receives the three diagonal subtractions of rows k+1 and
-// the one of row k+2, in order, for the per-column diagonal of the pressure.
-static void u_reduce_bot4(Band& B, int k, double dsub[3][3])
-{
-    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
-    auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
-    auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
-    double fac, t;
-    fac = a[kp1] / b[k];
-    a[kp1] -= b[k] * fac; b[kp1] -= c[k] * fac; c[kp1] -= d[k] * fac;
-    t = e[k] * fac; d[kp1] -= t; if (dsub) dsub[0][0] = t;
-    e[kp1] -= f[k] * fac; f[kp1] -= g[k] * fac;
-    fac = b[kp1] / d[km1];
-    b[kp1] -= d[km1] * fac; c[kp1] -= e[km1] * fac;
-    t = f[km1] * fac; d[kp1] -= t; if (dsub) dsub[0][1] = t;
-    e[kp1] -= g[km1] * fac; r[kp1] -= r[km1] * fac;
-    fac = c[kp1] / f[km2];
-    c[kp1] -= f[km2] * fac;
-    t = g[km2] * fac; d[kp1] -= t; if (dsub) dsub[0][2] = t;
-    fac = a[kp2] / d[km1];
-    a[kp2] -= d[km1] * fac; b[kp2] -= e[km1] * fac; c[kp2] -= f[km1] * fac;
-    t = g[km1] * fac; d[kp2] -= t; if (dsub) dsub[1][0] = t;
-    r[kp2] -= r[km1] * fac;
-    fac = b[kp2] / f[km2];
-    b[kp2] -= f[km2] * fac; c[kp2] -= g[km2] * fac;
-    fac = a[kp3] / f[km2];
-    a[kp3] -= f[km2] * fac; b[kp3] -= g[km2] * fac;
-}
-
-// Top elimination (diffuseu.c:853-896); dsub rows: k-1 (three), k-2 (one).
-static void u_reduce_top4(Band& B, int k, double dsub[3][3])
-{
-    int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
-    auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
-    auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
-    double fac, t;
-    fac = g[km1] / f[k];
-    g[km1] -= f[k] * fac; f[km1] -= e[k] * fac; e[km1] -= d[k] * fac;
-    t = c[k] * fac; d[km1] -= t; if (dsub) dsub[0][0] = t;
-    c[km1] -= b[k] * fac; b[km1] -= a[k] * fac;
-    fac = f[km1] / d[kp1];
-    f[km1] -= d[kp1] * fac; e[km1] -= c[kp1] * fac;
-    t = b[kp1] * fac; d[km1] -= t; if (dsub) dsub[0][1] = t;
-    c[km1] -= a[kp1] * fac; r[km1] -= r[kp1] * fac;
-    fac = e[km1] / b[kp2];
-    e[km1] -= b[kp2] * fac;
-    t = a[kp2] * fac; d[km1] -= t; if (dsub) dsub[0][2] = t;
-    fac = g[km2] / d[kp1];
-    g[km2] -= d[kp1] * fac; f[km2] -= c[kp1] * fac; e[km2] -= b[kp1] * fac;
-    t = a[kp1] * fac; d[km2] -= t; if (dsub) dsub[1][0] = t;
-    r[km2] -= r[kp1] * fac;
-    fac = f[km2] / b[kp2];
-    f[km2] -= b[kp2] * fac; e[km2] -= a[kp2] * fac;
-    fac = g[km3] / b[kp2];
-    g[km3] -= b[kp2] * fac; f[km3] -= a[kp2] * fac;
-}
-
-static void u_fill_bot4(Band& B, int k)
-{
-    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
-    auto& x = B.x;
-    x[k] = (B.g[km2] * x[kp1]) / -B.f[km2];
-    x[km1] = (B.e[km1] * x[k] + B.f[km1] * x[kp1] + B.g[km1] * x[kp2] - B.r[km1]) / -B.d[km1];
-    x[km2] = (B.c[k] * x[km1] + B.d[k] * x[k] + B.e[k] * x[kp1] + B.f[k] * x[kp2]
-              + B.g[k] * x[kp3]) / -B.b[k];
-}
-
-static void u_fill_top4(Band& B, int k)
-{
-    int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
-    auto& x = B.x;
-    x[k] = (B.a[kp2] * x[km1]) / -B.b[kp2];
-    x[kp1] = (B.a[kp1] * x[km2] + B.b[kp1] * x[km1] + B.c[kp1] * x[k] - B.r[kp1]) / -B.d[kp1];
-    x[kp2] = (B.a[k] * x[km3] + B.b[k] * x[km2] + B.c[k] * x[km1] + B.d[k] * x[k]
-              + B.e[k] * x[kp1]) / -B.f[k];
-}
-
-// Face fields (diffusew.c:617-884); Dirichlet only.
-static void w_stencil2(Band& B, int k, double bc) { B.a[k] = 0.0; B.b[k] = 1.0; B.c[k] = 0.0; B.r[k] = bc; }
-
-static void w_reduce_bot2(Band& B, int k)
-{
-    int kp1 = k + 1;
-    double fac = B.a[kp1] / B.b[k];
-    B.a[kp1] -= B.b[k] * fac;
-    B.r[kp1] -= B.r[k] * fac;
-}
-
-static void w_reduce_top2(Band& B, int k)
-{
-    int km1 = k - 1;
-    double fac = B.c[km1] / B.b[k];
-    B.c[km1] -= B.b[k] * fac;
-    B.r[km1] -= B.r[k] * fac;
-}
-
-static void w_fill2(Band& B, int k) { B.x[k] = (-B.r[k]) / -B.b[k]; }
-
+static void w_stencil2(Band& B, int k, double bc) { closure::face_stencil2(BandRef{B}, k, bc); }
+static void w_reduce_bot2(Band& B, int k) { closure::face_reduce_bot2(BandRef{B}, k); }
+static void w_reduce_top2(Band& B, int k) { closure::face_reduce_top2(BandRef{B}, k); }
+static void w_fill2(Band& B, int k) { closure::face_fill2(BandRef{B}, k); }
 static void w_stencil_bot4(Band& B, const std::vector<double>& dz, int k, double bc)
 {
-    int km2 = k - 2, km1 = k - 1;
-    double dzp0 = dz[k], dzp1 = dz[k + 1];
-    B.a[k] = 0.0;
-    B.b[k] = -A2 / dzp0;
-    B.c[k] = -A1 / dzp0 + A2 / dzp1;
-    B.d[k] = +A1 / dzp0 + A1 / dzp1;
-    B.e[k] = +A2 / dzp0 - A1 / dzp1;
-    B.f[k] = -A2 / dzp1;
-    B.g[k] = 0.0;
-    B.r[k] = 0.0;
-    B.a[km1] = 0.0; B.b[km1] = 0.0; B.c[km1] = 0.0; B.d[km1] = -1.0; B.e[km1] = +2.0;
-    B.f[km1] = -1.0; B.g[km1] = 0.0; B.r[km1] = 0.0;
-    B.a[km2] = 0.0; B.b[km2] = 0.0; B.c[km2] = 0.0; B.d[km2] = 0.0; B.e[km2] = 0.0;
-    B.f[km2] = 1.0; B.g[km2] = 0.0; B.r[km2] = bc;
+    closure::face_stencil_bot4(BandRef{B}, dz.data(), k, bc, A1, A2);
 }
-
 static void w_stencil_top4(Band& B, const std::vector<double>& dz, int k, double bc)
 {
-    int kp2 = k + 2, kp1 = k + 1;
-    double dzp0 = dz[k], dzp1 = dz[k + 1];
-    B.a[k] = 0.0;
-    B.b[k] = -A2 / dzp0;
-    B.c[k] = -A1 / dzp0 + A2 / dzp1;
-    B.d[k] = +A1 / dzp0 + A1 / dzp1;
-    B.e[k] = +A2 / dzp0 - A1 / dzp1;
-    B.f[k] = -A2 / dzp1;
-    B.g[k] = 0.0;
-    B.r[k] = 0.0;
-    B.a[kp1] = 0.0; B.b[kp1] = -1.0; B.c[kp1] = +2.0; B.d[kp1] = -1.0;
-    B.e[kp1] = 0.0; B.f[kp1] = 0.0; B.g[kp1] = 0.0; B.r[kp1] = 0.0;
-    B.a[kp2] = 0.0; B.b[kp2] = 1.0; B.c[kp2] = 0.0; B.d[kp2] = 0.0;
-    B.e[kp2] = 0.0; B.f[kp2] = 0.0; B.g[kp2] = 0.0; B.r[kp2] = bc;
+    closure::face_stencil_top4(BandRef{B}, dz.data(), k, bc, A1, A2);
 }
-
-// `dsub` (optional) receives the two diagonal subtractions of row k+1.
-static void w_reduce_bot4(Band& B, int k, double dsub[3][3] = nullptr)
-{
-    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2, kp3 = k + 3;
-    auto& a = B.a; auto& b = B.b; auto& c = B.c; auto& d = B.d;
-    auto& e = B.e; auto& f = B.f; auto& r = B.r;
-    double fac, t;
-    fac = a[kp1] / b[k];
-    a[kp1] -= b[k] * fac; b[kp1] -= c[k] * fac; c[kp1] -= d[k] * fac;
-    t = e[k] * fac; d[kp1] -= t; if (dsub) dsub[0][0] = t;
-    e[kp1] -= f[k] * fac;
-    fac = b[kp1] / d[km1];
-    b[kp1] -= d[km1] * fac; c[kp1] -= e[km1] * fac;
-    t = f[km1] * fac; d[kp1] -= t; if (dsub) dsub[0][1] = t;
-    fac = c[kp1] / f[km2];
-    c[kp1] -= f[km2] * fac; r[kp1] -= r[km2] * fac;
-    fac = a[kp2] / d[km1];
-    a[kp2] -= d[km1] * fac; b[kp2] -= e[km1] * fac; c[kp2] -= f[km1] * fac;
-    fac = b[kp2] / f[km2];
-    b[kp2] -= f[km2] * fac; r[kp2] -= r[km2] * fac;
-    fac = a[kp3] / f[km2];
-    a[kp3] -= f[km2] * fac; r[kp3] -= r[km2] * fac;
-}
-
-// `dsub` (optional) receives the two diagonal subtractions of row k-1.
-static void w_reduce_top4(Band& B, int k, double dsub[3][3] = nullptr)
-{
-    int km3 = k - 3, km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
-    auto& b = B.b; auto& c = B.c; auto& d = B.d;
-    auto& e = B.e; auto& f = B.f; auto& g = B.g; auto& r = B.r;
-    double fac, t;
-    fac = g[km1] / f[k];
-    g[km1] -= f[k] * fac; f[km1] -= e[k] * fac; e[km1] -= d[k] * fac;
-    t = c[k] * fac; d[km1] -= t; if (dsub) dsub[0][0] = t;
-    c[km1] -= b[k] * fac;
-    fac = f[km1] / d[kp1];
-    f[km1] -= d[kp1] * fac; e[km1] -= c[kp1] * fac;
-    t = b[kp1] * fac; d[km1] -= t; if (dsub) dsub[0][1] = t;
-    fac = e[km1] / b[kp2];
-    e[km1] -= b[kp2] * fac; r[km1] -= r[kp2] * fac;
-    fac = g[km2] / d[kp1];
-    g[km2] -= d[kp1] * fac; f[km2] -= c[kp1] * fac; e[km2] -= b[kp1] * fac;
-    fac = f[km2] / b[kp2];
-    f[km2] -= b[kp2] * fac; r[km2] -= r[kp2] * fac;
-    fac = g[km3] / b[kp2];
-    g[km3] -= b[kp2] * fac; r[km3] -= r[kp2] * fac;
-}
-
-static void w_fill_bot4(Band& B, int k)
-{
-    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
-    auto& x = B.x;
-    x[k] = (-B.r[km2]) / -B.f[km2];
-    x[km1] = (B.e[km1] * x[k] + B.f[km1] * x[kp1]) / -B.d[km1];
-    x[km2] = (B.c[k] * x[km1] + B.d[k] * x[k] + B.e[k] * x[kp1] + B.f[k] * x[kp2]) / -B.b[k];
-}
-
-static void w_fill_top4(Band& B, int k)
-{
-    int km2 = k - 2, km1 = k - 1, kp1 = k + 1, kp2 = k + 2;
-    auto& x = B.x;
-    x[k] = (-B.r[kp2]) / -B.b[kp2];
-    x[kp1] = (B.b[kp1] * x[km1] + B.c[kp1] * x[k]) / -B.d[kp1];
-    x[kp2] = (B.b[k] * x[km2] + B.c[k] * x[km1] + B.d[k] * x[k] + B.e[k] * x[kp1]) / -B.f[k];
-}
+static void w_reduce_bot4(Band& B, int k, double dsub[3][3] = nullptr) { closure::face_reduce_bot4(BandRef{B}, k, dsub); }
+static void w_reduce_top4(Band& B, int k, double dsub[3][3] = nullptr) { closure::face_reduce_top4(BandRef{B}, k, dsub); }
+static void w_fill_bot4(Band& B, int k) { closure::face_fill_bot4(BandRef{B}, k); }
+static void w_fill_top4(Band& B, int k) { closure::face_fill_top4(BandRef{B}, k); }
 
 static WallRows rows_of(const Band& B, int k0, int step)
 {

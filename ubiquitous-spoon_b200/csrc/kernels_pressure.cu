@@ -428,9 +428,10 @@ __device__ __forceinline__ void k_fftx_c2r_body(const Geo& G, const C2rArgs& A, 
     FftCtx F{sbuf, nx, FFT_L, false, +1, A.px.tw, A.c8};
     if constexpr (N > 0) fft_static<N, false>(sbuf, F);
     else fft_run<FFT_MAXC>(F, A.px);
+    double* const pz = bid.z == 0 ? A.p[0] : bid.z == 1 ? A.p[1] : bid.z == 2 ? A.p[2] : A.p[3];
     for (int idx = threadIdx.x; idx < nx * FFT_L; idx += blockDim.x) {
         int i = idx / FFT_L, jj = idx - i * FFT_L, j = j0 + jj;
-        if (j < ny) A.p[bid.z][((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
+        if (j < ny) pz[((long long) k * nx + i) * ny + j] = sbuf[i * FFT_L + jj].x;
     }
 }
 
@@ -1201,7 +1202,10 @@ __device__ __forceinline__ void k_fftx_c2r_p2_body(const Geo& G, const C2rArgs& 
     }
     fft_p2_line<M>(v, t, sbuf + l * p2_stride_x(M), A.px.tw, +1, A.c8, 2);
     if (!valid) return;
-    double* out = A.p[bid.z] + (long long) k * G.nx * ny + j;
+    // the field's pointer picked without indexing the parameter array by a
+    // run-time value (which would copy the parameters to the stack)
+    double* const pz = bid.z == 0 ? A.p[0] : bid.z == 1 ? A.p[1] : bid.z == 2 ? A.p[2] : A.p[3];
+    double* out = pz + (long long) k * G.nx * ny + j;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int m = t + q * T;

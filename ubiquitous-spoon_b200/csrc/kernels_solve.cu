@@ -46,7 +46,6 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A, ui
     // x_{i+1} last (one dependent operation per row on the critical path);
     // s of row i - PD loaded into registers while row i is computed.
     constexpr int PD = 4;
-    static_assert(PD == 4, "the row-sum butterfly below reduces groups of four rows");
     double ps[PD];
     auto fetch_s = [&](int i, int slot) {
         if (i >= 0) ps[slot] = sv[(long long) (k0 + i) * P + cc];
@@ -58,11 +57,9 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A, ui
     const bool stats = A.partial != nullptr;
     const long long wrow = ((long long) bid.x * blockDim.x + threadIdx.x) / 32;
     for (int i0 = n - 1; i0 >= 0; i0 -= PD) {
-        double yr[PD];   // this group's rows i0 - u, for the row sums
 #pragma unroll
         for (int u = 0; u < PD; u++) {
             const int i = i0 - u;
-            yr[u] = 0.0;
             if (i >= 0) {
                 const int k = k0 + i;
                 const double s = ps[u];
@@ -78,27 +75,11 @@ __device__ __forceinline__ void back_column(const Geo& G, const SolveArgs& A, ui
                 if (i == 0) bot0 = y;
                 if (i == 1) bot1 = y;
                 if (i == 2) bot2 = y;
-                if (active) yr[u] = y;
+                if (stats) {
+                    double t = warp_sum(active ? y : 0.0);
+                    if ((threadIdx.x & 31) == 0) A.partial[wrow * n2 + k] = t;
+                }
             }
-        }
-        if (stats) {
-            // Warp sums of the group's four rows at once: each butterfly
-            // level halves the values a lane holds (xor 16: rows 0,1 | 2,3;
-            // xor 8: one row), then xor 4, 2, 1 finish the sum.  Lane L ends
-            // with row u = (L >> 3) & 3; lanes L % 8 == 0 store it.  Six
-            // exchanges for four rows instead of twenty; a fixed order.
-            const unsigned lane = threadIdx.x & 31u;
-            const bool h16 = lane & 16u, h8 = lane & 8u;
-            double q0 = h16 ? yr[2] : yr[0], q1 = h16 ? yr[3] : yr[1];
-            q0 += __shfl_xor_sync(0xffffffffu, h16 ? yr[0] : yr[2], 16);
-            q1 += __shfl_xor_sync(0xffffffffu, h16 ? yr[1] : yr[3], 16);
-            double t = h8 ? q1 : q0;
-            t += __shfl_xor_sync(0xffffffffu, h8 ? q0 : q1, 8);
-            t += __shfl_xor_sync(0xffffffffu, t, 4);
-            t += __shfl_xor_sync(0xffffffffu, t, 2);
-            t += __shfl_xor_sync(0xffffffffu, t, 1);
-            const int i = i0 - (int) ((lane >> 3) & 3u);
-            if ((lane & 7u) == 0 && i >= 0) A.partial[wrow * n2 + k0 + i] = t;
         }
     }
 

@@ -9,9 +9,13 @@
 // that consecutive threads touch consecutive addresses.
 #pragma once
 
+#include "closures.h"
 #include <cuda_runtime.h>
 
 namespace lines {
+
+namespace closure = cf::closure;
+
 
 // The fourth-order coefficients a1, a2, b1, b2 (fourth.c:3-6) in use.
 struct Coef {
@@ -101,226 +105,72 @@ __device__ inline void line_heptdag(const Lines& L, long long l, int off, int n)
 
 // ================================================ wall closures of the line solves
 //
-// A closure adds the wall rows of a column's band system (stencil), folds
-// them out of the first interior rows (reduce) and recovers the ghost values
-// from the solution (fill).  Cell-centred fields and the pressure share one
-// set (diffuseu.c:572-940, pressure.c:505-769: Neumann or Dirichlet at the
-// wall); face fields have their own (diffusew.c:555-905: the wall value is a
-// Dirichlet condition on the face itself).  k is the first ghost row below
-// (bot) or above (top) the interior.
+// The closures themselves (stencil, reduce, fill; cell-centred fields and
+// the pressure, face fields) are in closures.h, shared with the engine's
+// host factorisations; here they run over one line of the [k][line] band
+// storage.  k is the first ghost row below (bot) or above (top) the interior.
 
 struct Rows {
     const Lines& L;
     long long l;
-    __device__ double& a(int k) const { return L.a[(long long) k * L.nl + l]; }
-    __device__ double& b(int k) const { return L.b[(long long) k * L.nl + l]; }
-    __device__ double& c(int k) const { return L.c[(long long) k * L.nl + l]; }
-    __device__ double& d(int k) const { return L.d[(long long) k * L.nl + l]; }
-    __device__ double& e(int k) const { return L.e[(long long) k * L.nl + l]; }
-    __device__ double& f(int k) const { return L.f[(long long) k * L.nl + l]; }
-    __device__ double& g(int k) const { return L.g[(long long) k * L.nl + l]; }
-    __device__ double& r(int k) const { return L.r[(long long) k * L.nl + l]; }
-    __device__ double& x(int k) const { return L.x[(long long) k * L.nl + l]; }
+    CF_HD double& a(int k) const { return L.a[(long long) k * L.nl + l]; }
+    CF_HD double& b(int k) const { return L.b[(long long) k * L.nl + l]; }
+    CF_HD double& c(int k) const { return L.c[(long long) k * L.nl + l]; }
+    CF_HD double& d(int k) const { return L.d[(long long) k * L.nl + l]; }
+    CF_HD double& e(int k) const { return L.e[(long long) k * L.nl + l]; }
+    CF_HD double& f(int k) const { return L.f[(long long) k * L.nl + l]; }
+    CF_HD double& g(int k) const { return L.g[(long long) k * L.nl + l]; }
+    CF_HD double& r(int k) const { return L.r[(long long) k * L.nl + l]; }
+    CF_HD double& x(int k) const { return L.x[(long long) k * L.nl + l]; }
     // set row k to (a..g | rhs)
     __device__ inline void set(int k, double va, double vb, double vc, double vd, double ve, double vf, double vg,
                         double vr) const
     {
-        a(k) = va; b(k) = vb; c(k) = vc; d(k) = vd; e(k) = ve; f(k) = vf; g(k) = vg; r(k) = vr;
+        closure::set_row(*this, k, va, vb, vc, vd, ve, vf, vg, vr);
     }
 };
 
-// ---- cell fields and pressure, second order (three-band rows a, b, c)
 __device__ inline void cell_stencil_bot2(const Rows& R, const double* dz, int k, double bc, bool neumann)
 {
-    const double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-    R.a(k) = 0.0;
-    if (neumann) { R.b(k) = -1.0 / dzp1h; R.c(k) = +1.0 / dzp1h; }
-    else { R.b(k) = 0.5; R.c(k) = 0.5; }
-    R.r(k) = bc;
+    closure::cell_stencil_bot2(R, dz, k, bc, neumann);
 }
 __device__ inline void cell_stencil_top2(const Rows& R, const double* dz, int k, double bc, bool neumann)
 {
-    const double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-    if (neumann) { R.a(k) = -1.0 / dzm1h; R.b(k) = +1.0 / dzm1h; }
-    else { R.a(k) = 0.5; R.b(k) = 0.5; }
-    R.c(k) = 0.0;
-    R.r(k) = bc;
+    closure::cell_stencil_top2(R, dz, k, bc, neumann);
 }
-__device__ inline void cell_reduce_bot2(const Rows& R, int k)
-{
-    const double fac = R.a(k + 1) / R.b(k);
-    R.a(k + 1) -= R.b(k) * fac;
-    R.b(k + 1) -= R.c(k) * fac;
-    R.r(k + 1) -= R.r(k) * fac;
-}
-__device__ inline void cell_reduce_top2(const Rows& R, int k)
-{
-    const double fac = R.c(k - 1) / R.b(k);
-    R.c(k - 1) -= R.b(k) * fac;
-    R.b(k - 1) -= R.a(k) * fac;
-    R.r(k - 1) -= R.r(k) * fac;
-}
-__device__ inline void cell_fill_bot2(const Rows& R, int k) { R.x(k) = (R.c(k) * R.x(k + 1) - R.r(k)) / -R.b(k); }
-__device__ inline void cell_fill_top2(const Rows& R, int k) { R.x(k) = (R.a(k) * R.x(k - 1) - R.r(k)) / -R.b(k); }
-
-// ---- cell fields and pressure, fourth order (seven-band rows a..g)
+__device__ inline void cell_reduce_bot2(const Rows& R, int k) { closure::cell_reduce_bot2(R, k); }
+__device__ inline void cell_reduce_top2(const Rows& R, int k) { closure::cell_reduce_top2(R, k); }
+__device__ inline void cell_fill_bot2(const Rows& R, int k) { closure::cell_fill_bot2(R, k); }
+__device__ inline void cell_fill_top2(const Rows& R, int k) { closure::cell_fill_top2(R, k); }
 __device__ inline void cell_stencil_bot4(const Rows& R, const double* dz, int k, double bc, bool neumann, const Coef& cf)
 {
-    const double A1 = cf.a1, A2 = cf.a2;
-    const double dzp3h = 0.5 * (dz[k + 2] + dz[k + 1]);
-    const double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-    const double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-    // row k: the fourth-order second difference across the wall vanishes
-    R.set(k, 0.0, -A2 / dzm1h, -A1 / dzm1h - 2.0 * -A2 / dzp1h, +A1 / dzm1h - 2.0 * -A1 / dzp1h - A2 / dzp3h,
-          +A2 / dzm1h - 2.0 * +A1 / dzp1h - A1 / dzp3h, -2.0 * +A2 / dzp1h + A1 / dzp3h, +A2 / dzp3h, 0.0);
-    // row k-1: the boundary condition
-    if (neumann) R.set(k - 1, 0.0, 0.0, 0.0, -A2 / dzp1h, -A1 / dzp1h, +A1 / dzp1h, +A2 / dzp1h, bc);
-    else R.set(k - 1, 0.0, 0.0, 0.0, 0.5 * A2, 0.5 * (A1 + 2.0 * A2), 0.5 * (A1 + 2.0 * A2), 0.5 * A2, bc);
-    // row k-2: even extension of the outermost ghost
-    R.set(k - 2, 0.0, 0.0, 0.0, 0.0, 0.0, -1.0, +1.0, 0.0);
+    closure::cell_stencil_bot4(R, dz, k, bc, neumann, cf.a1, cf.a2);
 }
 __device__ inline void cell_stencil_top4(const Rows& R, const double* dz, int k, double bc, bool neumann, const Coef& cf)
 {
-    const double A1 = cf.a1, A2 = cf.a2;
-    const double dzp1h = 0.5 * (dz[k + 1] + dz[k]);
-    const double dzm1h = 0.5 * (dz[k - 1] + dz[k]);
-    const double dzm3h = 0.5 * (dz[k - 2] + dz[k - 1]);
-    R.set(k, -A2 / dzm3h, -A1 / dzm3h - 2.0 * -A2 / dzm1h, +A1 / dzm3h - 2.0 * -A1 / dzm1h - A2 / dzp1h,
-          +A2 / dzm3h - 2.0 * +A1 / dzm1h - A1 / dzp1h, -2.0 * +A2 / dzm1h + A1 / dzp1h, +A2 / dzp1h, 0.0, 0.0);
-    if (neumann) R.set(k + 1, -A2 / dzm1h, -A1 / dzm1h, +A1 / dzm1h, +A2 / dzm1h, 0.0, 0.0, 0.0, bc);
-    else R.set(k + 1, 0.5 * A2, 0.5 * (A1 + 2.0 * A2), 0.5 * (A1 + 2.0 * A2), 0.5 * A2, 0.0, 0.0, 0.0, bc);
-    R.set(k + 2, -1.0, +1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0);
+    closure::cell_stencil_top4(R, dz, k, bc, neumann, cf.a1, cf.a2);
 }
-// Fold the three wall rows (pivots b(k), d(k-1), f(k-2)) out of rows k+1..k+3.
-__device__ inline void cell_reduce_bot4(const Rows& R, int k)
-{
-    double fac = R.a(k + 1) / R.b(k);
-    R.a(k + 1) -= R.b(k) * fac; R.b(k + 1) -= R.c(k) * fac; R.c(k + 1) -= R.d(k) * fac;
-    R.d(k + 1) -= R.e(k) * fac; R.e(k + 1) -= R.f(k) * fac; R.f(k + 1) -= R.g(k) * fac;
-    fac = R.b(k + 1) / R.d(k - 1);
-    R.b(k + 1) -= R.d(k - 1) * fac; R.c(k + 1) -= R.e(k - 1) * fac; R.d(k + 1) -= R.f(k - 1) * fac;
-    R.e(k + 1) -= R.g(k - 1) * fac; R.r(k + 1) -= R.r(k - 1) * fac;
-    fac = R.c(k + 1) / R.f(k - 2);
-    R.c(k + 1) -= R.f(k - 2) * fac; R.d(k + 1) -= R.g(k - 2) * fac;
-    fac = R.a(k + 2) / R.d(k - 1);
-    R.a(k + 2) -= R.d(k - 1) * fac; R.b(k + 2) -= R.e(k - 1) * fac; R.c(k + 2) -= R.f(k - 1) * fac;
-    R.d(k + 2) -= R.g(k - 1) * fac; R.r(k + 2) -= R.r(k - 1) * fac;
-    fac = R.b(k + 2) / R.f(k - 2);
-    R.b(k + 2) -= R.f(k - 2) * fac; R.c(k + 2) -= R.g(k - 2) * fac;
-    fac = R.a(k + 3) / R.f(k - 2);
-    R.a(k + 3) -= R.f(k - 2) * fac; R.b(k + 3) -= R.g(k - 2) * fac;
-}
-// Fold the wall rows (pivots f(k), d(k+1), b(k+2)) out of rows k-1..k-3.
-__device__ inline void cell_reduce_top4(const Rows& R, int k)
-{
-    double fac = R.g(k - 1) / R.f(k);
-    R.g(k - 1) -= R.f(k) * fac; R.f(k - 1) -= R.e(k) * fac; R.e(k - 1) -= R.d(k) * fac;
-    R.d(k - 1) -= R.c(k) * fac; R.c(k - 1) -= R.b(k) * fac; R.b(k - 1) -= R.a(k) * fac;
-    fac = R.f(k - 1) / R.d(k + 1);
-    R.f(k - 1) -= R.d(k + 1) * fac; R.e(k - 1) -= R.c(k + 1) * fac; R.d(k - 1) -= R.b(k + 1) * fac;
-    R.c(k - 1) -= R.a(k + 1) * fac; R.r(k - 1) -= R.r(k + 1) * fac;
-    fac = R.e(k - 1) / R.b(k + 2);
-    R.e(k - 1) -= R.b(k + 2) * fac; R.d(k - 1) -= R.a(k + 2) * fac;
-    fac = R.g(k - 2) / R.d(k + 1);
-    R.g(k - 2) -= R.d(k + 1) * fac; R.f(k - 2) -= R.c(k + 1) * fac; R.e(k - 2) -= R.b(k + 1) * fac;
-    R.d(k - 2) -= R.a(k + 1) * fac; R.r(k - 2) -= R.r(k + 1) * fac;
-    fac = R.f(k - 2) / R.b(k + 2);
-    R.f(k - 2) -= R.b(k + 2) * fac; R.e(k - 2) -= R.a(k + 2) * fac;
-    fac = R.g(k - 3) / R.b(k + 2);
-    R.g(k - 3) -= R.b(k + 2) * fac; R.f(k - 3) -= R.a(k + 2) * fac;
-}
-__device__ inline void cell_fill_bot4(const Rows& R, int k)
-{
-    R.x(k) = (R.g(k - 2) * R.x(k + 1)) / -R.f(k - 2);
-    R.x(k - 1) = (R.e(k - 1) * R.x(k) + R.f(k - 1) * R.x(k + 1) + R.g(k - 1) * R.x(k + 2) - R.r(k - 1)) / -R.d(k - 1);
-    R.x(k - 2) = (R.c(k) * R.x(k - 1) + R.d(k) * R.x(k) + R.e(k) * R.x(k + 1) + R.f(k) * R.x(k + 2)
-                  + R.g(k) * R.x(k + 3)) / -R.b(k);
-}
-__device__ inline void cell_fill_top4(const Rows& R, int k)
-{
-    R.x(k) = (R.a(k + 2) * R.x(k - 1)) / -R.b(k + 2);
-    R.x(k + 1) = (R.a(k + 1) * R.x(k - 2) + R.b(k + 1) * R.x(k - 1) + R.c(k + 1) * R.x(k) - R.r(k + 1)) / -R.d(k + 1);
-    R.x(k + 2) = (R.a(k) * R.x(k - 3) + R.b(k) * R.x(k - 2) + R.c(k) * R.x(k - 1) + R.d(k) * R.x(k)
-                  + R.e(k) * R.x(k + 1)) / -R.f(k);
-}
+__device__ inline void cell_reduce_bot4(const Rows& R, int k) { closure::cell_reduce_bot4(R, k); }
+__device__ inline void cell_reduce_top4(const Rows& R, int k) { closure::cell_reduce_top4(R, k); }
+__device__ inline void cell_fill_bot4(const Rows& R, int k) { closure::cell_fill_bot4(R, k); }
+__device__ inline void cell_fill_top4(const Rows& R, int k) { closure::cell_fill_top4(R, k); }
 
-// ---- face fields (w), second order: the wall face value is the unknown
-__device__ inline void face_stencil2(const Rows& R, int k, double bc) { R.a(k) = 0.0; R.b(k) = 1.0; R.c(k) = 0.0; R.r(k) = bc; }
-__device__ inline void face_reduce_bot2(const Rows& R, int k)
-{
-    const double fac = R.a(k + 1) / R.b(k);
-    R.a(k + 1) -= R.b(k) * fac;
-    R.r(k + 1) -= R.r(k) * fac;
-}
-__device__ inline void face_reduce_top2(const Rows& R, int k)
-{
-    const double fac = R.c(k - 1) / R.b(k);
-    R.c(k - 1) -= R.b(k) * fac;
-    R.r(k - 1) -= R.r(k) * fac;
-}
-__device__ inline void face_fill2(const Rows& R, int k) { R.x(k) = (-R.r(k)) / -R.b(k); }
-
-// ---- face fields (w), fourth order
+__device__ inline void face_stencil2(const Rows& R, int k, double bc) { closure::face_stencil2(R, k, bc); }
+__device__ inline void face_reduce_bot2(const Rows& R, int k) { closure::face_reduce_bot2(R, k); }
+__device__ inline void face_reduce_top2(const Rows& R, int k) { closure::face_reduce_top2(R, k); }
+__device__ inline void face_fill2(const Rows& R, int k) { closure::face_fill2(R, k); }
 __device__ inline void face_stencil_bot4(const Rows& R, const double* dz, int k, double bc, const Coef& cf)
 {
-    const double A1 = cf.a1, A2 = cf.a2, dzp0 = dz[k], dzp1 = dz[k + 1];
-    R.set(k, 0.0, -A2 / dzp0, -A1 / dzp0 + A2 / dzp1, +A1 / dzp0 + A1 / dzp1, +A2 / dzp0 - A1 / dzp1, -A2 / dzp1, 0.0,
-          0.0);
-    R.set(k - 1, 0.0, 0.0, 0.0, -1.0, +2.0, -1.0, 0.0, 0.0);
-    R.set(k - 2, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, bc);
+    closure::face_stencil_bot4(R, dz, k, bc, cf.a1, cf.a2);
 }
 __device__ inline void face_stencil_top4(const Rows& R, const double* dz, int k, double bc, const Coef& cf)
 {
-    const double A1 = cf.a1, A2 = cf.a2, dzp0 = dz[k], dzp1 = dz[k + 1];
-    R.set(k, 0.0, -A2 / dzp0, -A1 / dzp0 + A2 / dzp1, +A1 / dzp0 + A1 / dzp1, +A2 / dzp0 - A1 / dzp1, -A2 / dzp1, 0.0,
-          0.0);
-    R.set(k + 1, 0.0, -1.0, +2.0, -1.0, 0.0, 0.0, 0.0, 0.0);
-    R.set(k + 2, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, bc);
+    closure::face_stencil_top4(R, dz, k, bc, cf.a1, cf.a2);
 }
-__device__ inline void face_reduce_bot4(const Rows& R, int k)
-{
-    double fac = R.a(k + 1) / R.b(k);
-    R.a(k + 1) -= R.b(k) * fac; R.b(k + 1) -= R.c(k) * fac; R.c(k + 1) -= R.d(k) * fac;
-    R.d(k + 1) -= R.e(k) * fac; R.e(k + 1) -= R.f(k) * fac;
-    fac = R.b(k + 1) / R.d(k - 1);
-    R.b(k + 1) -= R.d(k - 1) * fac; R.c(k + 1) -= R.e(k - 1) * fac; R.d(k + 1) -= R.f(k - 1) * fac;
-    fac = R.c(k + 1) / R.f(k - 2);
-    R.c(k + 1) -= R.f(k - 2) * fac; R.r(k + 1) -= R.r(k - 2) * fac;
-    fac = R.a(k + 2) / R.d(k - 1);
-    R.a(k + 2) -= R.d(k - 1) * fac; R.b(k + 2) -= R.e(k - 1) * fac; R.c(k + 2) -= R.f(k - 1) * fac;
-    fac = R.b(k + 2) / R.f(k - 2);
-    R.b(k + 2) -= R.f(k - 2) * fac; R.r(k + 2) -= R.r(k - 2) * fac;
-    fac = R.a(k + 3) / R.f(k - 2);
-    R.a(k + 3) -= R.f(k - 2) * fac; R.r(k + 3) -= R.r(k - 2) * fac;
-}
-__device__ inline void face_reduce_top4(const Rows& R, int k)
-{
-    double fac = R.g(k - 1) / R.f(k);
-    R.g(k - 1) -= R.f(k) * fac; R.f(k - 1) -= R.e(k) * fac; R.e(k - 1) -= R.d(k) * fac;
-    R.d(k - 1) -= R.c(k) * fac; R.c(k - 1) -= R.b(k) * fac;
-    fac = R.f(k - 1) / R.d(k + 1);
-    R.f(k - 1) -= R.d(k + 1) * fac; R.e(k - 1) -= R.c(k + 1) * fac; R.d(k - 1) -= R.b(k + 1) * fac;
-    fac = R.e(k - 1) / R.b(k + 2);
-    R.e(k - 1) -= R.b(k + 2) * fac; R.r(k - 1) -= R.r(k + 2) * fac;
-    fac = R.g(k - 2) / R.d(k + 1);
-    R.g(k - 2) -= R.d(k + 1) * fac; R.f(k - 2) -= R.c(k + 1) * fac; R.e(k - 2) -= R.b(k + 1) * fac;
-    fac = R.f(k - 2) / R.b(k + 2);
-    R.f(k - 2) -= R.b(k + 2) * fac; R.r(k - 2) -= R.r(k + 2) * fac;
-    fac = R.g(k - 3) / R.b(k + 2);
-    R.g(k - 3) -= R.b(k + 2) * fac; R.r(k - 3) -= R.r(k + 2) * fac;
-}
-__device__ inline void face_fill_bot4(const Rows& R, int k)
-{
-    R.x(k) = (-R.r(k - 2)) / -R.f(k - 2);
-    R.x(k - 1) = (R.e(k - 1) * R.x(k) + R.f(k - 1) * R.x(k + 1)) / -R.d(k - 1);
-    R.x(k - 2) = (R.c(k) * R.x(k - 1) + R.d(k) * R.x(k) + R.e(k) * R.x(k + 1) + R.f(k) * R.x(k + 2)) / -R.b(k);
-}
-__device__ inline void face_fill_top4(const Rows& R, int k)
-{
-    R.x(k) = (-R.r(k + 2)) / -R.b(k + 2);
-    R.x(k + 1) = (R.b(k + 1) * R.x(k - 1) + R.c(k + 1) * R.x(k)) / -R.d(k + 1);
-    R.x(k + 2) = (R.b(k) * R.x(k - 2) + R.c(k) * R.x(k - 1) + R.d(k) * R.x(k) + R.e(k) * R.x(k + 1)) / -R.f(k);
-}
+__device__ inline void face_reduce_bot4(const Rows& R, int k) { closure::face_reduce_bot4(R, k); }
+__device__ inline void face_reduce_top4(const Rows& R, int k) { closure::face_reduce_top4(R, k); }
+__device__ inline void face_fill_bot4(const Rows& R, int k) { closure::face_fill_bot4(R, k); }
+__device__ inline void face_fill_top4(const Rows& R, int k) { closure::face_fill_top4(R, k); }
 
 // ============================================================ band rows and solve
 //
