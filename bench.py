@@ -48,6 +48,12 @@ WORKLOADS = {
     "config1": dict(name="chanfast4 256x256x192 Re_b=10000", order=4, nx=256, ny=256, nz=192,
                     lx=2 * math.pi, ly=math.pi, lz=2.0, dt=5e-4, nu=1.0 / 10000.0, prandtl=0.71,
                     seed=1, amp=0.1, c_amp=0.01, run_steps=200),
+    # the benchmark grid cut to a quarter of the planes, for profiling captures
+    # of the kernels whose parallelism follows the x-y size (the band solves:
+    # the same 66k column pairs as config2) in a quarter of the memory
+    "config2z96": dict(name="chanfast4 512x512x96 Re_b=20000", order=4, nx=512, ny=512, nz=96,
+                       lx=2 * math.pi, ly=math.pi, lz=2.0, dt=2.5e-4, nu=1.0 / 20000.0, prandtl=0.71,
+                       seed=2, amp=0.05, c_amp=0.01, run_steps=50),
     # the reference's own CPU-runnable case
     "config0": dict(name="chanfast2 64x64x64 Re_b=2800", order=2, nx=64, ny=64, nz=64,
                     lx=4 * math.pi, ly=4 * math.pi / 3, lz=2.0, dt=1e-3, nu=1.0 / 2800.0, prandtl=1.0,
