@@ -904,13 +904,18 @@ __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* 
         __syncthreads();
         const int k = t % Ns;
         const int step = N / (Ns * 8);
+        if (k) {
+            // Twiddles w^r, r = 1..7, of w = exp(-+2 pi i k step / N): three
+            // from the table (w, w^2, w^4), the rest as their products.
+            // Seven table reads per stage made the transforms bound by the
+            // load pipe, not by HBM; a product adds at most a few ulps.
+            double2 c1 = __ldg(&tw[tws * k * step]), c2 = __ldg(&tw[tws * 2 * k * step]);
+            double2 c4 = __ldg(&tw[tws * 4 * k * step]);
+            if (sign > 0) { c1.y = -c1.y; c2.y = -c2.y; c4.y = -c4.y; }
+            const double2 c3 = cmul(c1, c2);
+            const double2 cw[8] = {c1, c1, c2, c3, c4, cmul(c1, c4), cmul(c2, c4), cmul(c3, c4)};
 #pragma unroll
-        for (int r = 1; r < 8; r++) {
-            if (k) {
-                double2 c = __ldg(&tw[tws * r * k * step]);
-                if (sign > 0) c.y = -c.y;
-                w[r] = cmul(w[r], c);
-            }
+            for (int r = 1; r < 8; r++) w[r] = cmul(w[r], cw[r]);
         }
         bfly<8>(w, sign, c8);
         if (Ns * 8 == N) {
