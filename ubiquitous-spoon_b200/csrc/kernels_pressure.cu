@@ -227,10 +227,26 @@ __device__ __forceinline__ void fft_stage_s(double2* buf, const FftCtx& F)
             const int line = LM ? b / NR : b % FFT_L;
             const int j = LM ? b - line * NR : b / FFT_L;
             const int k = j % NS;
+            // twiddles w^r of w = exp(-+2 pi i k TSTEP / N): w, w^2 and w^4
+            // from the table, w^3, w^5, w^6, w^7 as products (fewer table
+            // reads; the transforms are bound by the load pipe)
+            double2 cw[8];
+            if (k > 0) {
+                const int m = k * TSTEP;
+                cw[1] = twid(F, m);
+                if constexpr (R > 2) cw[2] = twid(F, 2 * m);
+                if constexpr (R > 3) cw[3] = cmul(cw[1], cw[2]);
+                if constexpr (R > 4) cw[4] = twid(F, 4 * m);
+                if constexpr (R > 5) {
+                    cw[5] = cmul(cw[1], cw[4]);
+                    cw[6] = cmul(cw[2], cw[4]);
+                    cw[7] = cmul(cw[3], cw[4]);
+                }
+            }
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 double2 a = buf[sslot<N, LM>(j + r * NR, line)];
-                if (r > 0 && k > 0) a = cmul(a, twid(F, r * k * TSTEP));
+                if (r > 0 && k > 0) a = cmul(a, cw[r]);
                 v[t][r] = a;
             }
             dft_small<R>(v[t], F);
