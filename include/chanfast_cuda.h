@@ -36,7 +36,10 @@ enum {
     CF_ECUDA = -3,       /* a CUDA runtime call failed */
     CF_EPIVOT = -4,      /* zero pivot in a band factorisation */
     CF_ENONFINITE = -5,  /* the state went NaN or Inf (see cf_sync) */
-    CF_EIO = -6          /* restart / log file error (drivers) */
+    CF_EIO = -6,         /* restart / log file error (drivers) */
+    CF_ETIMEOUT = -7     /* a kernel gave up (after about a second) waiting for
+                            one of its own asynchronous copies; the substep's
+                            results are invalid (see cf_sync) */
 };
 
 enum { CF_U = 0, CF_V = 1, CF_W = 2, CF_C = 3, CF_P = 4 };
@@ -108,8 +111,9 @@ int cf_step_graph(cf_instance *inst, int nsteps);
  * Inf: a blown-up or NaN-seeded state is detected within one substep, and
  * within two for v, w and p, which feed u in the next substep.  The
  * reference has no such check (its check(), check.h:8-12, aborts only on
- * allocation, order and pivot failures).  The flag stays set until
- * cf_set_field or cf_init_fields loads new fields. */
+ * allocation, order and pivot failures).  Returns CF_ETIMEOUT once a
+ * kernel has given up waiting for one of its own asynchronous copies.  The
+ * flags stay set until cf_set_field or cf_init_fields loads new fields. */
 int cf_sync(cf_instance *inst);
 
 /* Per-substep log rows (10 doubles each): mdpdx, nu du/dz bottom, top, bulk
@@ -164,6 +168,8 @@ int cf_device_field(cf_instance *inst, int field, double **dev_ptr, long long *n
  *   solves, 2 back substitution of u, v, c and w (one launch), 3 mass-flux
  *   control u, 4 scalar-mean control c, 5 divergence + x FFT, 6 y FFT,
  *   7 Poisson, 8 inverse y FFT, 9 inverse x FFT, 10 projection.
+ * With power-of-two ny the y transforms run inside the Poisson launch
+ * (k_poisson_fft): groups 6 and 8 are then empty and 7 holds all three.
  * Synchronises after every substep (timing only). */
 #define CF_NKERNEL_GROUPS 11
 int cf_profile(cf_instance *inst, int nsub, double *ms);

@@ -1,0 +1,106 @@
+"""The y transforms fused with the Poisson solve (k_poisson_fft, one block per
+kx, used for ny = 512) against the three separate launches (k_ffty_p2,
+k_poisson, k_ffty_p2) that CF_FUSE_PRESSURE=0 selects at creation.
+
+Both run the same elimination code (PairRows, HeptSweep) and the same
+radix-8 transform (fft_p2_line), the fused one with its twiddles read from a
+per-stage table instead of formed as products, and both kernels are compiled
+with FMA contraction, which may pair a few multiply-adds differently; so the
+states agree to rounding, not bit for bit (measured at most 1.3e-14 on u,
+v, w, c and 4.5e-12 on p): relative L2 <= 1e-13 on u, v, w, c and <= 1e-10
+on p, the engine's bars against the reference, after 3 eager
+substeps and two graph-replayed RK3 steps.  The grids reach every path of
+the kernel: the ninth warp, whose one thread solves the ky = ny/2 pair; a
+last row group shorter than the 4-row groups; the smallest nz of each
+order; orders 2 and 4 (order 4 with its back-sweep inputs in shared
+memory); and non-power-of-two nx.  Other ny keep the separate launches.  A
+batch mixing fused and separate members gives each member the result it
+has alone."""
+import os
+
+import numpy as np
+import pytest
+
+import chanfast_np as cn
+
+pytestmark = pytest.mark.gpu
+
+# order, nx, ny, nz
+CASES = [(4, 32, 512, 22), (2, 16, 512, 9), (4, 64, 512, 37), (4, 48, 512, 20), (2, 32, 512, 4),
+         (4, 16, 512, 6), (2, 24, 512, 14)]
+
+
+def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0):
+    prm = cn.Params(order=order, nx=nx, ny=ny, nz=nz, lx=4 * np.pi, ly=4 * np.pi / 3, lz=2.0, dt=1e-3,
+                    nu=1.0 / re, prandtl=0.71)
+    os.environ["CF_FUSE_PRESSURE"] = "1" if fused else "0"
+    try:
+        inst = cf.Instance(cf.Config.from_params(prm))
+    finally:
+        os.environ.pop("CF_FUSE_PRESSURE", None)
+    inst.init_fields(seed, 0.1, 0.01)
+    return inst
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def compare(a, b, what):
+    err = {nm: rel(a.get_field(nm), b.get_field(nm)) for nm in "uvwcp"}
+    same = all(np.array_equal(a.get_field(nm), b.get_field(nm)) for nm in "uvwcp")
+    print(what, "bitwise" if same else {k: "%.1e" % v for k, v in err.items()})
+    assert all(err[nm] <= 1e-13 for nm in "uvwc"), (what, err)
+    assert err["p"] <= 1e-10, (what, err)
+    la, lb = a.log(), b.log()
+    assert la.shape == lb.shape
+    assert np.all(np.abs(la - lb) <= 1e-9 * np.maximum(np.abs(lb).max(axis=0), 1e-3)), what
+
+
+@pytest.mark.parametrize("order,nx,ny,nz", CASES)
+def test_fused_equals_separate(cf, gpu, order, nx, ny, nz):
+    fused = make(cf, order, nx, ny, nz, True)
+    sep = make(cf, order, nx, ny, nz, False)
+    assert fused.launches_per_substep() == sep.launches_per_substep() - 2
+    fused.step(3)
+    sep.step(3)
+    compare(fused, sep, f"o{order} {nx}x{ny}x{nz} 3 substeps")
+    fused.step_graph(2)
+    sep.step_graph(2)
+    compare(fused, sep, f"o{order} {nx}x{ny}x{nz} +2 steps")
+    fused.sync()
+    assert fused.max_divergence() < 1e-12
+    fused.close()
+    sep.close()
+
+
+@pytest.mark.parametrize("ny", [64, 256])
+def test_other_sizes_keep_separate_launches(cf, gpu, ny):
+    a = make(cf, 4, 32, ny, 16, True)
+    b = make(cf, 4, 32, ny, 16, False)
+    assert a.launches_per_substep() == b.launches_per_substep()
+    a.close()
+    b.close()
+
+
+def test_batch_mixing_fused_and_separate(cf, gpu):
+    """Members that fuse (power-of-two ny) and members that cannot (ny = 48)
+    or chose not to share one batch; each ends where it ends alone."""
+    # order, nx, ny, nz, fused, seed (members 0 and 3: one state, both paths)
+    spec = [(4, 32, 512, 24, True, 20), (2, 64, 48, 20, True, 21), (2, 16, 512, 10, True, 22),
+            (4, 32, 512, 24, False, 20), (2, 32, 128, 16, True, 24)]
+    mixed = [make(cf, *m[:4], fused=m[4], seed=m[5]) for m in spec]
+    alone = [make(cf, *m[:4], fused=m[4], seed=m[5]) for m in spec]
+    cf.batch_step(mixed, 5)
+    for inst in alone:
+        cf.batch_step([inst], 5)
+    for a, b in zip(alone, mixed):
+        a.sync()
+        b.sync()
+        for nm in "uvwcp":
+            assert np.array_equal(a.get_field(nm), b.get_field(nm)), nm
+        assert np.array_equal(a.log(), b.log())
+    # the fused and the separate member of the same configuration agree
+    compare(mixed[0], mixed[3], "batch o4 32x512x24 fused vs separate")
+    for inst in mixed + alone:
+        inst.close()

@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_CUDA = os.path.join(HERE, "libchanfast_cuda.so")
 LIB_DRIVER = os.path.join(HERE, "libchanfast.so")
 
-CF_OK, CF_EINVAL, CF_ENOMEM, CF_ECUDA, CF_EPIVOT, CF_ENONFINITE, CF_EIO = 0, -1, -2, -3, -4, -5, -6
+CF_OK, CF_EINVAL, CF_ENOMEM, CF_ECUDA, CF_EPIVOT, CF_ENONFINITE, CF_EIO, CF_ETIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7
 FIELDS = {"u": 0, "v": 1, "w": 2, "c": 3, "p": 4}
 LAYOUT_PADDED, LAYOUT_INTERIOR = 0, 1
 LOG_COLS = 10

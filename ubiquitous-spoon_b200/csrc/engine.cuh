@@ -207,6 +207,17 @@ constexpr int POIS_PF = 8;         // forward rows in flight per thread (both co
 constexpr int POIS_PB = 2;         // back-substitution rows loaded ahead (registers)
 inline size_t pois_smem_bytes(int threads) { return (size_t) POIS_PF * 2 * threads * 16; }
 
+// k_poisson_fft: forward y transform + Poisson solve (with the wall ghost
+// rows) + inverse y transform, one block per kx, for power-of-two ny
+struct PoissonFftArgs {
+    PoissonArgs P;
+    const double2* twy;   // exp(-2 pi i m / ny)
+    double c8;            // cos(pi/4) from the host table
+    double* fault;        // set to 1 when a wait for a row copy gave up
+};
+bool poisson_fft_supported(const Geo& G);
+void launch_poisson_fft(const Geo& G, const PoissonFftArgs& A, cudaStream_t st);
+
 struct ProjArgs {
     double *u, *v, *w, *c;
     const double* p;
@@ -267,6 +278,8 @@ int fft_kernel_key(int n);                          // n with its own transform 
 size_t fft_generic_smem(int n, bool line_major);    // shared memory of the non-power-of-two transforms
 void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st);   // ny: power of two, else generic
 void launch_poisson_batch(const BatchLaunch& L, int order, cudaStream_t st);
+// key: 8 * ny + order
+void launch_poisson_fft_batch(const BatchLaunch& L, int key, cudaStream_t st);
 void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st);    // nx: power of two, else generic
 void launch_project_batch(const BatchLaunch& L, int order, cudaStream_t st);
 cudaError_t rhs_set_smem_limits();

@@ -414,6 +414,9 @@ struct cf_instance {
     cf_config cfg;
     Metrics m;
     Geo geo;
+    // y transforms fused with the Poisson solve where ny is a power of two;
+    // CF_FUSE_PRESSURE=0 at creation selects the three separate launches
+    bool fuse_pressure = true;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -426,7 +429,7 @@ struct cf_instance {
     double* partial_c = nullptr;   // and of the c solve
     double* avg = nullptr;
     double* avg_c = nullptr;        // channel scheme: xy-average of c (avg holds u's)
-    double* dscal = nullptr;        // [0] mdpdx, [1] dcdt, [2] non-finite flag
+    double* dscal = nullptr;        // [0] mdpdx, [1] dcdt, [2] non-finite flag, [3] copy-wait fault flag
     long long* dcount = nullptr;    // device substep counter (log row)
     double* dlog = nullptr;
     int log_cap = 0;
@@ -659,6 +662,9 @@ struct Sink {
     virtual void div_fftx(const Geo& G, const DivArgs& A) { launch_div_fftx(G, A, st); }
     virtual void ffty(const Geo& G, const FftyArgs& A, int nrows) { launch_ffty(G, A, nrows, st); }
     virtual void poisson(const Geo& G, const PoissonArgs& A) { launch_poisson(G, A, st); }
+    // the y transforms fused with the Poisson solve (power-of-two ny)
+    virtual bool fused_pressure(const Geo& G) const { return poisson_fft_supported(G); }
+    virtual void poisson_fft(const Geo& G, const PoissonFftArgs& A) { launch_poisson_fft(G, A, st); }
     virtual void c2r(const Geo& G, const C2rArgs& A, int nrows) { launch_fftx_c2r(G, A, nrows, st); }
     virtual void project(const Geo& G, const ProjArgs& A) { launch_project(G, A, st); }
 };
@@ -676,14 +682,23 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
               I->spec, I->px, I->c8, I->p};
     K.div_fftx(G, D);
     K.mark();
-    FftyArgs Y{I->spec, I->py, -1, GZ, I->c8};
-    K.ffty(G, Y, G.nz);
-    K.mark();
-    K.poisson(G, poisson_args(I, po, pdt));
-    K.mark();
-    FftyArgs Yb{I->spec, I->py, +1, 0, I->c8};
-    K.ffty(G, Yb, G.n2);
-    K.mark();
+    if (I->fuse_pressure && K.fused_pressure(G)) {
+        // one launch; its time is the Poisson group's, the y-transform groups stay empty
+        K.mark();
+        PoissonFftArgs F{poisson_args(I, po, pdt), I->py.tw, I->c8, I->dscal + 3};
+        K.poisson_fft(G, F);
+        K.mark();
+        K.mark();
+    } else {
+        FftyArgs Y{I->spec, I->py, -1, GZ, I->c8};
+        K.ffty(G, Y, G.nz);
+        K.mark();
+        K.poisson(G, poisson_args(I, po, pdt));
+        K.mark();
+        FftyArgs Yb{I->spec, I->py, +1, 0, I->c8};
+        K.ffty(G, Yb, G.n2);
+        K.mark();
+    }
     C2rArgs X{I->spec, {I->p, nullptr, nullptr, nullptr}, I->px, I->c8, 0, 0};
     K.c2r(G, X, G.n2);
     K.mark();
@@ -888,7 +903,10 @@ void enqueue_substep(cf_instance* I, Timeline* tl = nullptr)
 // transforms), lays them out in one device block with each record's first
 // flat block, and turns every group into one batched launch (batch.cuh).
 
-enum StageKind { ST_GHOSTS, ST_RHS, ST_BACK4, ST_MASS, ST_DIV, ST_FFTY, ST_POISSON, ST_C2R, ST_PROJECT };
+// ST_PSOLVE: y transforms and Poisson solve, per member either the three
+// separate launches or the fused one (the member's own choice, so that a
+// member's result does not depend on its neighbours in a batch)
+enum StageKind { ST_GHOSTS, ST_RHS, ST_BACK4, ST_MASS, ST_DIV, ST_PSOLVE, ST_C2R, ST_PROJECT };
 
 struct BatchStage {
     int kind = -1;
@@ -900,8 +918,10 @@ struct BatchStage {
     std::vector<BatchRec<DivArgs>> div;        // power-of-two nx: the divergence ...
     std::vector<BatchRec<R2cArgs>> r2c;        // ... then its x transform
     std::vector<BatchRec<DivArgs>> div_fftx;   // other nx: both in one kernel
-    std::vector<BatchRec<FftyArgs>> ffty;
-    std::vector<BatchRec<PoissonArgs>> poisson;
+    std::vector<BatchRec<FftyArgs>> ffty;       // forward y transforms ...
+    std::vector<BatchRec<PoissonArgs>> poisson; // ... Poisson solves ...
+    std::vector<BatchRec<FftyArgs>> ffty_bwd;   // ... inverse y transforms
+    std::vector<BatchRec<PoissonFftArgs>> pfft; // fused members
     std::vector<BatchRec<C2rArgs>> c2r;
     std::vector<BatchRec<ProjArgs>> project;
 };
@@ -923,6 +943,8 @@ struct BatchSink : Sink {
     std::vector<BatchStage> stages;
     size_t cursor = 0;
     bool mismatch = false;
+    bool fuse = false;   // members may take the fused y-transform + Poisson launch
+    size_t psolve = 0;   // the open ST_PSOLVE stage of a member's separate launches
     BatchStage& next(int kind)
     {
         if (cursor == stages.size()) {
@@ -960,13 +982,26 @@ struct BatchSink : Sink {
             S.div_fftx.push_back(batch_rec(G, A, grid_div_fftx(G)));
         }
     }
+    // forward y transform (opens the member's ST_PSOLVE stage), Poisson,
+    // inverse y transform
     void ffty(const Geo& G, const FftyArgs& A, int nrows) override
     {
-        next(ST_FFTY).ffty.push_back(batch_rec(G, A, grid_ffty(G, nrows, 1)));
+        if (A.sign < 0) {
+            next(ST_PSOLVE);
+            psolve = cursor - 1;
+            stages[psolve].ffty.push_back(batch_rec(G, A, grid_ffty(G, nrows, 1)));
+        } else {
+            stages[psolve].ffty_bwd.push_back(batch_rec(G, A, grid_ffty(G, nrows, 1)));
+        }
     }
     void poisson(const Geo& G, const PoissonArgs& A) override
     {
-        next(ST_POISSON).poisson.push_back(batch_rec(G, A, grid_poisson(G)));
+        stages[psolve].poisson.push_back(batch_rec(G, A, grid_poisson(G)));
+    }
+    bool fused_pressure(const Geo& G) const override { return fuse && poisson_fft_supported(G); }
+    void poisson_fft(const Geo& G, const PoissonFftArgs& A) override
+    {
+        next(ST_PSOLVE).pfft.push_back(batch_rec(G, A, dim3(G.nkx)));
     }
     void c2r(const Geo& G, const C2rArgs& A, int nrows) override
     {
@@ -979,7 +1014,7 @@ struct BatchSink : Sink {
 };
 
 enum BatchKernel { BK_GHOSTS, BK_RHS, BK_BACK4, BK_ROWAVG, BK_CONTROL, BK_DIV, BK_R2C, BK_DIV_FFTX, BK_FFTY,
-                   BK_POISSON, BK_C2R, BK_PROJECT };
+                   BK_POISSON, BK_PFFT, BK_C2R, BK_PROJECT };
 
 struct BatchOp {
     int kernel;
@@ -1065,8 +1100,12 @@ void compile(const BatchSink& K, BatchProgram& P)
             add_groups(P, BK_DIV_FFTX, S.div_fftx, [](const auto& r) { return 1024 * fft_kernel_key(r.G.nx) + r.G.order; },
                        smem_nx);
             break;
-        case ST_FFTY: add_groups(P, BK_FFTY, S.ffty, keyny, smem_ny); break;
-        case ST_POISSON: add_groups(P, BK_POISSON, S.poisson, order, none, poisson_block(S.poisson)); break;
+        case ST_PSOLVE:
+            add_groups(P, BK_FFTY, S.ffty, keyny, smem_ny);
+            add_groups(P, BK_POISSON, S.poisson, order, none, poisson_block(S.poisson));
+            add_groups(P, BK_FFTY, S.ffty_bwd, keyny, smem_ny);
+            add_groups(P, BK_PFFT, S.pfft, [](const auto& r) { return 8 * r.G.ny + r.G.order; }, none);
+            break;
         case ST_C2R: add_groups(P, BK_C2R, S.c2r, keynx, smem_nx); break;
         default: add_groups(P, BK_PROJECT, S.project, order, none, project_block(S.project)); break;
         }
@@ -1097,6 +1136,7 @@ void run_program(const BatchProgram& P, cudaStream_t st)
         case BK_DIV_FFTX: launch_div_fftx_batch(L, op.key % 1024, op.key / 1024, st); break;
         case BK_FFTY: launch_ffty_batch(L, op.key, st); break;
         case BK_POISSON: launch_poisson_batch(L, op.key, st); break;
+        case BK_PFFT: launch_poisson_fft_batch(L, op.key, st); break;
         case BK_C2R: launch_c2r_batch(L, op.key, st); break;
         default: launch_project_batch(L, op.key, st); break;
         }
@@ -1137,6 +1177,7 @@ int record_sink(const std::vector<cf_instance*>& v, int nsub, const LaunchShape&
 int record(const std::vector<cf_instance*>& v, int nsub, BatchProgram& P, const LaunchShape& shape)
 {
     BatchSink K;
+    K.fuse = true;
     const int rc = record_sink(v, nsub, shape, K);
     if (rc) return rc;
     compile(K, P);
@@ -1369,6 +1410,7 @@ struct CaptureSink : Sink {
     void div_fftx(const Geo&, const DivArgs&) override {}
     void ffty(const Geo&, const FftyArgs&, int) override {}
     void poisson(const Geo& g, const PoissonArgs& A) override { G = g; pois_args = A; has_pois = true; }
+    bool fused_pressure(const Geo&) const override { return false; }   // capture the separate solve
     void c2r(const Geo&, const C2rArgs&, int) override {}
     void project(const Geo& g, const ProjArgs& A) override { G = g; proj_args = A; has_proj = true; }
 };
@@ -1484,7 +1526,7 @@ int tune_batch(const std::vector<cf_instance*>& v, cudaStream_t st, LaunchShape&
     std::vector<BatchRec<ProjArgs>> proj;
     for (const BatchStage& S : K.stages) {
         if (S.kind == ST_BACK4) back4 = S.back4;
-        if (S.kind == ST_POISSON) pois = S.poisson;
+        if (S.kind == ST_PSOLVE) pois = S.poisson;
         if (S.kind == ST_PROJECT) proj = S.project;
     }
     if (back4.size() != v.size() || pois.size() != v.size() || proj.size() != v.size()) return CF_OK;
@@ -1572,6 +1614,7 @@ const char* cf_strerror(int status)
     case CF_EPIVOT: return "zero pivot in a band factorisation";
     case CF_ENONFINITE: return "non-finite value";
     case CF_EIO: return "file I/O error";
+    case CF_ETIMEOUT: return "a device wait for an asynchronous copy gave up";
     default: return "unknown status";
     }
 }
@@ -1696,6 +1739,8 @@ int cf_create(const cf_config* cfg, void* stream, cf_instance** out)
     if (rc) return rc;
     cf_instance* I = new (std::nothrow) cf_instance();
     if (!I) return CF_ENOMEM;
+    const char* fp = std::getenv("CF_FUSE_PRESSURE");
+    I->fuse_pressure = !(fp && fp[0] == '0');
     rc = create_impl(cfg, stream, I);
     if (rc) {
         cf_destroy(I);
@@ -1755,7 +1800,7 @@ int cf_set_field(cf_instance* I, int field, const double* host, int layout)
     dim3 blk(32, 8), grd((K + 31) / 32, (I->geo.ny + 31) / 32, I->geo.nx);
     k_host2dev<<<grd, blk, 0, I->stream>>>(I->geo, I->staging, field_ptr(I, field), B, K, ox, oy, oz);
     CF_CUDA(cudaGetLastError());
-    CF_CUDA(cudaMemsetAsync(I->dscal + 2, 0, sizeof(double), I->stream));
+    CF_CUDA(cudaMemsetAsync(I->dscal + 2, 0, 2 * sizeof(double), I->stream));
     CF_CUDA(cudaStreamSynchronize(I->stream));
     return CF_OK;
 }
@@ -1783,7 +1828,7 @@ int cf_init_fields(cf_instance* I, unsigned long long seed, double amp, double c
     dim3 blk(128), grd((G.ny + 127) / 128, G.nx, G.n2);
     k_init_raw<<<grd, blk, 0, I->stream>>>(G, I->u, I->v, I->w, I->c, I->zp, seed, amp, c_amp);
     CF_CUDA(cudaGetLastError());
-    CF_CUDA(cudaMemsetAsync(I->dscal + 2, 0, sizeof(double), I->stream));
+    CF_CUDA(cudaMemsetAsync(I->dscal + 2, 0, 2 * sizeof(double), I->stream));
     pressure_sequence(I, I->pois_init, 1.0, 0, false);
     CF_CUDA(cudaGetLastError());
     CF_CUDA(cudaStreamSynchronize(I->stream));
@@ -1829,13 +1874,15 @@ int cf_step_graph(cf_instance* I, int nsteps)
 }
 
 // CF_ENONFINITE once a mass-control kernel has found a NaN / Inf bulk mean
-// of u or c (the caller has synchronised the instance's stream).  The flag
-// is cleared when fields are set again.
+// of u or c, CF_ETIMEOUT once a kernel gave up waiting for one of its own
+// asynchronous copies (the caller has synchronised the instance's stream).
+// Both flags are cleared when fields are set again.
 static int finite_status(cf_instance* I)
 {
-    double flag = 0.0;
-    CF_CUDA(cudaMemcpy(&flag, I->dscal + 2, sizeof(double), cudaMemcpyDeviceToHost));
-    return flag != 0.0 ? CF_ENONFINITE : CF_OK;
+    double flag[2] = {0.0, 0.0};
+    CF_CUDA(cudaMemcpy(flag, I->dscal + 2, sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag[1] != 0.0) return CF_ETIMEOUT;
+    return flag[0] != 0.0 ? CF_ENONFINITE : CF_OK;
 }
 
 int cf_sync(cf_instance* I)
@@ -2328,8 +2375,10 @@ int cf_launches_per_substep(const cf_instance* I)
     // four back substitutions, 2 x (row average + mass control).  channel
     // (power-of-two nx only): ghosts, rhs + Helmholtz right-hand sides, fftx,
     // ffty, four spectral solves, ffty, fftx_c2r, apply_bc, 2 x mass control.
+    // With power-of-two ny the y transforms and the Poisson solve are one
+    // launch (two fewer).
     if (!I) return CF_EINVAL;
-    const int pressure = fftx_batched_supported(I->cfg.nx) ? 7 : 6;
+    const int pressure = (fftx_batched_supported(I->cfg.nx) ? 7 : 6) - (I->fuse_pressure && poisson_fft_supported(I->geo) ? 2 : 0);
     return (I->cfg.scheme == CF_SCHEME_CHANNEL ? 13 : 7) + pressure;
 }
 

@@ -17,6 +17,7 @@
 // FFTs run in shared memory: a Stockham autosort mixed-radix (2/3/4/5/8)
 // transform over L lines of one thread block, twiddles from a host table.
 #include <algorithm>
+#include <type_traits>
 
 #include "engine.cuh"
 #include "host_band.h"
@@ -533,6 +534,97 @@ __device__ void average_walls(const PoissonArgs& A, int n2)
     if (ORDER == 4) { avg[kt + 1] = g2; avg[kt + 2] = g3; }
 }
 
+// Band rows of one (kx, +-ky) column pair: the interior stencil rows with the
+// pair's diagonal, and the closure-reduced rows 0..2 and n-3..n-1 (var 1 is
+// the (0, 0) mode's closure, pressure.c:331-338).
+struct PairRows {
+    const PoissonArgs& A;
+    double lamx, lamy;
+    int var, n;
+    __device__ __forceinline__ int bq(int i) const { return i < 3 ? i : (i >= n - 3 ? 6 - (n - i) : -1); }
+    // Coefficients of interior row i from its staged table values
+    // st = (a, b, c, e, f, g, dpart, cx, cy) of row k = GZ + i.
+    __device__ __forceinline__ void coef_from(int i, const double* st, double* cf) const
+    {
+        const int q = bq(i);
+        double d = (st[6] - lamx * st[7]) - lamy * st[8];   // cx = dv dt / dx^2, cy = dv dt / dy^2
+        if (q >= 0) {
+            d = ((d - A.dsub[var][q][0]) - A.dsub[var][q][1]) - A.dsub[var][q][2];
+            for (int t = 0; t < 7; t++) cf[t] = A.red[var][q][t];
+        } else {
+            cf[0] = st[0]; cf[1] = st[1]; cf[2] = st[2];
+            cf[4] = st[3]; cf[5] = st[4]; cf[6] = st[5];
+        }
+        cf[3] = d;
+    }
+    // Table value f of row k: a, b, c, e, f, g, dpart, cx, cy, dvol.
+    __device__ __forceinline__ double table(int f, int k) const
+    {
+        switch (f) {
+        case 0: return A.a[k];
+        case 1: return A.b[k];
+        case 2: return A.c[k];
+        case 3: return A.e[k];
+        case 4: return A.f[k];
+        case 5: return A.g[k];
+        case 6: return A.dpart[k];
+        case 7: return A.cx[k];
+        case 8: return A.cy[k];
+        default: return A.dvol[k];
+        }
+    }
+    // Coefficients of interior row i (k = GZ + i).
+    __device__ __forceinline__ void coef(int i, double* cf) const
+    {
+        const int k = GZ + i;
+        double st[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, A.dpart[k], A.cx[k], A.cy[k]};
+        if (bq(i) < 0) {   // closure rows take their band from red
+            st[0] = A.a[k]; st[1] = A.b[k]; st[2] = A.c[k];
+            st[3] = A.e[k]; st[4] = A.f[k]; st[5] = A.g[k];
+        }
+        coef_from(i, st, cf);
+    }
+};
+
+// heptdag.c:5-61 for two complex right-hand sides sharing one factorisation,
+// one row per step().  One elimination formula serves every row: with zero
+// history (p, q, r, s of rows -3..-1) it reduces exactly to the special forms
+// of rows 0..2.
+struct HeptSweep {
+    double p3 = 0, q3 = 0, r3 = 0, p2 = 0, q2 = 0, r2 = 0, p1 = 0, q1 = 0, r1 = 0;   // rows i-3, i-2, i-1
+    double2 s3A = {0, 0}, s2A = {0, 0}, s1A = {0, 0}, s3B = {0, 0}, s2B = {0, 0}, s1B = {0, 0};
+    // cf: the row's band (a b c d e f g); hA, hB: right-hand sides already
+    // scaled by the cell volume.  Out: the row's multipliers p, q, r and the
+    // forward-substituted values.
+    __device__ __forceinline__ void step(const double* cf, double2 hA, double2 hB, double& p, double& q, double& r,
+                                         double2& svA, double2& svB)
+    {
+        const double a = cf[0], b = cf[1], c = cf[2], d = cf[3], e = cf[4], f = cf[5], g = cf[6];
+        const double alp = b - a * p3;
+        const double bet = c - a * q3 - alp * p2;
+        const double den = d - a * r3 - alp * q2 - bet * p1;
+        const double iden = 1.0 / den;
+        p = (e - alp * r2 - bet * q1) * iden;
+        q = (f - bet * r1) * iden;
+        r = g * iden;
+        svA = make_double2((hA.x - a * s3A.x - alp * s2A.x - bet * s1A.x) * iden,
+                           (hA.y - a * s3A.y - alp * s2A.y - bet * s1A.y) * iden);
+        svB = make_double2((hB.x - a * s3B.x - alp * s2B.x - bet * s1B.x) * iden,
+                           (hB.y - a * s3B.y - alp * s2B.y - bet * s1B.y) * iden);
+        p3 = p2; q3 = q2; r3 = r2; p2 = p1; q2 = q1; r2 = r1; p1 = p; q1 = q; r1 = r;
+        s3A = s2A; s2A = s1A; s1A = svA;
+        s3B = s2B; s2B = s1B; s1B = svB;
+    }
+};
+
+// Back substitution of one heptdag row (heptdag.c:50-55); the previous row's
+// x1 enters last: one dependent operation per row.
+__device__ __forceinline__ double2 hept_back(double2 sv, double p, double q, double r, double2 x1, double2 x2,
+                                             double2 x3)
+{
+    return make_double2(((sv.x - r * x3.x) - q * x2.x) - p * x1.x, ((sv.y - r * x3.y) - q * x2.y) - p * x1.y);
+}
+
 // Banded solve of a pair of (kx, ky) columns over spectrum rows
 // GZ .. GZ+n-1: pressure_poisson{2,4} (pressure.c:293-443) with FILL (the
 // wall ghost rows of the solution are filled from the closure, as p needs
@@ -561,23 +653,9 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
     double2* sp = A.spec;
     auto SA = [&](int k) -> double2& { return sp[(long long) k * ncol + colA]; };
     auto SB = [&](int k) -> double2& { return sp[(long long) k * ncol + colB]; };
-    auto bq = [&](int i) { return i < 3 ? i : (i >= n - 3 ? 6 - (n - i) : -1); };
     auto scal = [](double2 v, double f) { return make_double2(v.x * f, v.y * f); };
-
-    // Coefficients of interior row i (k = GZ + i) for this pair.
-    auto coef = [&](int i, double* cf) {
-        const int k = GZ + i;
-        const int q = bq(i);
-        double d = (A.dpart[k] - lamx * A.cx[k]) - lamy * A.cy[k];   // cx = dv dt / dx^2, cy = dv dt / dy^2
-        if (q >= 0) {
-            d = ((d - A.dsub[var][q][0]) - A.dsub[var][q][1]) - A.dsub[var][q][2];
-            for (int t = 0; t < 7; t++) cf[t] = A.red[var][q][t];
-        } else {
-            cf[0] = A.a[k]; cf[1] = A.b[k]; cf[2] = A.c[k];
-            cf[4] = A.e[k]; cf[5] = A.f[k]; cf[6] = A.g[k];
-        }
-        cf[3] = d;
-    };
+    const PairRows rows{A, lamx, lamy, var, n};
+    auto coef = [&](int i, double* cf) { rows.coef(i, cf); };
     auto at = [&](double* base, int k) -> double& { return base[(long long) k * npair + pair]; };
 
     if (ORDER == 2) {
@@ -650,10 +728,8 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
         return;
     }
 
-    // heptdag.c:5-61 with per-pair pivots; p, q, r spill to scratch.  One
-    // elimination formula serves every row: with zero history (p, q, r, s of
-    // rows -3..-1) it reduces exactly to the special forms of rows 0..2.
-    // In the forward sweep each thread keeps the spectrum values of the next
+    // heptdag.c:5-61 with per-pair pivots (HeptSweep); p, q, r spill to
+    // scratch.  In the forward sweep each thread keeps the spectrum values of the next
     // POIS_PF rows of both columns in flight as cp.async copies into its own
     // slots of a shared-memory ring; none of those rows has been rewritten yet.
     double* Pp = A.scratch;
@@ -671,8 +747,7 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
         cp_async_commit_ordered();
     };
     for (int i = 0; i < POIS_PF; i++) ffetch(i);
-    double p3 = 0, q3 = 0, r3 = 0, p2 = 0, q2 = 0, r2 = 0, p1 = 0, q1 = 0, r1 = 0;   // rows i-3, i-2, i-1
-    double2 s3A = make_double2(0, 0), s2A = s3A, s1A = s3A, s3B = s3A, s2B = s3A, s1B = s3A;
+    HeptSweep H;
     double cf[7];
     for (int i = 0; i < n; i++) {
         const int k = GZ + i;
@@ -680,27 +755,15 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
         double2 hA = *fslot(i, 0), hB = *fslot(i, 1);
         ffetch(i + POIS_PF);
         coef(i, cf);
-        const double a = cf[0], b = cf[1], c = cf[2], d = cf[3], e = cf[4], f = cf[5], g = cf[6];
         const double dv = A.dvol[k];
         hA = scal(hA, dv);
         hB = scal(hB, dv);
-        const double alp = b - a * p3;
-        const double bet = c - a * q3 - alp * p2;
-        const double den = d - a * r3 - alp * q2 - bet * p1;
-        const double iden = 1.0 / den;
-        const double p = (e - alp * r2 - bet * q1) * iden;
-        const double q = (f - bet * r1) * iden;
-        const double r = g * iden;
-        const double2 svA = make_double2((hA.x - a * s3A.x - alp * s2A.x - bet * s1A.x) * iden,
-                                         (hA.y - a * s3A.y - alp * s2A.y - bet * s1A.y) * iden);
-        const double2 svB = make_double2((hB.x - a * s3B.x - alp * s2B.x - bet * s1B.x) * iden,
-                                         (hB.y - a * s3B.y - alp * s2B.y - bet * s1B.y) * iden);
+        double p, q, r;
+        double2 svA, svB;
+        H.step(cf, hA, hB, p, q, r, svA, svB);
         at(Pp, k) = p; at(Qp, k) = q; at(Rp, k) = r;
         SA(k) = svA;
         SB(k) = svB;
-        p3 = p2; q3 = q2; r3 = r2; p2 = p1; q2 = q1; r2 = r1; p1 = p; q1 = q; r1 = r;
-        s3A = s2A; s2A = s1A; s1A = svA;
-        s3B = s2B; s2B = s1B; s1B = svB;
     }
     cp_async_wait_ordered<0>();
 
@@ -728,11 +791,8 @@ __device__ __forceinline__ void band_column(const Geo& G, const PoissonArgs& A, 
                 const double2 svA = lsA[u], svB = lsB[u];
                 const double p = lp[u], q = lq[u], r = lr[u];
                 bload(i - POIS_PB, u);
-                // the previous row's x1 enters last: one dependent operation per row
-                const double2 xA = make_double2(((svA.x - r * x3A.x) - q * x2A.x) - p * x1A.x,
-                                                ((svA.y - r * x3A.y) - q * x2A.y) - p * x1A.y);
-                const double2 xB = make_double2(((svB.x - r * x3B.x) - q * x2B.x) - p * x1B.x,
-                                                ((svB.y - r * x3B.y) - q * x2B.y) - p * x1B.y);
+                const double2 xA = hept_back(svA, p, q, r, x1A, x2A, x3A);
+                const double2 xB = hept_back(svB, p, q, r, x1B, x2B, x3B);
                 SA(GZ + i) = xA;
                 SB(GZ + i) = xB;
                 if (stats) A.avg[GZ + i] = xA.x;
@@ -888,16 +948,47 @@ __device__ __forceinline__ void bfly(double2* w, int s, double c8)
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
-// In-place transform of one line; every thread of the block must call it
-// (it synchronises the block).  sl: this line's padded shared buffer; tw:
-// exp(-2 pi i m / (tws N)), read with stride tws.
+// Block-wide barrier of the transforms; FftBar256 is the named barrier of
+// the first 256 threads (the transform threads of a larger block).
+struct CtaBar {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct FftBar256 {
+    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
+};
+
+__host__ __device__ constexpr int p2_lead_radix(int n)
+{
+    return ilog2c(n) % 3 == 0 ? 8 : (ilog2c(n) % 3 == 1 ? 2 : 4);
+}
+
+// Twiddles of the radix-8 stages of a power-of-two transform in the order a
+// stage reads them: stage Ns (Ns = R0, 8 R0, .. < N) holds w^(r k N/(8 Ns))
+// at [Ns - R0 + (r-1) Ns + k], r = 1..7, k < Ns (7 (N - R0) / 7 entries in
+// all; at most N).  A warp then reads consecutive entries, free of bank
+// conflicts.  tw: exp(-2 pi i m / N).
 template <int N>
+__device__ __forceinline__ void fill_stage_twiddles(double2* dst, const double2* __restrict__ tw, int tid, int nthreads)
+{
+    constexpr int R0 = p2_lead_radix(N);
+    for (int e = tid; e < N - R0; e += nthreads) {
+        int Ns = R0;
+        while (e >= Ns - R0 + 7 * Ns) Ns *= 8;   // the stage holding entry e
+        const int o = e - (Ns - R0), r = 1 + o / Ns, k = o - (r - 1) * Ns;
+        dst[e] = __ldg(&tw[r * k * (N / (8 * Ns))]);
+    }
+}
+
+// In-place transform of one line; every thread that `bar` synchronises must
+// call it.  sl: this line's padded shared buffer.  TWM 0: tw is
+// exp(-2 pi i m / (tws N)) in global memory, read with stride tws; TWM 1: tw
+// is the stage table of fill_stage_twiddles<N> in shared memory.
+template <int N, class Bar = CtaBar, int TWM = 0>
 __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* __restrict__ tw, int sign,
-                            double c8, int tws = 1)
+                            double c8, int tws = 1, Bar bar = Bar())
 {
     constexpr int T = N / 8;
-    constexpr int LOG = ilog2c(N);
-    constexpr int R0 = LOG % 3 == 0 ? 8 : (LOG % 3 == 1 ? 2 : 4);
+    constexpr int R0 = p2_lead_radix(N);
     {   // leading stage, Ns = 1: no twiddles; output position j*R0 + r
         constexpr int NB = 8 / R0;
 #pragma unroll
@@ -911,16 +1002,23 @@ __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* 
             for (int r = 0; r < R0; r++) sl[pad8(j * R0 + r)] = w[r];
         }
     }
-    __syncthreads();
+    bar();
 #pragma unroll
     for (int Ns = R0; Ns < N; Ns *= 8) {
         double2 w[8];
 #pragma unroll
         for (int r = 0; r < 8; r++) w[r] = sl[pad8(t + r * T)];
-        __syncthreads();
+        bar();
         const int k = t % Ns;
         const int step = N / (Ns * 8);
-        if (k) {
+        if (k && TWM == 1) {
+#pragma unroll
+            for (int r = 1; r < 8; r++) {
+                double2 c = tw[Ns - R0 + (r - 1) * Ns + k];
+                if (sign > 0) c.y = -c.y;
+                w[r] = cmul(w[r], c);
+            }
+        } else if (k) {
             // Twiddles w^r, r = 1..7, of w = exp(-+2 pi i k step / N): three
             // from the table (w, w^2, w^4), the rest as their products.
             // Seven table reads per stage made the transforms bound by the
@@ -941,7 +1039,7 @@ __device__ void fft_p2_line(double2 (&v)[8], int t, double2* sl, const double2* 
             const int base = (t / Ns) * Ns * 8 + k;
 #pragma unroll
             for (int r = 0; r < 8; r++) sl[pad8(base + r * Ns)] = w[r];
-            __syncthreads();
+            bar();
         }
     }
 }
@@ -1192,6 +1290,481 @@ __global__ void __launch_bounds__(256, 4) k_ffty_p2_batch(const BatchRec<FftyArg
     k_ffty_p2_body<N>(R.G, R.A, b);
 }
 
+// ------------------------------------ y transforms fused with the Poisson solve
+
+// Bulk copies global -> shared completing on an mbarrier (no multicast), and
+// the barrier's bounded wait.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned) __cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* b)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(b)) : "memory");
+}
+// generic-proxy accesses of shared memory before a bulk copy into it
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Wait for phase `parity` of barrier b to complete; false after about one
+// second without completion.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity)
+{
+    const unsigned a = smem_u32(b);
+    unsigned long long t0 = 0;
+    for (;;) {
+        unsigned ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+        if (ok) return true;
+        const unsigned long long t = global_ns();
+        if (t0 == 0) t0 = t;
+        else if (t - t0 > 1000000000ull) return false;
+    }
+}
+
+// k_poisson_fft: one block per kx does the forward y transform of that kx's
+// interior rows (ffty_i2o, fft.c:186-202, with its 1/ny), the Poisson band
+// solve of its (ky, ny - ky) column pairs with the wall ghost rows filled
+// (pressure_poisson{2,4}, pressure.c:293-443), and the inverse y transform of
+// all n2 rows (ffty_o2i), for ny = 512.  The spectrum makes one round trip
+// through HBM instead of three; the transforms and the elimination are those
+// of k_ffty_p2 and band_column.
+//
+// Two roles, each in its own warps.  Transform warps (the first 256
+// threads: L = 4 lines of 64 threads) and solver warps (one thread per
+// column pair, 257 of 288 threads) hand row groups of L rows to each other
+// through two shared buffers (named barriers FULL / EMPTY per buffer), so
+// that one role works on a group while the other works on the next.
+//   Forward: rows arrive by bulk copies two groups ahead; the transform
+//   warps transform a group, scale it by 1/ny and stage the group's band
+//   rows; the solvers advance their pairs' elimination through it, storing
+//   the forward-substituted values in place and the multipliers in scratch
+//   (rows of ny/2 + 2 values, 16-byte aligned).
+//   Back: groups top down; the solvers back-substitute a group (its inputs
+//   as bulk copies two groups ahead at order 4, two rows ahead through
+//   registers at order 2) and the six wall ghost rows, the transform warps
+//   transform and store each.
+constexpr int PF_FT = 256;                  // transform threads
+template <int N>
+__host__ __device__ constexpr int pfft_solvers() { return (N / 2 + 1 + 31) / 32 * 32; }
+template <int N>
+__host__ __device__ constexpr int pfft_threads() { return PF_FT + pfft_solvers<N>(); }
+template <int N>
+__host__ __device__ constexpr int pfft_blocks() { return 1; }
+// back-sweep inputs per slot (order 4): forward-substituted rows [L][ny]
+// (complex) and p, q, r rows [3][L][ny/2 + 2]
+template <int ORDER, int N>
+__host__ __device__ constexpr bool pfft_back_ring() { return ORDER == 4; }
+template <int N>
+__host__ __device__ constexpr int pfft_back_slot() { return 2 * 2048 + 3 * (2048 / N) * (N / 2 + 2); }   // doubles
+// layout: copy ring (forward rows [2][L][ny], or back-sweep inputs
+// [2][slot]) | transform lines [L][ny + ny/8] | hand-over buffers [2][L][ny] |
+// band rows [2][L][10] | twiddles [ny] | 4 mbarriers
+template <int ORDER, int N>
+__host__ __device__ constexpr size_t pfft_ring_bytes()
+{
+    return pfft_back_ring<ORDER, N>() && 2 * pfft_back_slot<N>() * sizeof(double) > 2 * 2048 * sizeof(double2)
+               ? 2 * pfft_back_slot<N>() * sizeof(double)
+               : 2 * 2048 * sizeof(double2);
+}
+template <int ORDER, int N>
+constexpr size_t pfft_smem_bytes()
+{
+    return pfft_ring_bytes<ORDER, N>() + 2304 * sizeof(double2) + 2 * 2048 * sizeof(double2)
+         + 2 * (2048 / N) * 10 * sizeof(double) + N * sizeof(double2) + 4 * sizeof(unsigned long long);
+}
+
+// named barriers: 1 transform warps (fft_p2_line), 2/3 FULL, 4/5 EMPTY of
+// buffer 0/1, 6 solver warps
+__device__ __forceinline__ void nbar_sync(int id, int n) { asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void nbar_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(n) : "memory"); }
+// barrier id over n threads that also ORs p across them
+__device__ __forceinline__ bool nbar_or(int id, int n, bool p)
+{
+    int r;
+    asm volatile("{\n .reg .pred a, b;\n setp.ne.b32 a, %1, 0;\n bar.red.or.pred b, %2, %3, a;\n selp.s32 %0, 1, 0, b;\n}\n"
+                 : "=r"(r) : "r"((int) p), "r"(id), "r"(n) : "memory");
+    return r != 0;
+}
+
+template <int ORDER, int N>
+__device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftArgs& F, uint3 bid)
+{
+    static_assert(N == 512, "one block per kx fills the GPU only for ny = 512");
+    constexpr int T = N / 8, L = p2_lines(N), NP = N / 2 + 1, PAD = p2_pad(N);
+    constexpr int SW = pfft_solvers<N>(), BT = PF_FT + SW;
+    constexpr bool BRING = pfft_back_ring<ORDER, N>();
+    constexpr int NPS = NP + 1;                        // pair stride of the multiplier rows (even)
+    constexpr int BSLOT = pfft_back_slot<N>();
+    constexpr int B_FULL = 2, B_EMPTY = 4, B_SOLVE = 6;
+    extern __shared__ double2 pfft_sm[];
+    double2* ring = pfft_sm;                                                  // forward copies
+    double* bring = reinterpret_cast<double*>(pfft_sm);                       // back-sweep copies (BRING)
+    double2* sl = reinterpret_cast<double2*>(reinterpret_cast<char*>(pfft_sm) + pfft_ring_bytes<ORDER, N>());
+    double2* xb = sl + L * PAD;                       // [2][L][N] hand-over buffers
+    double* cst = reinterpret_cast<double*>(xb + 2 * L * N);   // [2][L][10] band rows of a group
+    double2* tws = reinterpret_cast<double2*>(cst + 2 * L * 10);   // stage twiddles (fill_stage_twiddles)
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(tws + N);   // [2] forward, [2] back
+    const PoissonArgs& A = F.P;
+    const int tid = threadIdx.x;
+    const int kx = bid.x;
+    const int nkx = G.nkx, n2 = G.n2, n = A.nrows;
+    const bool fthr = tid < PF_FT;
+    const int t = tid % T, l = tid / T;               // transform lane and line (transform warps)
+    const int ky0 = tid - PF_FT;
+    const bool solver = !fthr && ky0 < NP;
+    const int ky = solver ? ky0 : 0, kyb = (N - ky) & (N - 1);
+    const long long ncol = G.splane;
+    const long long npair = (long long) nkx * NPS, pair = (long long) kx * NPS + ky;
+    double2* sp = A.spec;
+    const long long colA = (long long) kx * N + ky, colB = (long long) kx * N + kyb;
+    auto SA = [&](int k) -> double2& { return sp[(long long) k * ncol + colA]; };
+    auto SB = [&](int k) -> double2& { return sp[(long long) k * ncol + colB]; };
+    auto at = [&](double* base, int k) -> double& { return base[(long long) k * npair + pair]; };
+    auto row = [&](int k) { return sp + ((long long) k * nkx + kx) * N; };   // spectrum row (k, kx)
+    const int var = (kx == 0 && ky == 0) ? 1 : 0;   // pressure.c:331-338
+    const PairRows rows{A, A.lamx[kx], A.lamy[ky], var, n};
+    const int ngrp = (n + L - 1) / L;
+    double* const Pp = A.scratch;                            // order 4: p, q, r; order 2: gamma
+    double* const Qp = A.scratch + (long long) n2 * npair;
+    double* const Rp = A.scratch + 2 * (long long) n2 * npair;
+
+    auto issue = [&](int g) {   // forward group g's rows into copy slot g & 1
+        const int slot = g & 1, r0 = g * L, nr = min(L, n - r0);
+        mbar_expect_tx(&bar[slot], (unsigned) (nr * N * sizeof(double2)));
+        for (int q = 0; q < nr; q++)
+            bulk_g2s(ring + (slot * L + q) * N, row(GZ + r0 + q), N * sizeof(double2), &bar[slot]);
+    };
+    auto bissue = [&](int j) {   // back group j (forward group ngrp - 1 - j): inputs into slot j & 1
+        const int g = ngrp - 1 - j, slot = j & 1, lo = g * L, nr = min(L, n - lo);
+        double* b = bring + slot * BSLOT;
+        mbar_expect_tx(&bar[2 + slot], (unsigned) (nr * (N * sizeof(double2) + 3 * NPS * sizeof(double))));
+        for (int q = 0; q < nr; q++) {
+            const long long k = GZ + lo + q;
+            bulk_g2s(b + 2 * q * N, row((int) k), N * sizeof(double2), &bar[2 + slot]);
+            bulk_g2s(b + 2 * L * N + q * NPS, Pp + (k * nkx + kx) * NPS, NPS * sizeof(double), &bar[2 + slot]);
+            bulk_g2s(b + 2 * L * N + (L + q) * NPS, Qp + (k * nkx + kx) * NPS, NPS * sizeof(double), &bar[2 + slot]);
+            bulk_g2s(b + 2 * L * N + (2 * L + q) * NPS, Rp + (k * nkx + kx) * NPS, NPS * sizeof(double),
+                     &bar[2 + slot]);
+        }
+    };
+
+    if (tid == 0) {
+        for (int q = 0; q < 4; q++) mbar_init(&bar[q], 1);
+        mbar_fence_init();
+    }
+    fill_stage_twiddles<N>(tws, F.twy, tid, BT);
+    __syncthreads();
+    if (tid == 0) {
+        issue(0);
+        if (ngrp > 1) issue(1);
+    }
+
+    const double2 z2 = make_double2(0.0, 0.0);
+    if (fthr) {
+        // ================= transform warps =================
+        const double scale = 1.0 / (double) N;
+        const bool cthr = tid < 10 * L;
+        const int crow = tid / 10, cfld = tid - 10 * (tid / 10);
+        bool failed = false;
+        for (int g = 0; g < ngrp; g++) {
+            const int b = g & 1;
+            const int ci = g * L + crow;   // this thread's band-row value of the group
+            const double cval = cthr && ci < n ? rows.table(cfld, GZ + ci) : 0.0;
+            if (!failed) {
+                const bool bad = !mbar_wait_bounded(&bar[b], (g >> 1) & 1);
+                if (nbar_or(1, PF_FT, bad)) {
+                    failed = true;   // carry on with the hand-overs, without data
+                    if (tid == 0) {
+                        *F.fault = 1.0;
+                        (void) mbar_wait_bounded(&bar[b], (g >> 1) & 1);
+                        if (g + 1 < ngrp) (void) mbar_wait_bounded(&bar[(g + 1) & 1], ((g + 1) >> 1) & 1);
+                    }
+                }
+            }
+            double2 v[8];
+            const double2* src = ring + (b * L + l) * N;
+#pragma unroll
+            for (int q = 0; q < 8; q++) v[q] = src[t + q * T];
+            fft_p2_line<N, FftBar256, 1>(v, t, sl + l * PAD, tws, -1, F.c8);
+            if (tid == 0 && !failed && g + 2 < ngrp) {   // every transform thread has read slot b
+                fence_proxy_async_smem();
+                issue(g + 2);
+            }
+            if (g >= 2) nbar_sync(B_EMPTY + b, BT);
+            double2* dst = xb + (b * L + l) * N;
+#pragma unroll
+            for (int q = 0; q < 8; q++) dst[t + q * T] = make_double2(v[q].x * scale, v[q].y * scale);
+            if (cthr) cst[(b * L + crow) * 10 + cfld] = cval;
+            nbar_arrive(B_FULL + b, BT);
+        }
+        __syncthreads();   // forward done (matches the solvers' barrier)
+        // back: the groups the solvers hand over, in their order
+        const int gt = max(n - 3, 0) / L;
+        const int S = ngrp + 2;
+        for (int s = 0; s < S; s++) {
+            const int b = s & 1;
+            int target;   // spectrum row of line l, or -1
+            if (s <= ngrp - 1 - gt || (s > ngrp - gt && s <= ngrp)) {
+                const int g = s <= ngrp - 1 - gt ? ngrp - 1 - s : ngrp - s;
+                target = g * L + l < n ? GZ + g * L + l : -1;
+            } else if (s == ngrp - gt) {
+                target = l < 3 ? n2 - GZ + l : -1;   // top wall ghost rows
+            } else {
+                target = l < 3 ? l : -1;             // bottom wall ghost rows
+            }
+            nbar_sync(B_FULL + b, BT);
+            double2 v[8];
+            const double2* src = xb + (b * L + l) * N;
+#pragma unroll
+            for (int q = 0; q < 8; q++) v[q] = src[t + q * T];
+            if (s + 2 < S) nbar_arrive(B_EMPTY + b, BT);
+            fft_p2_line<N, FftBar256, 1>(v, t, sl + l * PAD, tws, +1, F.c8);
+            if (target >= 0) {
+                double2* dst = row(target);
+#pragma unroll
+                for (int q = 0; q < 8; q++) dst[t + q * T] = v[q];
+            }
+        }
+        return;
+    }
+
+    // ================= solver warps =================
+    HeptSweep H;
+    double ibet = 0.0, cprev = 0.0;                          // order 2 (tridag.c:4-26)
+    double2 uA = z2, uB = z2;
+    for (int g = 0; g < ngrp; g++) {
+        const int b = g & 1;
+        nbar_sync(B_FULL + b, BT);
+        if (solver) {
+            for (int q = 0; q < L; q++) {
+                const int i = g * L + q;
+                if (i >= n) break;
+                const int k = GZ + i;
+                const double2 rA = xb[(b * L + q) * N + ky], rB = xb[(b * L + q) * N + kyb];
+                const double* st = cst + (b * L + q) * 10;
+                double cf[7];
+                rows.coef_from(i, st, cf);
+                const double dv = st[9];
+                if (ORDER == 2) {
+                    if (i == 0) {
+                        ibet = 1.0 / cf[3];
+                        uA = make_double2(rA.x * dv * ibet, rA.y * dv * ibet);
+                        uB = make_double2(rB.x * dv * ibet, rB.y * dv * ibet);
+                    } else {
+                        const double gm = cprev * ibet;
+                        ibet = 1.0 / (cf[3] - cf[0] * gm);
+                        at(Pp, k) = gm;
+                        uA = make_double2((rA.x * dv - cf[0] * uA.x) * ibet, (rA.y * dv - cf[0] * uA.y) * ibet);
+                        uB = make_double2((rB.x * dv - cf[0] * uB.x) * ibet, (rB.y * dv - cf[0] * uB.y) * ibet);
+                    }
+                    cprev = cf[2];
+                    SA(k) = uA;
+                    SB(k) = uB;
+                } else {
+                    double p, qq, r;
+                    double2 svA, svB;
+                    H.step(cf, make_double2(rA.x * dv, rA.y * dv), make_double2(rB.x * dv, rB.y * dv), p, qq, r,
+                           svA, svB);
+                    at(Pp, k) = p; at(Qp, k) = qq; at(Rp, k) = r;
+                    SA(k) = svA;
+                    SB(k) = svB;
+                }
+            }
+        }
+        if (g + 2 < ngrp) nbar_arrive(B_EMPTY + b, BT);
+    }
+    // the forward stores before the bulk copies that read them back
+    asm volatile("fence.proxy.async;\n" ::: "memory");
+    __syncthreads();
+    if (BRING && tid == PF_FT) {   // into the space the transform warps last read as the forward ring
+        fence_proxy_async_smem();
+        bissue(0);
+        if (ngrp > 1) bissue(1);
+    }
+
+    // ---- back: groups top down, then the wall ghost rows
+    double2 lsA[2], lsB[2];
+    double lp[2];
+    auto bload = [&](int i) {   // order 2: row i's forward values and gamma, in slot i & 1
+        if (BRING || i < 0 || !solver) return;
+        const int k = GZ + i;
+        const double2 a = SA(k), c = SB(k);
+        const double p = i + 1 < n ? at(Pp, k + 1) : 0.0;
+        if (i & 1) { lsA[1] = a; lsB[1] = c; lp[1] = p; }
+        else { lsA[0] = a; lsB[0] = c; lp[0] = p; }
+    };
+    bload(n - 1);
+    bload(n - 2);
+    double2 x1A = z2, x2A = z2, x3A = z2, x1B = z2, x2B = z2, x3B = z2;
+    double2 tpA[3] = {z2, z2, z2}, tpB[3] = {z2, z2, z2};   // rows n-1, n-2, n-3
+    bool failed = false;
+    int s = 0;   // hand-over count
+    // back substitution of row i into line i - lo of hand-over buffer `out`
+    auto back_row = [&](int i, int lo, double2 svA, double2 svB, double p, double q, double r, double2* out,
+                        auto top_tag) {
+        constexpr bool TOP = decltype(top_tag)::value;
+        double2 xA, xB;
+        if (TOP && i == n - 1) {
+            xA = svA;
+            xB = svB;
+        } else if (ORDER == 2) {
+            xA = make_double2(svA.x - p * x1A.x, svA.y - p * x1A.y);
+            xB = make_double2(svB.x - p * x1B.x, svB.y - p * x1B.y);
+        } else {
+            xA = hept_back(svA, p, q, r, x1A, x2A, x3A);
+            xB = hept_back(svB, p, q, r, x1B, x2B, x3B);
+        }
+        x3A = x2A; x2A = x1A; x1A = xA;
+        x3B = x2B; x2B = x1B; x1B = xB;
+        if (TOP) {
+            if (i == n - 1) { tpA[0] = xA; tpB[0] = xB; }
+            if (i == n - 2) { tpA[1] = xA; tpB[1] = xB; }
+            if (i == n - 3) { tpA[2] = xA; tpB[2] = xB; }
+        }
+        out[(i - lo) * N + ky] = xA;
+        out[(i - lo) * N + kyb] = xB;
+    };
+    auto back_group = [&](int g, auto top_tag) {
+        const int b = s & 1;
+        double2* out = xb + b * L * N;
+        const int lo = g * L, hi = min(n, lo + L) - 1;
+        if (s >= 2) nbar_sync(B_EMPTY + b, BT);
+        if constexpr (BRING) {
+            const int j = ngrp - 1 - g;   // back group j: copies in slot j & 1
+            if (!failed) {
+                const bool bad = !mbar_wait_bounded(&bar[2 + (j & 1)], (j >> 1) & 1);
+                if (nbar_or(B_SOLVE, SW, bad)) {
+                    failed = true;   // carry on with the hand-overs, without data
+                    if (tid == PF_FT) {
+                        *F.fault = 1.0;
+                        (void) mbar_wait_bounded(&bar[2 + (j & 1)], (j >> 1) & 1);
+                        if (j + 1 < ngrp) (void) mbar_wait_bounded(&bar[2 + ((j + 1) & 1)], ((j + 1) >> 1) & 1);
+                    }
+                }
+            }
+            if (solver) {
+                const double* bs = bring + (j & 1) * BSLOT;
+                const double2* bv = reinterpret_cast<const double2*>(bs);
+                const double* bp = bs + 2 * L * N;
+                for (int i = hi; i >= lo; i--) {
+                    const int q = i - lo;
+                    back_row(i, lo, bv[q * N + ky], bv[q * N + kyb], bp[q * NPS + ky], bp[(L + q) * NPS + ky],
+                             bp[(2 * L + q) * NPS + ky], out, top_tag);
+                }
+            }
+            nbar_sync(B_SOLVE, SW);   // every solver has read back slot j & 1
+            if (tid == PF_FT && !failed && j + 2 < ngrp) {
+                fence_proxy_async_smem();
+                bissue(j + 2);
+            }
+        } else if (solver) {
+            for (int i1 = hi | 1; i1 >= lo; i1 -= 2) {
+#pragma unroll
+                for (int u = 1; u >= 0; u--) {
+                    const int i = i1 - 1 + u;
+                    if (i > hi || i < lo) continue;
+                    const double2 svA = lsA[u], svB = lsB[u];
+                    const double p = lp[u];
+                    bload(i - 2);
+                    back_row(i, lo, svA, svB, p, 0.0, 0.0, out, top_tag);
+                }
+            }
+        }
+        nbar_arrive(B_FULL + b, BT);
+        s++;
+    };
+    // wall ghost rows (ghost_fill_{bot,top}{2,4}, pressure.c:516-531,
+    // 728-769) as one hand-over: lines 0..2 hold gA/gB[0..2]
+    auto ghost_group = [&](const double2* gA, const double2* gB) {
+        const int b = s & 1;
+        double2* out = xb + b * L * N;
+        if (s >= 2) nbar_sync(B_EMPTY + b, BT);
+        if (solver) {
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                out[q * N + ky] = gA[q];
+                out[q * N + kyb] = gB[q];
+            }
+        }
+        nbar_arrive(B_FULL + b, BT);
+        s++;
+    };
+    // the groups holding rows n-1 .. max(n-3, 0), the top ghost rows
+    // n2-3 .. n2-1 from rows n-1..n-3 (zero where n < 3), the other groups,
+    // the bottom ghost rows 0..2 from rows 0..2
+    const int gt = max(n - 3, 0) / L;
+    for (int g = ngrp - 1; g >= gt; g--) back_group(g, std::true_type{});
+    {
+        double2 gA[3], gB[3];
+        double g1, g2, g3, h1, h2, h3;
+        if (ORDER == 2) {
+            fill_top<2>(A.top, tpA[0].x, 0.0, 0.0, g1, g2, g3);
+            fill_top<2>(A.top, tpA[0].y, 0.0, 0.0, h1, g2, g3);
+            gA[0] = make_double2(g1, h1); gA[1] = gA[2] = z2;
+            fill_top<2>(A.top, tpB[0].x, 0.0, 0.0, g1, g2, g3);
+            fill_top<2>(A.top, tpB[0].y, 0.0, 0.0, h1, g2, g3);
+            gB[0] = make_double2(g1, h1); gB[1] = gB[2] = z2;
+        } else {
+            fill_top<4>(A.top, tpA[0].x, tpA[1].x, tpA[2].x, g1, g2, g3);
+            fill_top<4>(A.top, tpA[0].y, tpA[1].y, tpA[2].y, h1, h2, h3);
+            gA[0] = make_double2(g1, h1); gA[1] = make_double2(g2, h2); gA[2] = make_double2(g3, h3);
+            fill_top<4>(A.top, tpB[0].x, tpB[1].x, tpB[2].x, g1, g2, g3);
+            fill_top<4>(A.top, tpB[0].y, tpB[1].y, tpB[2].y, h1, h2, h3);
+            gB[0] = make_double2(g1, h1); gB[1] = make_double2(g2, h2); gB[2] = make_double2(g3, h3);
+        }
+        ghost_group(gA, gB);
+    }
+    for (int g = gt - 1; g >= 0; g--) back_group(g, std::false_type{});
+    {
+        double2 gA[3], gB[3];
+        double g1, g2, g3, h1, h2, h3;
+        if (ORDER == 2) {
+            fill_bot<2>(A.bot[var], x1A.x, 0.0, 0.0, g1, g2, g3);
+            fill_bot<2>(A.bot[var], x1A.y, 0.0, 0.0, h1, g2, g3);
+            gA[0] = gA[1] = z2; gA[2] = make_double2(g1, h1);
+            fill_bot<2>(A.bot[var], x1B.x, 0.0, 0.0, g1, g2, g3);
+            fill_bot<2>(A.bot[var], x1B.y, 0.0, 0.0, h1, g2, g3);
+            gB[0] = gB[1] = z2; gB[2] = make_double2(g1, h1);
+        } else {
+            fill_bot<4>(A.bot[var], x1A.x, x2A.x, x3A.x, g1, g2, g3);
+            fill_bot<4>(A.bot[var], x1A.y, x2A.y, x3A.y, h1, h2, h3);
+            gA[2] = make_double2(g1, h1); gA[1] = make_double2(g2, h2); gA[0] = make_double2(g3, h3);
+            fill_bot<4>(A.bot[var], x1B.x, x2B.x, x3B.x, g1, g2, g3);
+            fill_bot<4>(A.bot[var], x1B.y, x2B.y, x3B.y, h1, h2, h3);
+            gB[2] = make_double2(g1, h1); gB[1] = make_double2(g2, h2); gB[0] = make_double2(g3, h3);
+        }
+        ghost_group(gA, gB);
+    }
+}
+
+template <int ORDER, int N>
+__global__ void __launch_bounds__(pfft_threads<N>(), pfft_blocks<N>()) k_poisson_fft(Geo G, PoissonFftArgs A)
+{
+    poisson_fft_body<ORDER, N>(G, A, blockIdx);
+}
+
+template <int ORDER, int N>
+__global__ void __launch_bounds__(pfft_threads<N>(), pfft_blocks<N>()) k_poisson_fft_batch(const BatchRec<PoissonFftArgs>* r, int n)
+{
+    uint3 b;
+    const BatchRec<PoissonFftArgs>& R = batch_locate(r, n, b);
+    poisson_fft_body<ORDER, N>(R.G, R.A, b);
+}
+
 // Complex-to-real x transform (fftx_c2d, pressure.c:163-200) as an inverse
 // complex transform of half length: with X[0] and X[N/2] taken real (as
 // FFTW's c2r does), Z[k] = (X[k] + conj X[M-k]) + i exp(2 pi i k/N)
@@ -1297,6 +1870,15 @@ static cudaError_t p2_set_smem()
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_r2c_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sy);
+    if constexpr (N == 512) {   // the fused kernel's one size (poisson_fft_supported)
+        const int sp2 = (int) pfft_smem_bytes<2, N>(), sp4 = (int) pfft_smem_bytes<4, N>();
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_poisson_fft<2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp2);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_poisson_fft<4, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp4);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_poisson_fft_batch<2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp2);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_poisson_fft_batch<4, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp4);
+    }
     return e;
 }
 
@@ -1414,6 +1996,50 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st,
     }
 #undef CASE_
     k_fftx_c2r<0><<<grd, FFT_THREADS, sm, st>>>(G, A);
+}
+
+// Only ny = 512: there one block per kx has 257 column pairs; at smaller ny
+// the blocks are too few to fill the GPU (129 at ny = 256), and the separate
+// launches measured faster (0.27 against 0.37 ms at 256 x 256 x 192).
+bool poisson_fft_supported(const Geo& G)
+{
+    return G.ny == 512 && (G.order == 2 || G.order == 4);
+}
+
+template <int ORDER, int N>
+static void launch_poisson_fft_n(const Geo& G, const PoissonFftArgs& A, cudaStream_t st)
+{
+    k_poisson_fft<ORDER, N><<<G.nkx, pfft_threads<N>(), pfft_smem_bytes<ORDER, N>(), st>>>(G, A);
+}
+
+void launch_poisson_fft(const Geo& G, const PoissonFftArgs& A, cudaStream_t st)
+{
+#define CASE_(n_) \
+    case n_: \
+        if (G.order == 2) launch_poisson_fft_n<2, n_>(G, A, st); \
+        else launch_poisson_fft_n<4, n_>(G, A, st); \
+        return;
+    switch (G.ny) {   // poisson_fft_supported
+    CASE_(512)
+    default: break;
+    }
+#undef CASE_
+}
+
+void launch_poisson_fft_batch(const BatchLaunch& L, int key, cudaStream_t st)
+{
+    auto r = static_cast<const BatchRec<PoissonFftArgs>*>(L.recs);
+    const int order = key % 8, ny = key / 8;
+#define CASE_(n_) \
+    case n_: \
+        if (order == 2) k_poisson_fft_batch<2, n_><<<L.blocks, pfft_threads<n_>(), pfft_smem_bytes<2, n_>(), st>>>(r, L.n); \
+        else k_poisson_fft_batch<4, n_><<<L.blocks, pfft_threads<n_>(), pfft_smem_bytes<4, n_>(), st>>>(r, L.n); \
+        return;
+    switch (ny) {
+    CASE_(512)
+    default: break;
+    }
+#undef CASE_
 }
 
 void launch_poisson(const Geo& G, const PoissonArgs& A, cudaStream_t st)
