@@ -177,6 +177,11 @@ int cf_profile(cf_instance *inst, int nsub, double *ms);
 /* Number of kernel launches the engine issues per substep. */
 int cf_launches_per_substep(const cf_instance *inst);
 
+/* 1 when the instance runs its y transforms and Poisson solve as one launch
+ * (k_poisson_fft: ny = 512, unless CF_FUSE_PRESSURE=0 was set when it was
+ * created), 0 when as three, CF_EINVAL for a null instance. */
+int cf_pressure_fused(const cf_instance *inst);
+
 const char *cf_strerror(int status);
 
 /* ------------------------------------------------------------------------

@@ -62,6 +62,7 @@ def test_fused_equals_separate(cf, gpu, order, nx, ny, nz):
     fused = make(cf, order, nx, ny, nz, True)
     sep = make(cf, order, nx, ny, nz, False)
     assert fused.launches_per_substep() == sep.launches_per_substep() - 2
+    assert fused.pressure_fused() and not sep.pressure_fused()
     fused.step(3)
     sep.step(3)
     compare(fused, sep, f"o{order} {nx}x{ny}x{nz} 3 substeps")
@@ -79,6 +80,7 @@ def test_other_sizes_keep_separate_launches(cf, gpu, ny):
     a = make(cf, 4, 32, ny, 16, True)
     b = make(cf, 4, 32, ny, 16, False)
     assert a.launches_per_substep() == b.launches_per_substep()
+    assert not a.pressure_fused() and not b.pressure_fused()
     a.close()
     b.close()
 

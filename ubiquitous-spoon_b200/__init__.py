@@ -123,6 +123,7 @@ def _bind(L):
     L.cf_set_dt.argtypes = [vp, ctypes.c_double]
     L.cf_device_field.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)]
     L.cf_launches_per_substep.argtypes = [vp]
+    L.cf_pressure_fused.argtypes = [vp]
     L.cf_profile.argtypes = [vp, ip, dp]
     L.cf_strerror.restype = ctypes.c_char_p
     L.cf_strerror.argtypes = [ip]
@@ -301,6 +302,13 @@ class Instance:
 
     def launches_per_substep(self):
         return int(self.L.cf_launches_per_substep(self.h))
+
+    def pressure_fused(self):
+        """True when the y transforms and the Poisson solve run as one launch
+        (k_poisson_fft); the profile's y-transform groups are then empty."""
+        r = int(self.L.cf_pressure_fused(self.h))
+        _check(min(r, 0), "cf_pressure_fused")
+        return r == 1
 
     def launch_shape(self):
         """Tuned launch shape: (back-substitution threads, Poisson threads,

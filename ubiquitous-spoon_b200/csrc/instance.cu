@@ -2368,6 +2368,12 @@ unsigned long long cf_instance_bytes(const cf_config* c)
     return b;
 }
 
+int cf_pressure_fused(const cf_instance* I)
+{
+    if (!I) return CF_EINVAL;
+    return I->fuse_pressure && poisson_fft_supported(I->geo) ? 1 : 0;
+}
+
 int cf_launches_per_substep(const cf_instance* I)
 {
     // pressure: div+fftx (two launches for power-of-two nx), ffty, poisson,
