@@ -178,8 +178,11 @@ int cf_profile(cf_instance *inst, int nsub, double *ms);
 int cf_launches_per_substep(const cf_instance *inst);
 
 /* 1 when the instance runs its y transforms and Poisson solve as one launch
- * (k_poisson_fft: ny = 512, unless CF_FUSE_PRESSURE=0 was set when it was
- * created), 0 when as three, CF_EINVAL for a null instance. */
+ * (k_poisson_fft), 0 when as three, CF_EINVAL for a null instance.  The
+ * fused launch needs ny = 512; it is taken by default where its one block
+ * per kx fills the GPU (nx/2 + 1 at least the SM count).  CF_FUSE_PRESSURE=1
+ * in the environment at creation takes it whenever ny = 512,
+ * CF_FUSE_PRESSURE=0 never. */
 int cf_pressure_fused(const cf_instance *inst);
 
 const char *cf_strerror(int status);

@@ -31,9 +31,12 @@ CASES = [(4, 32, 512, 22), (2, 16, 512, 9), (4, 64, 512, 37), (4, 48, 512, 20), 
 
 
 def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0):
+    """fused: True forces the fused launch where ny = 512, False the separate
+    ones, None leaves the choice to the default rule."""
     prm = cn.Params(order=order, nx=nx, ny=ny, nz=nz, lx=4 * np.pi, ly=4 * np.pi / 3, lz=2.0, dt=1e-3,
                     nu=1.0 / re, prandtl=0.71)
-    os.environ["CF_FUSE_PRESSURE"] = "1" if fused else "0"
+    if fused is not None:
+        os.environ["CF_FUSE_PRESSURE"] = "1" if fused else "0"
     try:
         inst = cf.Instance(cf.Config.from_params(prm))
     finally:
@@ -83,6 +86,20 @@ def test_other_sizes_keep_separate_launches(cf, gpu, ny):
     assert not a.pressure_fused() and not b.pressure_fused()
     a.close()
     b.close()
+
+
+def test_default_rule(cf, gpu):
+    """By default the fused launch is taken only where its one block per kx
+    fills the GPU: ny = 512 and nx/2 + 1 at least the SM count."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    nx_big = 512 if 512 // 2 + 1 >= sms else 2 * sms
+    small = make(cf, 4, 32, 512, 8, None)
+    big = make(cf, 4, nx_big, 512, 8, None)
+    assert not small.pressure_fused()
+    assert big.pressure_fused()
+    small.close()
+    big.close()
 
 
 def test_batch_mixing_fused_and_separate(cf, gpu):

@@ -414,8 +414,10 @@ struct cf_instance {
     cf_config cfg;
     Metrics m;
     Geo geo;
-    // y transforms fused with the Poisson solve where ny is a power of two;
-    // CF_FUSE_PRESSURE=0 at creation selects the three separate launches
+    // y transforms fused with the Poisson solve (k_poisson_fft, ny = 512):
+    // by default where its one block per kx fills the GPU (nx/2 + 1 at least
+    // the SM count); CF_FUSE_PRESSURE=1 at creation fuses whenever ny = 512,
+    // CF_FUSE_PRESSURE=0 never
     bool fuse_pressure = true;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1740,7 +1742,13 @@ int cf_create(const cf_config* cfg, void* stream, cf_instance** out)
     cf_instance* I = new (std::nothrow) cf_instance();
     if (!I) return CF_ENOMEM;
     const char* fp = std::getenv("CF_FUSE_PRESSURE");
-    I->fuse_pressure = !(fp && fp[0] == '0');
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 0;
+    if (fp && fp[0] == '0') I->fuse_pressure = false;
+    else if (fp && fp[0] == '1') I->fuse_pressure = true;
+    else I->fuse_pressure = sms > 0 && cfg->nx / 2 + 1 >= sms;
     rc = create_impl(cfg, stream, I);
     if (rc) {
         cf_destroy(I);
