@@ -1,5 +1,5 @@
 """The y transforms fused with the Poisson solve (k_poisson_fft, one block per
-kx, used for ny = 512) against the three separate launches (k_ffty_p2,
+kx, for ny = 256 and 512) against the three separate launches (k_ffty_p2,
 k_poisson, k_ffty_p2) that CF_FUSE_PRESSURE=0 selects at creation.
 
 Both run the same elimination code (PairRows, HeptSweep) and the same
@@ -10,12 +10,14 @@ states agree to rounding, not bit for bit (measured at most 1.3e-14 on u,
 v, w, c and 4.5e-12 on p): relative L2 <= 1e-13 on u, v, w, c and <= 1e-10
 on p, the engine's bars against the reference, after 3 eager
 substeps and two graph-replayed RK3 steps.  The grids reach every path of
-the kernel: the ninth warp, whose one thread solves the ky = ny/2 pair; a
-last row group shorter than the 4-row groups; the smallest nz of each
-order; orders 2 and 4 (order 4 with its back-sweep inputs in shared
-memory); and non-power-of-two nx.  Other ny keep the separate launches.  A
-batch mixing fused and separate members gives each member the result it
-has alone."""
+the kernel: both sizes (groups of 4 rows of 512 and of 8 rows of 256); the
+last solver warp, whose one thread solves the ky = ny/2 pair; a last row
+group shorter than the others; the smallest nz of each order; orders 2
+and 4 (order 4 with its back-sweep inputs in shared memory); and
+non-power-of-two nx.  Other ny keep the separate launches, and by default
+the fused launch is taken only where its blocks fill the GPU.  A batch
+mixing fused and separate members gives each member the result it has
+alone."""
 import os
 
 import numpy as np
@@ -27,7 +29,8 @@ pytestmark = pytest.mark.gpu
 
 # order, nx, ny, nz
 CASES = [(4, 32, 512, 22), (2, 16, 512, 9), (4, 64, 512, 37), (4, 48, 512, 20), (2, 32, 512, 4),
-         (4, 16, 512, 6), (2, 24, 512, 14)]
+         (4, 16, 512, 6), (2, 24, 512, 14), (4, 32, 256, 20), (2, 16, 256, 9), (4, 48, 256, 13),
+         (4, 64, 256, 6)]
 
 
 def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0):
@@ -78,7 +81,7 @@ def test_fused_equals_separate(cf, gpu, order, nx, ny, nz):
     sep.close()
 
 
-@pytest.mark.parametrize("ny", [64, 256])
+@pytest.mark.parametrize("ny", [64, 128])
 def test_other_sizes_keep_separate_launches(cf, gpu, ny):
     a = make(cf, 4, 32, ny, 16, True)
     b = make(cf, 4, 32, ny, 16, False)
@@ -88,14 +91,15 @@ def test_other_sizes_keep_separate_launches(cf, gpu, ny):
     b.close()
 
 
-def test_default_rule(cf, gpu):
+@pytest.mark.parametrize("ny", [256, 512])
+def test_default_rule(cf, gpu, ny):
     """By default the fused launch is taken only where its one block per kx
-    fills the GPU: ny = 512 and nx/2 + 1 at least the SM count."""
+    gives the GPU enough blocks: nx/2 + 1 at least half the SM count."""
     import torch
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    nx_big = 512 if 512 // 2 + 1 >= sms else 2 * sms
-    small = make(cf, 4, 32, 512, 8, None)
-    big = make(cf, 4, nx_big, 512, 8, None)
+    nx_big = next(n for n in (64, 128, 256, 512) if 2 * (n // 2 + 1) >= sms)
+    small = make(cf, 4, 32, ny, 8, None)
+    big = make(cf, 4, nx_big, ny, 8, None)
     assert not small.pressure_fused()
     assert big.pressure_fused()
     small.close()
@@ -106,7 +110,7 @@ def test_batch_mixing_fused_and_separate(cf, gpu):
     """Members that fuse (power-of-two ny) and members that cannot (ny = 48)
     or chose not to share one batch; each ends where it ends alone."""
     # order, nx, ny, nz, fused, seed (members 0 and 3: one state, both paths)
-    spec = [(4, 32, 512, 24, True, 20), (2, 64, 48, 20, True, 21), (2, 16, 512, 10, True, 22),
+    spec = [(4, 32, 512, 24, True, 20), (2, 64, 48, 20, True, 21), (2, 16, 256, 10, True, 22),
             (4, 32, 512, 24, False, 20), (2, 32, 128, 16, True, 24)]
     mixed = [make(cf, *m[:4], fused=m[4], seed=m[5]) for m in spec]
     alone = [make(cf, *m[:4], fused=m[4], seed=m[5]) for m in spec]

@@ -414,10 +414,10 @@ struct cf_instance {
     cf_config cfg;
     Metrics m;
     Geo geo;
-    // y transforms fused with the Poisson solve (k_poisson_fft, ny = 512):
-    // by default where its one block per kx fills the GPU (nx/2 + 1 at least
-    // the SM count); CF_FUSE_PRESSURE=1 at creation fuses whenever ny = 512,
-    // CF_FUSE_PRESSURE=0 never
+    // y transforms fused with the Poisson solve (k_poisson_fft, ny = 256 or
+    // 512): by default where its one block per kx gives the GPU enough
+    // blocks (nx/2 + 1 at least half the SM count); CF_FUSE_PRESSURE=1 at
+    // creation fuses wherever supported, CF_FUSE_PRESSURE=0 never
     bool fuse_pressure = true;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1748,7 +1748,7 @@ int cf_create(const cf_config* cfg, void* stream, cf_instance** out)
         sms = 0;
     if (fp && fp[0] == '0') I->fuse_pressure = false;
     else if (fp && fp[0] == '1') I->fuse_pressure = true;
-    else I->fuse_pressure = sms > 0 && cfg->nx / 2 + 1 >= sms;
+    else I->fuse_pressure = sms > 0 && 2 * (cfg->nx / 2 + 1) >= sms;
     rc = create_impl(cfg, stream, I);
     if (rc) {
         cf_destroy(I);

@@ -1403,7 +1403,7 @@ __device__ __forceinline__ bool nbar_or(int id, int n, bool p)
 template <int ORDER, int N>
 __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftArgs& F, uint3 bid)
 {
-    static_assert(N == 512, "one block per kx fills the GPU only for ny = 512");
+    static_assert(N == 256 || N == 512, "groups of 2048 points: 8 or 4 rows");
     constexpr int T = N / 8, L = p2_lines(N), NP = N / 2 + 1, PAD = p2_pad(N);
     constexpr int SW = pfft_solvers<N>(), BT = PF_FT + SW;
     constexpr bool BRING = pfft_back_ring<ORDER, N>();
@@ -1870,7 +1870,7 @@ static cudaError_t p2_set_smem()
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_r2c_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fftx_c2r_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ffty_p2_batch<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sy);
-    if constexpr (N == 512) {   // the fused kernel's one size (poisson_fft_supported)
+    if constexpr (N == 256 || N == 512) {   // the fused kernel's sizes (poisson_fft_supported)
         const int sp2 = (int) pfft_smem_bytes<2, N>(), sp4 = (int) pfft_smem_bytes<4, N>();
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_poisson_fft<2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp2);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_poisson_fft<4, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp4);
@@ -1998,12 +1998,13 @@ void launch_fftx_c2r(const Geo& G, const C2rArgs& A, int nrows, cudaStream_t st,
     k_fftx_c2r<0><<<grd, FFT_THREADS, sm, st>>>(G, A);
 }
 
-// Only ny = 512: there one block per kx has 257 column pairs; at smaller ny
-// the blocks are too few to fill the GPU (129 at ny = 256), and the separate
-// launches measured faster (0.27 against 0.37 ms at 256 x 256 x 192).
+// ny = 256 or 512: a row group is 2048 points (8 or 4 rows of ny), the
+// transform warps' one layout.  Whether an instance takes the fused launch
+// by default (one block per kx must give the GPU enough blocks) is decided
+// at creation (cf_create).
 bool poisson_fft_supported(const Geo& G)
 {
-    return G.ny == 512 && (G.order == 2 || G.order == 4);
+    return (G.ny == 256 || G.ny == 512) && (G.order == 2 || G.order == 4);
 }
 
 template <int ORDER, int N>
@@ -2020,7 +2021,7 @@ void launch_poisson_fft(const Geo& G, const PoissonFftArgs& A, cudaStream_t st)
         else launch_poisson_fft_n<4, n_>(G, A, st); \
         return;
     switch (G.ny) {   // poisson_fft_supported
-    CASE_(512)
+    CASE_(256) CASE_(512)
     default: break;
     }
 #undef CASE_
@@ -2036,7 +2037,7 @@ void launch_poisson_fft_batch(const BatchLaunch& L, int key, cudaStream_t st)
         else k_poisson_fft_batch<4, n_><<<L.blocks, pfft_threads<n_>(), pfft_smem_bytes<4, n_>(), st>>>(r, L.n); \
         return;
     switch (ny) {
-    CASE_(512)
+    CASE_(256) CASE_(512)
     default: break;
     }
 #undef CASE_
