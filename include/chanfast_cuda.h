@@ -179,10 +179,10 @@ int cf_launches_per_substep(const cf_instance *inst);
 
 /* 1 when the instance runs its y transforms and Poisson solve as one launch
  * (k_poisson_fft), 0 when as three, CF_EINVAL for a null instance.  The
- * fused launch needs ny = 512; it is taken by default where its one block
- * per kx fills the GPU (nx/2 + 1 at least the SM count).  CF_FUSE_PRESSURE=1
- * in the environment at creation takes it whenever ny = 512,
- * CF_FUSE_PRESSURE=0 never. */
+ * fused launch needs ny = 256 or 512; it is taken by default where its one
+ * block per kx gives the GPU enough blocks (nx/2 + 1 at least half the SM
+ * count).  CF_FUSE_PRESSURE=1 in the environment at creation takes it
+ * wherever supported, CF_FUSE_PRESSURE=0 never. */
 int cf_pressure_fused(const cf_instance *inst);
 
 const char *cf_strerror(int status);
