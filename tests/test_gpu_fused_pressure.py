@@ -17,7 +17,8 @@ and 4 (order 4 with its back-sweep inputs in shared memory); and
 non-power-of-two nx.  Other ny keep the separate launches, and by default
 the fused launch is taken only where its blocks fill the GPU.  A batch
 mixing fused and separate members gives each member the result it has
-alone."""
+alone.  The fully implicit scheme's four spectral Helmholtz solves take the
+same kernel without the ghost fill."""
 import os
 
 import numpy as np
@@ -33,15 +34,15 @@ CASES = [(4, 32, 512, 22), (2, 16, 512, 9), (4, 64, 512, 37), (4, 48, 512, 20), 
          (4, 64, 256, 6)]
 
 
-def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0):
-    """fused: True forces the fused launch where ny = 512, False the separate
-    ones, None leaves the choice to the default rule."""
+def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0, scheme="chanfast"):
+    """fused: True forces the fused launch where supported, False the
+    separate ones, None leaves the choice to the default rule."""
     prm = cn.Params(order=order, nx=nx, ny=ny, nz=nz, lx=4 * np.pi, ly=4 * np.pi / 3, lz=2.0, dt=1e-3,
                     nu=1.0 / re, prandtl=0.71)
     if fused is not None:
         os.environ["CF_FUSE_PRESSURE"] = "1" if fused else "0"
     try:
-        inst = cf.Instance(cf.Config.from_params(prm))
+        inst = cf.Instance(cf.Config.from_params(prm, scheme=scheme))
     finally:
         os.environ.pop("CF_FUSE_PRESSURE", None)
     inst.init_fields(seed, 0.1, 0.01)
@@ -76,6 +77,26 @@ def test_fused_equals_separate(cf, gpu, order, nx, ny, nz):
     sep.step_graph(2)
     compare(fused, sep, f"o{order} {nx}x{ny}x{nz} +2 steps")
     fused.sync()
+    assert fused.max_divergence() < 1e-12
+    fused.close()
+    sep.close()
+
+
+@pytest.mark.parametrize("order,nx,ny,nz", [(4, 64, 256, 12), (2, 64, 512, 9), (4, 64, 512, 10)])
+def test_channel_fused_equals_separate(cf, gpu, order, nx, ny, nz):
+    """The fully implicit scheme: its four spectral Helmholtz solves with
+    their y transforms in one launch (k_poisson_fft_batch without the ghost
+    fill; w over nz - 1 faces; the xy-average profiles of u and c from the
+    (0, 0) column), and the pressure solve fused as above."""
+    fused = make(cf, order, nx, ny, nz, True, scheme="channel")
+    sep = make(cf, order, nx, ny, nz, False, scheme="channel")
+    assert fused.launches_per_substep() == sep.launches_per_substep() - 7
+    fused.step(3)
+    sep.step(3)
+    compare(fused, sep, f"channel o{order} {nx}x{ny}x{nz} 3 substeps")
+    fused.step_graph(2)
+    sep.step_graph(2)
+    compare(fused, sep, f"channel o{order} {nx}x{ny}x{nz} +2 steps")
     assert fused.max_divergence() < 1e-12
     fused.close()
     sep.close()

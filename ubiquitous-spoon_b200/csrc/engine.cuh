@@ -280,6 +280,9 @@ void launch_ffty_batch(const BatchLaunch& L, int ny, cudaStream_t st);   // ny: 
 void launch_poisson_batch(const BatchLaunch& L, int order, cudaStream_t st);
 // key: 8 * ny + order
 void launch_poisson_fft_batch(const BatchLaunch& L, int key, cudaStream_t st);
+// the four spectral Helmholtz solves of the fully implicit scheme with their y
+// transforms, one record per field (ny = 256 or 512)
+void launch_helmholtz_fft_batch(const BatchLaunch& L, int order, int ny, cudaStream_t st);
 void launch_c2r_batch(const BatchLaunch& L, int nx, cudaStream_t st);    // nx: power of two, else generic
 void launch_project_batch(const BatchLaunch& L, int order, cudaStream_t st);
 cudaError_t rhs_set_smem_limits();

@@ -432,6 +432,9 @@ struct cf_instance {
     double* avg = nullptr;
     double* avg_c = nullptr;        // channel scheme: xy-average of c (avg holds u's)
     double* dscal = nullptr;        // [0] mdpdx, [1] dcdt, [2] non-finite flag, [3] copy-wait fault flag
+    // channel scheme with the fused Helmholtz solves: device records [3][4]
+    // (substep set, field u v w c) of k_poisson_fft_batch without FILL
+    void* hrec = nullptr;
     long long* dcount = nullptr;    // device substep counter (log row)
     double* dlog = nullptr;
     int log_cap = 0;
@@ -479,6 +482,9 @@ int check_config(const cf_config* c)
 }
 
 // Build every per-substep coefficient table for time step dt and upload.
+int build_helm_records(cf_instance* I);
+bool helm_fused(const cf_instance* I);
+
 int build_tables(cf_instance* I, double dt)
 {
     const cf_config& C = I->cfg;
@@ -598,6 +604,10 @@ int build_tables(cf_instance* I, double dt)
     // a new graph is needed whenever the tables move
     if (I->gexec) { cudaGraphExecDestroy(I->gexec); I->gexec = nullptr; }
     if (I->graph) { cudaGraphDestroy(I->graph); I->graph = nullptr; }
+    if (helm_fused(I)) {
+        const int hr = build_helm_records(I);
+        if (hr) return hr;
+    }
     return CF_OK;
 }
 
@@ -766,25 +776,36 @@ void enqueue_implicit3d(cf_instance* I, int s, Timeline* tl)
     const long long sstride = G.splane * G.n2;     // between the four spectra
     R2cArgs X{I->gbuf[0], I->spec, I->px, I->c8, GZ, fstride, sstride};
     launch_fftx_r2c(G, X, G.nz, 4, st);
-    FftyArgs Y{I->spec, I->py, -1, GZ, I->c8, sstride};
-    launch_ffty(G, Y, G.nz, st, 4);
-    // slot order u, v, w, c; sets u/v 0, c 1, w 2
-    const int set_of_slot[4] = {0, 0, 2, 1};
-    for (int f = 0; f < 4; f++) {
-        PoissonArgs H = poisson_args(I, I->hspec[s][set_of_slot[f]], 0.0);
-        H.spec = I->spec + f * sstride;
-        H.nrows = f == 2 ? C.nz - 1 : C.nz;
-        if (f == 0 || f == 3) {   // u, c: the xy-average profile for the controls
-            H.avg = f == 0 ? I->avg : I->avg_c;
-            H.abot = I->bc_ub;
-            H.atop = I->bc_ut;
-            H.abc_bot = f == 0 ? 0.0 - C.setuframe : -0.5;
-            H.abc_top = f == 0 ? 0.0 - C.setuframe : +0.5;
+    if (helm_fused(I)) {
+        // y transforms and the four solves in one launch (records of set s)
+        BatchLaunch L;
+        L.recs = static_cast<const char*>(I->hrec) + 4 * s * sizeof(BatchRec<PoissonFftArgs>);
+        L.n = 4;
+        L.blocks = 4u * (unsigned) G.nkx;
+        L.smem = 0;
+        L.block = dim3(1);
+        launch_helmholtz_fft_batch(L, G.order, G.ny, st);
+    } else {
+        FftyArgs Y{I->spec, I->py, -1, GZ, I->c8, sstride};
+        launch_ffty(G, Y, G.nz, st, 4);
+        // slot order u, v, w, c; sets u/v 0, c 1, w 2
+        const int set_of_slot[4] = {0, 0, 2, 1};
+        for (int f = 0; f < 4; f++) {
+            PoissonArgs H = poisson_args(I, I->hspec[s][set_of_slot[f]], 0.0);
+            H.spec = I->spec + f * sstride;
+            H.nrows = f == 2 ? C.nz - 1 : C.nz;
+            if (f == 0 || f == 3) {   // u, c: the xy-average profile for the controls
+                H.avg = f == 0 ? I->avg : I->avg_c;
+                H.abot = I->bc_ub;
+                H.atop = I->bc_ut;
+                H.abc_bot = f == 0 ? 0.0 - C.setuframe : -0.5;
+                H.abc_top = f == 0 ? 0.0 - C.setuframe : +0.5;
+            }
+            launch_helmholtz_spectral(G, H, st);
         }
-        launch_helmholtz_spectral(G, H, st);
+        FftyArgs Yb{I->spec, I->py, +1, GZ, I->c8, sstride};
+        launch_ffty(G, Yb, G.nz, st, 4);
     }
-    FftyArgs Yb{I->spec, I->py, +1, GZ, I->c8, sstride};
-    launch_ffty(G, Yb, G.nz, st, 4);
     C2rArgs Xb{I->spec, {I->u, I->v, I->w, I->c}, I->px, I->c8, GZ, sstride};
     launch_fftx_c2r(G, Xb, G.nz, st, 4);
     GhostArgs GA;
@@ -939,6 +960,56 @@ BatchRec<Args> batch_rec(const Geo& G, const Args& A, dim3 g)
     r.gz = g.z;
     r.begin = 0;
     return r;
+}
+
+// The fully implicit scheme's four spectral Helmholtz solves run fused with
+// their y transforms (k_poisson_fft_batch, FILL off) where the pressure
+// solve of the instance is fused.
+bool helm_fused(const cf_instance* I)
+{
+    return I->cfg.scheme == CF_SCHEME_CHANNEL && I->fuse_pressure && poisson_fft_supported(I->geo);
+}
+
+// Scratch of one field's Helmholtz solve (k_poisson_fft's multiplier rows).
+size_t helm_scratch_stride(const cf_instance* I)
+{
+    const Geo& G = I->geo;
+    return (size_t) (I->cfg.order == 4 ? 3 : 1) * G.n2 * G.nkx * (G.ny / 2 + 2);
+}
+
+// Records of the fused solves of u, v, w, c for each substep set: the
+// arguments enqueue_implicit3d gives the separate solves, each field with its
+// own spectrum and scratch, its blocks after the previous field's.
+int build_helm_records(cf_instance* I)
+{
+    const cf_config& C = I->cfg;
+    const Geo& G = I->geo;
+    const long long sstride = G.splane * G.n2;
+    const int set_of_slot[4] = {0, 0, 2, 1};
+    std::vector<BatchRec<PoissonFftArgs>> recs;
+    for (int s = 0; s < 3; s++) {
+        for (int f = 0; f < 4; f++) {
+            PoissonArgs H = poisson_args(I, I->hspec[s][set_of_slot[f]], 0.0);
+            H.spec = I->spec + f * sstride;
+            H.scratch = I->scratch + f * helm_scratch_stride(I);
+            H.nrows = f == 2 ? C.nz - 1 : C.nz;
+            if (f == 0 || f == 3) {   // u, c: the xy-average profile for the controls
+                H.avg = f == 0 ? I->avg : I->avg_c;
+                H.abot = I->bc_ub;
+                H.atop = I->bc_ut;
+                H.abc_bot = f == 0 ? 0.0 - C.setuframe : -0.5;
+                H.abc_top = f == 0 ? 0.0 - C.setuframe : +0.5;
+            }
+            PoissonFftArgs F{H, I->py.tw, I->c8, I->dscal + 3};
+            BatchRec<PoissonFftArgs> r = batch_rec(G, F, dim3(G.nkx));
+            r.begin = (unsigned) (f * G.nkx);
+            recs.push_back(r);
+        }
+    }
+    const size_t bytes = recs.size() * sizeof(BatchRec<PoissonFftArgs>);
+    if (!I->hrec) CF_CUDA(cudaMalloc(&I->hrec, bytes));
+    CF_CUDA(cudaMemcpy(I->hrec, recs.data(), bytes, cudaMemcpyHostToDevice));
+    return CF_OK;
 }
 
 struct BatchSink : Sink {
@@ -1636,6 +1707,7 @@ int cf_destroy(cf_instance* I)
                     I->twy};
     for (void* b : bufs)
         if (b) cudaFree(b);
+    if (I->hrec) cudaFree(I->hrec);
     if (I->own_stream && I->stream) cudaStreamDestroy(I->stream);
     cudaSetDevice(prev);
     delete I;
@@ -1686,7 +1758,9 @@ static int create_impl(const cf_config* cfg, void* stream, cf_instance* I)
     CF_CUDA(cudaMalloc(&I->spec, nspec * sizeof(double2)));
     CF_CUDA(cudaMemsetAsync(I->spec, 0, nspec * sizeof(double2), I->stream));
     const int nscr = C.order == 4 ? 3 : 1;
-    CF_CUDA(cudaMalloc(&I->scratch, (size_t) nscr * G.splane * G.n2 * sizeof(double)));
+    size_t nscratch = (size_t) nscr * G.splane * G.n2;
+    if (helm_fused(I)) nscratch = std::max(nscratch, 4 * helm_scratch_stride(I));   // one per field
+    CF_CUDA(cudaMalloc(&I->scratch, nscratch * sizeof(double)));
     // per-warp partial sums of k_back4, for its largest block size
     const long long nwarps = ((G.plane + SOLVE_THREADS_MAX - 1) / SOLVE_THREADS_MAX) * (SOLVE_THREADS_MAX / 32);
     CF_CUDA(cudaMalloc(&I->partial, (size_t) nwarps * G.n2 * sizeof(double)));
@@ -2393,7 +2467,8 @@ int cf_launches_per_substep(const cf_instance* I)
     // launch (two fewer).
     if (!I) return CF_EINVAL;
     const int pressure = (fftx_batched_supported(I->cfg.nx) ? 7 : 6) - (I->fuse_pressure && poisson_fft_supported(I->geo) ? 2 : 0);
-    return (I->cfg.scheme == CF_SCHEME_CHANNEL ? 13 : 7) + pressure;
+    // the channel scheme's y transforms and four spectral solves: 6 launches, or 1 fused
+    return (I->cfg.scheme == CF_SCHEME_CHANNEL ? (helm_fused(I) ? 8 : 13) : 7) + pressure;
 }
 
 }  // extern "C"

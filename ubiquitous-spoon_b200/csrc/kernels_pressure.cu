@@ -1400,7 +1400,11 @@ __device__ __forceinline__ bool nbar_or(int id, int n, bool p)
     return r != 0;
 }
 
-template <int ORDER, int N>
+// FILL: the Poisson solve, with the wall ghost rows of the solution; else a
+// spectral Helmholtz solve of the fully implicit scheme (band_column without
+// FILL): no ghost rows, the xy-average profile from the (0, 0) column when
+// A.avg is set, w's top wall face zeroed.
+template <int ORDER, int N, bool FILL = true>
 __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftArgs& F, uint3 bid)
 {
     static_assert(N == 256 || N == 512, "groups of 2048 points: 8 or 4 rows");
@@ -1514,11 +1518,14 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
         __syncthreads();   // forward done (matches the solvers' barrier)
         // back: the groups the solvers hand over, in their order
         const int gt = max(n - 3, 0) / L;
-        const int S = ngrp + 2;
+        const int S = FILL ? ngrp + 2 : ngrp;
         for (int s = 0; s < S; s++) {
             const int b = s & 1;
             int target;   // spectrum row of line l, or -1
-            if (s <= ngrp - 1 - gt || (s > ngrp - gt && s <= ngrp)) {
+            if (!FILL) {
+                const int g = ngrp - 1 - s;
+                target = g * L + l < n ? GZ + g * L + l : -1;
+            } else if (s <= ngrp - 1 - gt || (s > ngrp - gt && s <= ngrp)) {
                 const int g = s <= ngrp - 1 - gt ? ngrp - 1 - s : ngrp - s;
                 target = g * L + l < n ? GZ + g * L + l : -1;
             } else if (s == ngrp - gt) {
@@ -1538,6 +1545,11 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
 #pragma unroll
                 for (int q = 0; q < 8; q++) dst[t + q * T] = v[q];
             }
+        }
+        if (!FILL && GZ + n < n2 - GZ && l == 0) {   // w: the top wall face
+            double2* dst = row(GZ + n);
+#pragma unroll
+            for (int q = 0; q < 8; q++) dst[t + q * T] = make_double2(0.0, 0.0);
         }
         return;
     }
@@ -1613,6 +1625,7 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
     double2 tpA[3] = {z2, z2, z2}, tpB[3] = {z2, z2, z2};   // rows n-1, n-2, n-3
     bool failed = false;
     int s = 0;   // hand-over count
+    const bool stats = !FILL && A.avg != nullptr && kx == 0 && ky0 == 0;   // the (0, 0) column
     // back substitution of row i into line i - lo of hand-over buffer `out`
     auto back_row = [&](int i, int lo, double2 svA, double2 svB, double p, double q, double r, double2* out,
                         auto top_tag) {
@@ -1637,6 +1650,7 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
         }
         out[(i - lo) * N + ky] = xA;
         out[(i - lo) * N + kyb] = xB;
+        if (stats) A.avg[GZ + i] = xA.x;
     };
     auto back_group = [&](int g, auto top_tag) {
         const int b = s & 1;
@@ -1708,6 +1722,11 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
     // the bottom ghost rows 0..2 from rows 0..2
     const int gt = max(n - 3, 0) / L;
     for (int g = ngrp - 1; g >= gt; g--) back_group(g, std::true_type{});
+    if constexpr (!FILL) {
+        for (int g = gt - 1; g >= 0; g--) back_group(g, std::false_type{});
+        if (stats) average_walls<ORDER>(A, n2);
+        return;
+    }
     {
         double2 gA[3], gB[3];
         double g1, g2, g3, h1, h2, h3;
@@ -1757,12 +1776,12 @@ __global__ void __launch_bounds__(pfft_threads<N>(), pfft_blocks<N>()) k_poisson
     poisson_fft_body<ORDER, N>(G, A, blockIdx);
 }
 
-template <int ORDER, int N>
+template <int ORDER, int N, bool FILL = true>
 __global__ void __launch_bounds__(pfft_threads<N>(), pfft_blocks<N>()) k_poisson_fft_batch(const BatchRec<PoissonFftArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<PoissonFftArgs>& R = batch_locate(r, n, b);
-    poisson_fft_body<ORDER, N>(R.G, R.A, b);
+    poisson_fft_body<ORDER, N, FILL>(R.G, R.A, b);
 }
 
 // Complex-to-real x transform (fftx_c2d, pressure.c:163-200) as an inverse
@@ -1878,6 +1897,10 @@ static cudaError_t p2_set_smem()
             e = cudaFuncSetAttribute(k_poisson_fft_batch<2, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp2);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_poisson_fft_batch<4, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp4);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_poisson_fft_batch<2, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp2);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_poisson_fft_batch<4, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp4);
     }
     return e;
 }
@@ -2021,6 +2044,23 @@ void launch_poisson_fft(const Geo& G, const PoissonFftArgs& A, cudaStream_t st)
         else launch_poisson_fft_n<4, n_>(G, A, st); \
         return;
     switch (G.ny) {   // poisson_fft_supported
+    CASE_(256) CASE_(512)
+    default: break;
+    }
+#undef CASE_
+}
+
+// The four spectral Helmholtz solves of the fully implicit scheme with their
+// y transforms: one record per field (FILL off).
+void launch_helmholtz_fft_batch(const BatchLaunch& L, int order, int ny, cudaStream_t st)
+{
+    auto r = static_cast<const BatchRec<PoissonFftArgs>*>(L.recs);
+#define CASE_(n_) \
+    case n_: \
+        if (order == 2) k_poisson_fft_batch<2, n_, false><<<L.blocks, pfft_threads<n_>(), pfft_smem_bytes<2, n_>(), st>>>(r, L.n); \
+        else k_poisson_fft_batch<4, n_, false><<<L.blocks, pfft_threads<n_>(), pfft_smem_bytes<4, n_>(), st>>>(r, L.n); \
+        return;
+    switch (ny) {
     CASE_(256) CASE_(512)
     default: break;
     }
