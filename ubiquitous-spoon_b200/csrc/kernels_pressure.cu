@@ -1362,8 +1362,6 @@ template <int N>
 __host__ __device__ constexpr int pfft_solvers() { return (N / 2 + 1 + 31) / 32 * 32; }
 template <int N>
 __host__ __device__ constexpr int pfft_threads() { return PF_FT + pfft_solvers<N>(); }
-template <int N>
-__host__ __device__ constexpr int pfft_blocks() { return 1; }
 // back-sweep inputs per slot (order 4): forward-substituted rows [L][ny]
 // (complex) and p, q, r rows [3][L][ny/2 + 2]
 template <int ORDER, int N>
@@ -1771,13 +1769,13 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
 }
 
 template <int ORDER, int N>
-__global__ void __launch_bounds__(pfft_threads<N>(), pfft_blocks<N>()) k_poisson_fft(Geo G, PoissonFftArgs A)
+__global__ void __launch_bounds__(pfft_threads<N>(), 1) k_poisson_fft(Geo G, PoissonFftArgs A)
 {
     poisson_fft_body<ORDER, N>(G, A, blockIdx);
 }
 
 template <int ORDER, int N, bool FILL = true>
-__global__ void __launch_bounds__(pfft_threads<N>(), pfft_blocks<N>()) k_poisson_fft_batch(const BatchRec<PoissonFftArgs>* r, int n)
+__global__ void __launch_bounds__(pfft_threads<N>(), 1) k_poisson_fft_batch(const BatchRec<PoissonFftArgs>* r, int n)
 {
     uint3 b;
     const BatchRec<PoissonFftArgs>& R = batch_locate(r, n, b);
