@@ -185,6 +185,14 @@ int cf_launches_per_substep(const cf_instance *inst);
  * wherever supported, CF_FUSE_PRESSURE=0 never. */
 int cf_pressure_fused(const cf_instance *inst);
 
+/* Test hook for the bounded waits: with on != 0, the instance's fused pressure
+ * launches (cf_pressure_fused) leave their forward row copies unissued, so
+ * that the first wait of every block runs out after about a second; the
+ * kernel then finishes without data and cf_sync returns CF_ETIMEOUT.  Nothing
+ * faults or hangs.  The hook stays until called with on = 0; the status
+ * clears with cf_set_field / cf_init_fields. */
+int cf_debug_stall_copies(cf_instance *inst, int on);
+
 const char *cf_strerror(int status);
 
 /* ------------------------------------------------------------------------

@@ -102,6 +102,33 @@ def test_channel_fused_equals_separate(cf, gpu, order, nx, ny, nz):
     sep.close()
 
 
+def test_copy_wait_timeout(cf, gpu):
+    """A bounded wait that runs out, with nothing faulted: with
+    cf_debug_stall_copies the fused launch leaves its row copies unissued (an
+    mbarrier phase that nothing completes).  Every block's wait gives up after
+    about a second, the kernel finishes without data, and cf_sync reports
+    CF_ETIMEOUT.  Reloading the fields clears the status, and the GPU goes on
+    working: two fresh instances step to equal states."""
+    inst = make(cf, 4, 32, 256, 8, True)
+    assert inst.pressure_fused()
+    inst.debug_stall_copies(True)
+    inst.step(1)
+    with pytest.raises(cf.ChanfastError) as e:
+        inst.sync()
+    assert e.value.status == cf.CF_ETIMEOUT
+    inst.debug_stall_copies(False)
+    inst.init_fields(3, 0.1, 0.01)
+    inst.sync()
+    a = make(cf, 4, 32, 256, 8, True)
+    b = make(cf, 4, 32, 256, 8, True)
+    a.step(3)
+    b.step(3)
+    for nm in "uvwcp":
+        assert np.array_equal(a.get_field(nm), b.get_field(nm)), nm
+    for x in (inst, a, b):
+        x.close()
+
+
 @pytest.mark.parametrize("ny", [64, 128])
 def test_other_sizes_keep_separate_launches(cf, gpu, ny):
     a = make(cf, 4, 32, ny, 16, True)

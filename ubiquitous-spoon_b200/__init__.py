@@ -124,6 +124,7 @@ def _bind(L):
     L.cf_device_field.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)]
     L.cf_launches_per_substep.argtypes = [vp]
     L.cf_pressure_fused.argtypes = [vp]
+    L.cf_debug_stall_copies.argtypes = [vp, ip]
     L.cf_profile.argtypes = [vp, ip, dp]
     L.cf_strerror.restype = ctypes.c_char_p
     L.cf_strerror.argtypes = [ip]
@@ -302,6 +303,11 @@ class Instance:
 
     def launches_per_substep(self):
         return int(self.L.cf_launches_per_substep(self.h))
+
+    def debug_stall_copies(self, on):
+        """Test hook: the fused pressure launches leave their row copies
+        unissued, so their bounded waits run out (cf_sync: CF_ETIMEOUT)."""
+        _check(self.L.cf_debug_stall_copies(self.h, int(bool(on))), "cf_debug_stall_copies")
 
     def pressure_fused(self):
         """True when the y transforms and the Poisson solve run as one launch

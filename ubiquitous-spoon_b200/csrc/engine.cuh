@@ -214,6 +214,8 @@ struct PoissonFftArgs {
     const double2* twy;   // exp(-2 pi i m / ny)
     double c8;            // cos(pi/4) from the host table
     double* fault;        // set to 1 when a wait for a row copy gave up
+    int stall;            // test hook: nonzero leaves the forward row copies unissued,
+                          // so that the first wait runs out (cf_debug_stall_copies)
 };
 bool poisson_fft_supported(const Geo& G);
 void launch_poisson_fft(const Geo& G, const PoissonFftArgs& A, cudaStream_t st);

@@ -435,6 +435,7 @@ struct cf_instance {
     // channel scheme with the fused Helmholtz solves: device records [3][4]
     // (substep set, field u v w c) of k_poisson_fft_batch without FILL
     void* hrec = nullptr;
+    bool stall_copies = false;      // test hook (cf_debug_stall_copies)
     long long* dcount = nullptr;    // device substep counter (log row)
     double* dlog = nullptr;
     int log_cap = 0;
@@ -697,7 +698,7 @@ void pressure_sequence(cf_instance* I, const PoissonOffsets& po, double pdt, int
     if (I->fuse_pressure && K.fused_pressure(G)) {
         // one launch; its time is the Poisson group's, the y-transform groups stay empty
         K.mark();
-        PoissonFftArgs F{poisson_args(I, po, pdt), I->py.tw, I->c8, I->dscal + 3};
+        PoissonFftArgs F{poisson_args(I, po, pdt), I->py.tw, I->c8, I->dscal + 3, I->stall_copies ? 1 : 0};
         K.poisson_fft(G, F);
         K.mark();
         K.mark();
@@ -1000,7 +1001,7 @@ int build_helm_records(cf_instance* I)
                 H.abc_bot = f == 0 ? 0.0 - C.setuframe : -0.5;
                 H.abc_top = f == 0 ? 0.0 - C.setuframe : +0.5;
             }
-            PoissonFftArgs F{H, I->py.tw, I->c8, I->dscal + 3};
+            PoissonFftArgs F{H, I->py.tw, I->c8, I->dscal + 3, 0};
             BatchRec<PoissonFftArgs> r = batch_rec(G, F, dim3(G.nkx));
             r.begin = (unsigned) (f * G.nkx);
             recs.push_back(r);
@@ -2448,6 +2449,16 @@ unsigned long long cf_instance_bytes(const cf_config* c)
     b += n2 * 8 * 512 + (unsigned long long) (c->nx + c->ny) * 8;              // coefficient tables (bound)
     b += (unsigned long long) (c->nx + 2 * c->ngx) * (c->ny + 2 * c->ngy) * n2 * 8;   // staging
     return b;
+}
+
+int cf_debug_stall_copies(cf_instance* I, int on)
+{
+    if (!I) return CF_EINVAL;
+    I->stall_copies = on != 0;
+    // a captured graph holds the launches as they were
+    if (I->gexec) { cudaGraphExecDestroy(I->gexec); I->gexec = nullptr; }
+    if (I->graph) { cudaGraphDestroy(I->graph); I->graph = nullptr; }
+    return CF_OK;
 }
 
 int cf_pressure_fused(const cf_instance* I)

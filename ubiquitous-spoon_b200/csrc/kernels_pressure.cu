@@ -1318,21 +1318,21 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 // Wait for phase `parity` of barrier b to complete; false after about one
-// second without completion.
+// second without completion (global timer), or after 2^26 polls should the
+// timer not advance.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity)
 {
     const unsigned a = smem_u32(b);
-    unsigned long long t0 = 0;
-    for (;;) {
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 0; it < (1u << 26); it++) {
         unsigned ok;
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
                      " selp.u32 %0, 1, 0, p;\n}\n"
                      : "=r"(ok) : "r"(a), "r"(parity) : "memory");
         if (ok) return true;
-        const unsigned long long t = global_ns();
-        if (t0 == 0) t0 = t;
-        else if (t - t0 > 1000000000ull) return false;
+        if (global_ns() - t0 > 1000000000ull) return false;
     }
+    return false;
 }
 
 // k_poisson_fft: one block per kx does the forward y transform of that kx's
@@ -1470,7 +1470,7 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
     }
     fill_stage_twiddles<N>(tws, F.twy, tid, BT);
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && !F.stall) {
         issue(0);
         if (ngrp > 1) issue(1);
     }
@@ -1492,8 +1492,10 @@ __device__ __forceinline__ void poisson_fft_body(const Geo& G, const PoissonFftA
                     failed = true;   // carry on with the hand-overs, without data
                     if (tid == 0) {
                         *F.fault = 1.0;
-                        (void) mbar_wait_bounded(&bar[b], (g >> 1) & 1);
-                        if (g + 1 < ngrp) (void) mbar_wait_bounded(&bar[(g + 1) & 1], ((g + 1) >> 1) & 1);
+                        if (!F.stall) {   // the copies of groups g and g + 1 are in flight
+                            (void) mbar_wait_bounded(&bar[b], (g >> 1) & 1);
+                            if (g + 1 < ngrp) (void) mbar_wait_bounded(&bar[(g + 1) & 1], ((g + 1) >> 1) & 1);
+                        }
                     }
                 }
             }
