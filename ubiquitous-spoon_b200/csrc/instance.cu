@@ -1113,6 +1113,9 @@ void add_groups(BatchProgram& P, int kernel, const std::vector<BatchRec<Args>>& 
     for (const auto& r : recs) groups[key(r)].push_back(r);
     for (auto& kv : groups) {
         auto& g = kv.second;
+        // the members with the tallest columns first: blocks start roughly in
+        // index order, so the longest-running ones are not left for the end
+        std::stable_sort(g.begin(), g.end(), [](const auto& a, const auto& b) { return a.G.n2 > b.G.n2; });
         unsigned begin = 0;
         size_t sm = 0;
         for (auto& r : g) {
