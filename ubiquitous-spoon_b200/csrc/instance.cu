@@ -2444,7 +2444,13 @@ unsigned long long cf_instance_bytes(const cf_config* c)
     const unsigned long long fb = plane * n2 * 8;
     unsigned long long b = 5 * fb + 8 * fb;                                     // u v w c p, f and g blocks
     b += (c->scheme == CF_SCHEME_CHANNEL ? 4 : 1) * splane * n2 * 16;          // spectra
-    b += (c->order == 4 ? 3 : 1) * splane * n2 * 8;                            // band-solve scratch
+    unsigned long long scr = (c->order == 4 ? 3 : 1) * splane * n2 * 8;        // band-solve scratch
+    if (c->scheme == CF_SCHEME_CHANNEL && (c->ny == 256 || c->ny == 512)) {
+        // the fused spectral solves may take one scratch per field, and their records
+        const unsigned long long per = (c->order == 4 ? 3ull : 1ull) * n2 * (c->nx / 2 + 1) * (c->ny / 2 + 2) * 8;
+        scr = std::max(scr, 4 * per) + 65536;
+    }
+    b += scr;
     const unsigned long long nwarps = (plane + SOLVE_THREADS_MAX - 1) / SOLVE_THREADS_MAX * (SOLVE_THREADS_MAX / 32);
     b += 2 * nwarps * n2 * 8 + 2 * n2 * 8 + 64 + 8;                            // row sums, averages, scalars
     b += 3ull * 4096 * LOG_COLS * 8;                                           // log ring
