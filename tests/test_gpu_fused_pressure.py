@@ -34,10 +34,10 @@ CASES = [(4, 32, 512, 22), (2, 16, 512, 9), (4, 64, 512, 37), (4, 48, 512, 20), 
          (4, 64, 256, 6)]
 
 
-def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0, scheme="chanfast"):
+def make(cf, order, nx, ny, nz, fused, seed=3, re=4000.0, scheme="chanfast", dt=1e-3):
     """fused: True forces the fused launch where supported, False the
     separate ones, None leaves the choice to the default rule."""
-    prm = cn.Params(order=order, nx=nx, ny=ny, nz=nz, lx=4 * np.pi, ly=4 * np.pi / 3, lz=2.0, dt=1e-3,
+    prm = cn.Params(order=order, nx=nx, ny=ny, nz=nz, lx=4 * np.pi, ly=4 * np.pi / 3, lz=2.0, dt=dt,
                     nu=1.0 / re, prandtl=0.71)
     if fused is not None:
         os.environ["CF_FUSE_PRESSURE"] = "1" if fused else "0"
@@ -127,6 +127,24 @@ def test_copy_wait_timeout(cf, gpu):
         assert np.array_equal(a.get_field(nm), b.get_field(nm)), nm
     for x in (inst, a, b):
         x.close()
+
+
+@pytest.mark.parametrize("scheme", ["chanfast", "channel"])
+def test_set_dt_rebuilds_fused_records(cf, gpu, scheme):
+    """cf_set_dt rebuilds the band tables, and with them the fused channel
+    solves' precomputed records: an instance whose dt was changed steps as
+    one created with that dt."""
+    a = make(cf, 4, 64, 256, 10, True, scheme=scheme)
+    b = make(cf, 4, 64, 256, 10, True, scheme=scheme, dt=5e-4)
+    a.set_dt(5e-4)
+    a.step(3)
+    b.step(3)
+    a.step_graph(1)
+    b.step_graph(1)
+    for nm in "uvwcp":
+        assert np.array_equal(a.get_field(nm), b.get_field(nm)), nm
+    a.close()
+    b.close()
 
 
 @pytest.mark.parametrize("ny", [64, 128])
