@@ -996,17 +996,19 @@ def modified_wavenumbers(n, order):
     return lam
 
 
-def pressure_poisson(ch, g: Grid, dt, order):
+def pressure_poisson(ch, g: Grid, dt, order, kx0=0):
     """Per (kx, ky) line solve of the discrete Poisson equation in z, Re and
     Im parts separately (pressure.c:293-354 / 357-443).  ch: complex array
-    (nx/2+1, ny, n2), modified in place; all n2 entries written.  The mean
-    mode (0, 0) uses p = 0 (Dirichlet) at the bottom wall, every other mode
-    Neumann at both walls."""
+    (nkx, ny, n2) of the wavenumbers kx0 .. kx0 + nkx - 1 (all nx/2+1 of them
+    by default; a range of them for one rank of a kx-slab decomposition),
+    modified in place; all n2 entries written.  The mean mode (0, 0) uses
+    p = 0 (Dirichlet) at the bottom wall, every other mode Neumann at both
+    walls."""
     p = g.p
     n2, gz, nz = g.n2, p.ngz, p.nz
     dx, dy, dz = g.dx, g.dy, g.dz
-    nkx = p.nx // 2 + 1
-    lamx = modified_wavenumbers(p.nx, order)[:nkx]
+    nkx = ch.shape[0]
+    lamx = modified_wavenumbers(p.nx, order)[kx0:kx0 + nkx]
     lamy = modified_wavenumbers(p.ny, order)
     LX = np.repeat(lamx, p.ny)
     LY = np.tile(lamy, nkx)
@@ -1024,7 +1026,7 @@ def pressure_poisson(ch, g: Grid, dt, order):
         _band_u(g, dt, order, B)
         src = cols.real if part == 0 else cols.imag
         B.r[:, K] = src[:, K] * B.dvol[K]
-        _pressure_closure_and_solve(B, g, order, ncol)
+        _pressure_closure_and_solve(B, g, order, ncol, kx0 == 0)
         if part == 0:
             out.real = B.x
         else:
@@ -1032,13 +1034,16 @@ def pressure_poisson(ch, g: Grid, dt, order):
     cols[:] = out
 
 
-def _pressure_closure_and_solve(B, g, order, ncol):
+def _pressure_closure_and_solve(B, g, order, ncol, mean_mode=True):
     """ghost_stencil/reduce/solve/fill of pressure_poisson{2,4} with per-column
-    coefficient rows (mode (0, 0) is column 0)."""
+    coefficient rows (mode (0, 0) is column 0 when mean_mode)."""
     n2, gz, nz = g.n2, g.p.ngz, g.p.nz
     K = slice(gz, n2 - gz)
     # Column 0 is (kx, ky) = (0, 0): Dirichlet bottom; all others Neumann.
-    groups = [(np.arange(1), DIRICHP), (np.arange(1, ncol), NEUMANP)]
+    if mean_mode:
+        groups = [(np.arange(1), DIRICHP), (np.arange(1, ncol), NEUMANP)]
+    else:
+        groups = [(np.arange(ncol), NEUMANP)]
     for idx, btype in groups:
         if idx.size == 0:
             continue
@@ -1117,10 +1122,11 @@ def new_state(u, v, w, c, grid: Grid) -> State:
                  f=[fill() for _ in range(4)], g=[fill() for _ in range(4)])
 
 
-def _mass_control(x, h, solve, g: Grid, gamdt, kappa, order):
+def _mass_control(x, h, solve, g: Grid, gamdt, kappa, order, comm=None):
     """Bulk-mean statistics of chanfast.c:485-523 / 572-610: xy-average,
     z-average, wall gradients, centreline; for x and for the Green's function
     h = solve(gamdt)."""
+    comm = comm or SINGLE_RANK
     p = g.p
     gx, gy, gz, n2, nz = p.ngx, p.ngy, p.ngz, g.n2, p.nz
     dz = g.dz
@@ -1130,7 +1136,7 @@ def _mass_control(x, h, solve, g: Grid, gamdt, kappa, order):
             h[:] = gamdt
             solve(h, h)
         src = x if pass_ == 0 else h
-        avg = get_xy_avg(src, g)
+        avg = comm.xy_avg(src, g)
         vol = get_z_avg(avg, nz, gz, dz)
         if order == 4:
             bot = kappa * (A1 * (avg[gz] - avg[gz - 1]) + A2 * (avg[gz + 1] - avg[gz - 2])) / (0.5 * (dz[gz] + dz[gz - 1]))
@@ -1160,9 +1166,34 @@ def get_z_avg(avg, nz, gz, dz):
     return a / lz
 
 
-def substep(st: State, prm: Params, g: Grid):
+class SingleRank:
+    """The three operations of a substep that need the whole x-y plane, on
+    one rank: periodic halos (ghostz_periodic), xy averages (get_xy_avg) and
+    the pressure solve (FFT3D_FWD, pressure_poisson, FFT3D_BWD).  A
+    decomposed run passes its own object with the same methods to
+    substep()."""
+
+    def halo(self, a, g: Grid):
+        ghostz_periodic(a, g)
+
+    def xy_avg(self, a, g: Grid):
+        return get_xy_avg(a, g)
+
+    def pressure(self, d, g: Grid, dt, order):
+        """p (interior, (nx, ny, n2)) from the divergence d (padded)."""
+        ch = fft_forward(d, g)
+        pressure_poisson(ch, g, dt, order)
+        return fft_backward(ch, g)
+
+
+SINGLE_RANK = SingleRank()
+
+
+def substep(st: State, prm: Params, g: Grid, comm=None):
     """One RK3 substep of chanfast2/chanfast4 (chanfast.c:395-656 /
-    1319-1580), in the reference's order."""
+    1319-1580), in the reference's order.  comm: the whole-plane operations
+    (SingleRank by default)."""
+    comm = comm or SINGLE_RANK
     order = prm.order
     step = st.substep % 3
     st.f, st.g = st.g, st.f
@@ -1173,9 +1204,9 @@ def substep(st: State, prm: Params, g: Grid):
     bcs = {"u": (0.0 - uf, 0.0 - uf), "v": (0.0 - vf, 0.0 - vf), "c": (-0.5, 0.5), "w": (0.0, 0.0)}
 
     for a, nm in ((u, "u"), (v, "v"), (c, "c")):
-        ghostz_periodic(a, g)
+        comm.halo(a, g)
         apply_bc_u(a, g, *bcs[nm], order)
-    ghostz_periodic(w, g)
+    comm.halo(w, g)
     apply_bc_w(w, g, *bcs["w"], order)
 
     mu, mv, mw = massflux(u, v, w, g, order, 0)
@@ -1192,7 +1223,7 @@ def substep(st: State, prm: Params, g: Grid):
     add_laplacexy_operator(c, fc, g, prm.nu / prm.prandtl, order, False)
     add_buoyancy(c, fu, fv, fw, g, (prm.betg_x, prm.betg_y, prm.betg_z), order)
     for a in (fu, fv, fw, fc):
-        ghostz_periodic(a, g)
+        comm.halo(a, g)
 
     nu, dt, pr = prm.nu, prm.dt, prm.prandtl
     nuadt = nu * RK3_ALP[step] * dt
@@ -1224,7 +1255,7 @@ def substep(st: State, prm: Params, g: Grid):
         abc(x)
         if name in ("u", "c"):
             kappa = nu if name == "u" else nu / pr
-            s0, s1 = _mass_control(x, h, solve, g, gamdt, kappa, order)
+            s0, s1 = _mass_control(x, h, solve, g, gamdt, kappa, order, comm)
             if name == "u":
                 m = (prm.want_uvolavg - uf - s0[0]) / s1[0] if prm.uvolavgmode == 1 else -prm.dpdx
             else:
@@ -1237,18 +1268,16 @@ def substep(st: State, prm: Params, g: Grid):
 
     d = np.full(g.shape, np.nan)
     divergence(u, v, w, d, g, order)
-    ch = fft_forward(d, g)
-    pressure_poisson(ch, g, abdt, order)
-    pad_interior(st.p, fft_backward(ch, g), g)
-    ghostz_periodic(st.p, g)
+    pad_interior(st.p, comm.pressure(d, g, abdt, order), g)
+    comm.halo(st.p, g)
     project(u, v, w, st.p, g, abdt, order)
     st.log.append(row)
     st.substep += 1
 
 
-def run(st: State, prm: Params, g: Grid, nsub: int):
+def run(st: State, prm: Params, g: Grid, nsub: int, comm=None):
     for _ in range(nsub):
-        substep(st, prm, g)
+        substep(st, prm, g, comm)
     return st
 
 
