@@ -1237,8 +1237,12 @@ __device__ __forceinline__ void k_fftx_r2c_p2_body(const Geo& G, const R2cArgs& 
     }
 }
 
+// Four resident blocks per SM (64 registers instead of 80, no spills):
+// 32 warps instead of 24 keep more lines' loads in flight; at 512 x 512 x
+// 384 the x transform with the divergence takes 0.943 instead of 0.960 ms.
+// The batched variant keeps 80 registers: capped, it spills at 64 and 128.
 template <int N>
-__global__ void __launch_bounds__(256) k_fftx_r2c_p2(Geo G, R2cArgs A)
+__global__ void __launch_bounds__(256, 4) k_fftx_r2c_p2(Geo G, R2cArgs A)
 {
     k_fftx_r2c_p2_body<N>(G, A, blockIdx);
 }
@@ -1827,8 +1831,10 @@ __device__ __forceinline__ void k_fftx_c2r_p2_body(const Geo& G, const C2rArgs& 
     }
 }
 
+// Four resident blocks per SM, as the forward transform (64 registers, a
+// 4-byte spill at N = 512): 0.340 instead of 0.357 ms at 512 x 512 x 384.
 template <int N>
-__global__ void __launch_bounds__(256) k_fftx_c2r_p2(Geo G, C2rArgs A)
+__global__ void __launch_bounds__(256, 4) k_fftx_c2r_p2(Geo G, C2rArgs A)
 {
     k_fftx_c2r_p2_body<N>(G, A, blockIdx);
 }
