@@ -80,7 +80,7 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def _worker(rank, world, port, order, nx, ny, nz, control, nsub):
+def _worker(rank, world, port, order, nx, ny, nz, control, nsub, betg=(0.0, 0.0, 0.0)):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     for q in (root, os.path.join(root, "oracle")):
@@ -95,7 +95,7 @@ def _worker(rank, world, port, order, nx, ny, nz, control, nsub):
     try:
         prm = cn.Params(order=order, nx=nx, ny=ny, nz=nz, lx=4 * np.pi, ly=4 * np.pi / 3, lz=2.0, dt=1e-3,
                         nu=1 / 2800.0, prandtl=0.71, uvolavgmode=1 if control else 0,
-                        cvolavgmode=1 if control else 0)
+                        cvolavgmode=1 if control else 0, betg_x=betg[0], betg_y=betg[1], betg_z=betg[2])
         g = cn.Grid(prm)
         u, v, w, c = ic.raw_state(prm, g.dz, 5, 0.1, 0.01)
         cn.project_initial(u, v, w, prm, g, 1.0)
@@ -139,3 +139,10 @@ def test_slab_substeps_match_single_rank(world, order, nx, ny, nz):
 @pytest.mark.parametrize("world,order", [(2, 4), (3, 2)])
 def test_slab_substeps_without_control_are_bitwise(world, order):
     mp.spawn(_worker, args=(world, _free_port(), order, 12, 12, 6, False, 3), nprocs=world, join=True)
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_slab_substeps_with_buoyancy(order):
+    """add_buoyancy (scalar.c:6-76) interpolates c to the u, v, w faces,
+    in y across the slab edge: the ghosts carry it."""
+    mp.spawn(_worker, args=(2, _free_port(), order, 12, 10, 6, True, 3, (0.3, -0.2, 0.5)), nprocs=2, join=True)
